@@ -1,0 +1,96 @@
+// c2_device.cuh -- device-side layouts and kernel arguments of the B200
+// implementation of the COMER2 search hot path.
+//
+// HBM layout (built by c2_upload_db / c2_set_query):
+//  * db position records, DR_STRIDE floats (224 B) per position, everything a
+//    score column and a DP column need, so one warp-uniform (broadcast) read
+//    stream per column feeds all 32 lanes (lanes own query rows):
+//      [0,20)  target probabilities          [20,39) context vector
+//      39      cvnorm2 + 1 + 1/kappa0         40      CV log prior
+//      [41,44) SS probabilities C,E,H         44      SS table indices, packed
+//      45      P(H) + 0.1                     [48,55) DP transitions of the column
+//      55      residue letter
+//  * query position records, QR_STRIDE floats (256 B), the same fields for the
+//    query rows plus the column -1 boundary states of the reference's DP
+//    (see c2_host.cu: colm1 states).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace c2 {
+
+constexpr int NAA = 20, NCV = 19, NSS = 3;
+constexpr float LOG0 = -32768.0f;
+
+enum : int {
+    QR_TRG = 0, QR_CV = 20, QR_CN = 39, QR_PRIOR = 40, QR_SS = 41, QR_SSIDX = 44,
+    QR_HQ = 47, QR_TRN = 48, QR_C = 55, QR_CP = 58, QR_STRIDE = 64
+};
+enum : int {
+    DR_TRG = 0, DR_CV = 20, DR_CN = 39, DR_PRIOR = 40, DR_SS = 41, DR_SSIDX = 44,
+    DR_HD = 45, DR_TRN = 48, DR_AA = 55, DR_STRIDE = 56
+};
+// DP transitions of a row/column: MM and MD, IM, DM, DD into the position,
+// MI and II out of it (the reference's MMp, MIc, MDp, IMp, IIc, DMp, DDp;
+// src/libmycu/cudp/CuBatchDP_init.cuh:132-155)
+enum : int { TMM = 0, TMI, TMD, TIM, TII, TDM, TDD };
+
+// btck codes (src/libmycu/cudp/CuBatchDP_com.h:99-104)
+enum : int { BT_STOP = 0, BT_LEFT = 1, BT_UP = 2, BT_DIAG = 3 };
+
+struct ScoreConsts {
+    float ssswgt, cvswgt, shift;          // term weights, aa-term shift
+    float lokappa0, pownu0, cterm;        // context-vector constants
+    float cvkey_first, cvkey_last, cvval_first, cvval_last;
+    int cvcard, cvshift, ssss_card;
+};
+
+constexpr int P1_WARPS = 8;               // warps per CTA of the DP kernels
+constexpr int MAX_SSSS_CARD = 32;
+constexpr int MAX_CVCARD = 256;
+
+struct P1Args {
+    const float* qrec;      // [Lq][QR_STRIDE]
+    int Lq;
+    const float* drec;      // [npos][DR_STRIDE]
+    const int* plen;        // [nprof]
+    const long long* poff;  // [nprof]
+    const float* pbkg;      // [nprof][20]
+    int nwork;              // number of work items (profiles or candidates)
+    const int* order;       // work item -> profile
+    int* counter;           // work-queue head
+    const float* ssss;      // [card][card]
+    const float* cvvals;    // [cvcard]
+    ScoreConsts sc;
+    float* bot;             // strip-boundary rows: per warp slot 2 x 5 x Lmax
+    long long botstride;    // floats per warp slot
+    // phase-1 outputs (indexed by profile)
+    float* best;
+    unsigned* coords;
+    // traceback variant: per work item k, scratch at cand_off[k]
+    const long long* cand_off;  // byte offsets into btck / float offsets into smat
+    signed char* btck;          // [L][Lq] per candidate (column-major)
+    float* smat;                // [L][Lq] per candidate
+    int* status;                // device error word (0 = ok)
+};
+
+struct FinArgs {
+    int Lq;
+    int ncand;
+    const int* cand_prof;
+    const long long* cand_off;
+    const int* plen;
+    const signed char* btck;
+    const float* smat;
+    const float* best;
+    const unsigned* coords;
+    float scorethld;
+    // outputs [ncand]
+    float* score;
+    int* psts;
+    unsigned* beg;
+    unsigned* endc;
+    int* passed;
+};
+
+}  // namespace c2

@@ -1,0 +1,436 @@
+// c2_kernels.cu -- phase-1 (fused score matrix + Viterbi DP) and DP
+// finalisation kernels for sm_100a.
+//
+// Phase 1 replaces the reference's CalcSM_Init_SMEMUnroll2x +
+// CalcSM_SSSS_CVS2S_SMEMUnroll2x_2 (src/libmycu/cusco/) and the per-diagonal
+// ExecDP_Btck_Unroll32x launches (src/libmycu/cudp/CuBatchDP.cu:149-320,
+// CuBatchDP_init_btck.cu:65-494).  Instead of materialising the L_q x N score
+// matrix and a traceback byte per cell in HBM, one persistent warp owns one
+// (query, db profile) pair at a time:
+//  * lanes own query rows (a strip of 32 rows at a time); the query-row
+//    operands of the score live in registers for the whole strip;
+//  * each step, the warp reads one db column record with warp-uniform
+//    (broadcast) loads and every lane scores its row against it; the score
+//    goes to a per-lane ring in shared memory;
+//  * the DP runs as an anti-diagonal wavefront: lane t processes column k-t at
+//    step k, taking its "up" states from lane t-1 by __shfl_up_sync, its
+//    "diagonal" states from the previous step's "up", and the column's
+//    transitions passed down the lanes the same way;
+//  * the strip's last row is handed to the next strip through a per-warp
+//    boundary buffer (global memory, L2 resident).
+// The traceback variant (TB = true) recomputes the same DP for the pairs that
+// pass the phase-1 threshold and stores their scores and btck codes
+// column-major for the finalisation, statistics and MAP stages.
+#include "c2_device.cuh"
+
+namespace c2 {
+
+#define FULL 0xffffffffu
+
+__device__ __forceinline__ int corner_edge(int lq, int ld)
+{
+    // GetCornerMaxlen, src/libmycu/cudp/CuBatchDP_init_btck.cuh:118-127
+    int m = lq > ld ? lq : ld;
+    int e = (int)rintf(0.34f * (float)m);
+    return e > 60 ? 60 : e;
+}
+
+__device__ __forceinline__ bool in_corner(int lq, int ld, int e, int y, int x)
+{
+    // CellYXinCorners, src/libmycu/cudp/CuBatchDP_init_btck.cuh:129-145
+    return (lq <= y + e && x <= e + y - lq) || (ld - e + y <= x && y < e);
+}
+
+// Score of (own query row, db column) -- src/libmycu/cusco/CuBatchScoreMatrix_Init.cu:129-182,
+// _ssss.cuh:48-131, _cvs2s.cuh:47-136.  The aa term uses the per-pair row
+// factors Qt[a] = q(a) / (0.5 (bq(a) + bd(a))); the SS term uses the per-row
+// table U[c] = sum_s p_q(s) T[idx_q(s)][c].
+struct RowOps {
+    float Qt[NAA];
+    float qcv[NCV];
+    float cq, pq, hq;
+};
+
+__device__ __forceinline__ float cell_score(const RowOps& R, const float4* __restrict__ rp,
+                                            const float* __restrict__ U, const float* __restrict__ cvtab,
+                                            const ScoreConsts& sc, int lane, float& aa_out)
+{
+    float4 v;
+    // aa term
+    float s = 0.f;
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+        v = __ldg(rp + i);
+        s = fmaf(R.Qt[4 * i + 0], v.x, s);
+        s = fmaf(R.Qt[4 * i + 1], v.y, s);
+        s = fmaf(R.Qt[4 * i + 2], v.z, s);
+        s = fmaf(R.Qt[4 * i + 3], v.w, s);
+    }
+    const float s0 = __logf(s) - sc.shift;
+    // CV term: dot product over [20,39), then (cq)(cd) - (dot+1/kappa0)^2
+    float dot = 0.f;
+#pragma unroll
+    for (int i = 5; i < 10; i++) {
+        v = __ldg(rp + i);
+        const int b = 4 * i - DR_CV;
+        dot = fmaf(R.qcv[b + 0], v.x, dot);
+        dot = fmaf(R.qcv[b + 1], v.y, dot);
+        dot = fmaf(R.qcv[b + 2], v.z, dot);
+        if (b + 3 < NCV) dot = fmaf(R.qcv[b + 3], v.w, dot);
+    }
+    const float cd = v.w;  // DR_CN = 39
+    v = __ldg(rp + 10);    // 40 prior, 41..43 ss
+    const float pd = v.x;
+    const float ds0 = v.y, ds1 = v.z, ds2 = v.w;
+    const float4 v11 = __ldg(rp + 11);  // 44 ss idx, 45 hd
+    dot += sc.lokappa0;
+    float det = R.cq * cd - dot * dot;
+    float cvs = sc.cterm + sc.pownu0 * __logf(det) - R.pq - pd;
+    float cvm;
+    if (cvs <= sc.cvkey_first) cvm = sc.cvval_first;
+    else if (sc.cvkey_last <= cvs) cvm = sc.cvval_last;
+    else {
+        // clamp keeps the shared-memory read in bounds for any table/argument
+        const int ix = min(max(sc.cvshift + (int)rintf(2.f * cvs), 0), sc.cvcard - 1);
+        cvm = cvtab[ix * 32 + lane];
+    }
+    cvm *= sc.cvswgt;
+    // SS term
+    const int pk = __float_as_int(v11.x);
+    float ss = ds0 * U[(pk & 0xff) * 32 + lane];
+    ss = fmaf(ds1, U[((pk >> 8) & 0xff) * 32 + lane], ss);
+    ss = fmaf(ds2, U[((pk >> 16) & 0xff) * 32 + lane], ss);
+    if (-99.f < ss) {
+        ss += R.hq * v11.y * 0.1111111f;
+        ss -= 0.05f;
+        ss *= sc.ssswgt;
+    }
+    aa_out = s0;
+    return s0 + (ss + cvm);
+}
+
+struct St5 { float MM, MI, IM, DN, ND; };
+
+template <bool TB>
+__global__ void __launch_bounds__(P1_WARPS * 32, 2)
+p1_kernel(P1Args a, const float* __restrict__ qbkg)
+{
+    extern __shared__ float smem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int cvcard = a.sc.cvcard;
+    const int card = a.sc.ssss_card;
+    float* cvtab = smem;                                      // [cvcard][32]
+    float* wb = smem + cvcard * 32 + wid * (32 * 32 + MAX_SSSS_CARD * 32);
+    float* ring = wb;                                         // [32][32]
+    float* U = wb + 32 * 32;                                  // [card][32]
+    for (int i = threadIdx.x; i < cvcard * 32; i += blockDim.x) cvtab[i] = a.cvvals[i >> 5];
+    __syncthreads();
+
+    const long long slot = (long long)blockIdx.x * P1_WARPS + wid;
+    const int Lmax = (int)(a.botstride / 10);
+    float* bot0 = a.bot + slot * a.botstride;
+    const int Lq = a.Lq;
+    const int nstrips = (Lq + 31) >> 5;
+    const ScoreConsts sc = a.sc;
+
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.counter, 1);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= a.nwork) break;
+        const int p = a.order[item];
+        const int L = a.plen[p];
+        const long long off = a.poff[p];
+        const float* __restrict__ dr = a.drec + off * DR_STRIDE;
+        const float* __restrict__ bd = a.pbkg + (long long)p * NAA;
+        const int edge = corner_edge(Lq, L);
+        signed char* bt = nullptr;
+        float* smt = nullptr;
+        if (TB) {
+            bt = a.btck + a.cand_off[item];
+            smt = a.smat + a.cand_off[item];
+        }
+        float best = 0.f;
+        int brow = 0x7fffffff, bcol = 0x7fffffff;
+        float* botr = bot0;
+        float* botw = bot0 + 5 * Lmax;
+
+        for (int s = 0; s < nstrips; s++) {
+            const int r = s * 32 + lane;
+            const bool act = r < Lq;
+            const float* __restrict__ qr = a.qrec + (long long)(act ? r : Lq - 1) * QR_STRIDE;
+            RowOps R;
+#pragma unroll
+            for (int i = 0; i < NAA; i++)
+                R.Qt[i] = __fdividef(qr[QR_TRG + i], 0.5f * (qbkg[i] + bd[i]));
+#pragma unroll
+            for (int i = 0; i < NCV; i++) R.qcv[i] = qr[QR_CV + i];
+            R.cq = qr[QR_CN];
+            R.pq = qr[QR_PRIOR];
+            R.hq = qr[QR_HQ];
+            {
+                const float q0 = qr[QR_SS], q1 = qr[QR_SS + 1], q2 = qr[QR_SS + 2];
+                const int i0 = (int)(q0 * 9.999f), i1 = 10 + (int)(q1 * 9.999f), i2 = 20 + (int)(q2 * 9.999f);
+                for (int c = 0; c < card; c++)
+                    U[c * 32 + lane] = q0 * __ldg(a.ssss + i0 * card + c) + q1 * __ldg(a.ssss + i1 * card + c) +
+                                       q2 * __ldg(a.ssss + i2 * card + c);
+            }
+            float q7[7];
+#pragma unroll
+            for (int i = 0; i < 7; i++) q7[i] = act ? qr[QR_TRN + i] : LOG0;
+            // column -1 boundary states of this row and of the row above
+            const bool z_left = (lane == 31);
+            const bool z_diag = (lane == 31 || lane == 0);
+            const St5 LB = z_left ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
+                                  : St5{0.f, qr[QR_C + 0], qr[QR_C + 1], qr[QR_C + 2], LOG0};
+            const St5 DB = z_diag ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
+                                  : St5{0.f, qr[QR_CP + 0], qr[QR_CP + 1], qr[QR_CP + 2], LOG0};
+            __syncwarp();
+
+            St5 mine = {0.f, 0.f, 0.f, 0.f, 0.f};
+            St5 upp = {0.f, 0.f, 0.f, 0.f, 0.f};
+            float t7[7];
+#pragma unroll
+            for (int i = 0; i < 7; i++) t7[i] = LOG0;
+            // strip-boundary prefetch: lane i holds column c0 + i of the row above
+            float bcur[5], bnxt[5];
+#pragma unroll
+            for (int f = 0; f < 5; f++) {
+                bcur[f] = 0.f;
+                bnxt[f] = 0.f;
+                if (s > 0) {
+                    if (lane < L) bcur[f] = botr[f * Lmax + lane];
+                    if (32 + lane < L) bnxt[f] = botr[f * Lmax + 32 + lane];
+                }
+            }
+            const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
+            const int nsteps = L + 31;
+            for (int k = 0; k < nsteps; k++) {
+                // ---- score stage: column k for every lane's row
+                float tc[7];
+                if (k < L) {
+                    const float4* rp = reinterpret_cast<const float4*>(dr + (long long)k * DR_STRIDE);
+                    float aa;
+                    float S = cell_score(R, rp, U, cvtab, sc, lane, aa);
+                    if (!act) S = -9.f;
+                    ring[(k & 31) * 32 + lane] = S;
+                    if (TB && act) smt[(long long)k * Lq + r] = S;
+                    const float4 ta = __ldg(rp + 12), tb = __ldg(rp + 13);
+                    tc[0] = ta.x; tc[1] = ta.y; tc[2] = ta.z; tc[3] = ta.w;
+                    tc[4] = tb.x; tc[5] = tb.y; tc[6] = tb.z;
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 7; i++) tc[i] = LOG0;
+                }
+                // ---- DP stage: column j = k - lane
+#pragma unroll
+                for (int i = 0; i < 7; i++) {
+                    const float x = __shfl_up_sync(FULL, t7[i], 1);
+                    t7[i] = (lane == 0) ? tc[i] : x;
+                }
+                St5 up;
+                up.MM = __shfl_up_sync(FULL, mine.MM, 1);
+                up.MI = __shfl_up_sync(FULL, mine.MI, 1);
+                up.IM = __shfl_up_sync(FULL, mine.IM, 1);
+                up.DN = __shfl_up_sync(FULL, mine.DN, 1);
+                up.ND = __shfl_up_sync(FULL, mine.ND, 1);
+                {
+                    const int src = k & 31;
+                    const float b0 = __shfl_sync(FULL, bcur[0], src);
+                    const float b1 = __shfl_sync(FULL, bcur[1], src);
+                    const float b2 = __shfl_sync(FULL, bcur[2], src);
+                    const float b3 = __shfl_sync(FULL, bcur[3], src);
+                    const float b4 = __shfl_sync(FULL, bcur[4], src);
+                    if (lane == 0) up = St5{b0, b1, b2, b3, b4};
+                    if (src == 31) {
+#pragma unroll
+                        for (int f = 0; f < 5; f++) {
+                            bcur[f] = bnxt[f];
+                            const int c = k + 33 + lane;
+                            bnxt[f] = (s > 0 && c < L) ? botr[f * Lmax + c] : 0.f;
+                        }
+                    }
+                }
+                const int j = k - lane;
+                St5 left = mine, diag = upp;
+                if (j == 0) { left = LB; diag = DB; }
+                float S = -9.f;
+                if (j >= 0 && j < L) {
+                    S = ring[(j & 31) * 32 + lane];
+                    if (in_corner(Lq, L, edge, r, j)) S = -9.f;
+                }
+                St5 nw;
+                {
+                    float v = fmaxf((diag.MI + q7[TMM]) + t7[TIM], (diag.IM + q7[TIM]) + t7[TMM]);
+                    v = fmaxf(v, (diag.DN + q7[TDM]) + t7[TMM]);
+                    v = fmaxf(v, (diag.ND + q7[TMM]) + t7[TDM]);
+                    v = fmaxf(v, (diag.MM + q7[TMM]) + t7[TMM]);
+                    nw.MM = fmaxf(v + S, 0.f);
+                    nw.MI = fmaxf((up.MM + q7[TMM]) + t7[TMI], (up.MI + q7[TMM]) + t7[TII]);
+                    nw.IM = fmaxf((left.MM + q7[TMI]) + t7[TMM], (left.IM + q7[TII]) + t7[TMM]);
+                    nw.DN = fmaxf(up.MM + q7[TMD], up.DN + q7[TDD]);
+                    nw.ND = fmaxf(left.MM + t7[TMD], left.ND + t7[TDD]);
+                }
+                const bool valid = act && j >= 0 && j < L;
+                if (valid && nw.MM > best) { best = nw.MM; brow = r; bcol = j; }
+                if (TB && valid) {
+                    int b = BT_STOP;
+                    float mx = nw.MM;
+                    if (nw.MM != 0.f) b = BT_DIAG;
+                    if (mx < nw.MI) { mx = nw.MI; b = BT_UP; }
+                    if (mx < nw.IM) { mx = nw.IM; b = BT_LEFT; }
+                    if (mx < nw.DN) { mx = nw.DN; b = BT_UP; }
+                    if (mx < nw.ND) { b = BT_LEFT; }
+                    bt[(long long)j * Lq + r] = (signed char)b;
+                }
+                if (wr_bot && j >= 0 && j < L) {
+                    botw[0 * Lmax + j] = nw.MM;
+                    botw[1 * Lmax + j] = nw.MI;
+                    botw[2 * Lmax + j] = nw.IM;
+                    botw[3 * Lmax + j] = nw.DN;
+                    botw[4 * Lmax + j] = nw.ND;
+                }
+                mine = nw;
+                upp = up;
+            }
+            float* t = botr; botr = botw; botw = t;
+            __syncwarp();
+        }
+        // warp arg-max: largest score, then smallest row, then smallest column
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            const float ob = __shfl_xor_sync(FULL, best, o);
+            const int orr = __shfl_xor_sync(FULL, brow, o);
+            const int oc = __shfl_xor_sync(FULL, bcol, o);
+            if (ob > best || (ob == best && (orr < brow || (orr == brow && oc < bcol)))) {
+                best = ob; brow = orr; bcol = oc;
+            }
+        }
+        if (lane == 0) {
+            const unsigned xy = (best > 0.f) ? (((unsigned)bcol << 16) | ((unsigned)brow & 0xffffu)) : 0u;
+            if (TB) {
+                // consistency check against the phase-1 result of this pair
+                if (a.best[p] != best && a.status) atomicCAS(a.status, 0, 2);
+            } else {
+                a.best[p] = best;
+                a.coords[p] = xy;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Warp butterfly sum as the reference's FinalizeDPPro reduction
+// (src/libmycu/cudp/CuBatchDP_final.cu:254-260).
+__device__ __forceinline__ float warp_butterfly(float v)
+{
+    v += __shfl_xor_sync(FULL, v, 16);
+    v += __shfl_xor_sync(FULL, v, 8);
+    v += __shfl_xor_sync(FULL, v, 4);
+    v += __shfl_xor_sync(FULL, v, 2);
+    v += __shfl_xor_sync(FULL, v, 1);
+    return v;
+}
+
+// DP finalisation, one warp per candidate pair
+// (src/libmycu/cudp/CuBatchDP_final.cu:170-290).
+__global__ void __launch_bounds__(256) fin_kernel(FinArgs a)
+{
+    __shared__ float cache[8][36];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int c = blockIdx.x * 8 + wid;
+    if (c >= a.ncand) return;
+    const int p = a.cand_prof[c];
+    const int Lq = a.Lq;
+    const int L = a.plen[p];
+    const signed char* bt = a.btck + a.cand_off[c];
+    const float* sm = a.smat + a.cand_off[c];
+    float* ch = cache[wid];
+    const float maxsc = a.best[p];
+    const unsigned xx = a.coords[p];
+    int x = (int)(xx >> 16), y = (int)(xx & 0xffff);
+    int psts = 0;
+    int b = BT_DIAG;
+    int ndx = 0;
+    float sum = 0.f;
+    if (lane < 4) ch[32 + lane] = 0.f;
+    __syncwarp();
+    // the walk is bounded by the number of cells on any monotone path
+    int guard = Lq + L + 2;
+    while (b != BT_STOP) {
+        if (lane < 4) ch[lane] = ch[32 + lane];
+        __syncwarp();
+        if (lane == 0) {
+            for (ndx = 4; ndx < 36;) {
+                if (x < 0 || y < 0 || --guard < 0) { b = BT_STOP; break; }
+                const long long qp = (long long)x * Lq + y;
+                b = bt[qp];
+                if (b == BT_STOP) break;
+                if (b == BT_UP) { y--; continue; }
+                if (b == BT_LEFT) { x--; continue; }
+                ch[ndx] = sm[qp];
+                if (ch[ndx] > 0.f) psts++;
+                x--; y--;
+                ndx++;
+            }
+        }
+        __syncwarp();
+        b = __shfl_sync(FULL, b, 0);
+        ndx = __shfl_sync(FULL, ndx, 0);
+        float cs = 0.f;
+        if (!(ndx <= lane + 4))
+            cs = ch[lane + 4] * (((ch[lane] + ch[lane + 1]) + ch[lane + 2]) + ch[lane + 3]);
+        sum += warp_butterfly(cs);
+        __syncwarp();
+    }
+    if (lane == 0) {
+        sum *= 0.5f;
+        sum = sum < 0.f ? -sqrtf(-sum) : sqrtf(sum);
+        const float sc = maxsc + sum;
+        a.score[c] = sc;
+        a.psts[c] = psts;
+        a.beg[c] = ((unsigned)(x + 1) << 16) | ((unsigned)(y + 1) & 0xffffu);
+        a.endc[c] = xx;
+        a.passed[c] = (a.scorethld < sc) ? 1 : 0;
+        (void)L;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers (host)
+size_t p1_smem_bytes(int cvcard)
+{
+    return (size_t)(cvcard * 32 + P1_WARPS * (32 * 32 + MAX_SSSS_CARD * 32)) * sizeof(float);
+}
+
+cudaError_t launch_p1(const P1Args& a, const float* qbkg, bool tb, int grid, cudaStream_t st)
+{
+    const size_t sm = p1_smem_bytes(a.sc.cvcard);
+    if (tb) {
+        cudaFuncSetAttribute(p1_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        p1_kernel<true><<<grid, P1_WARPS * 32, sm, st>>>(a, qbkg);
+    } else {
+        cudaFuncSetAttribute(p1_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        p1_kernel<false><<<grid, P1_WARPS * 32, sm, st>>>(a, qbkg);
+    }
+    return cudaGetLastError();
+}
+
+int p1_blocks_per_sm(int cvcard)
+{
+    int n = 0;
+    const size_t sm = p1_smem_bytes(cvcard);
+    cudaFuncSetAttribute(p1_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, p1_kernel<false>, P1_WARPS * 32, sm);
+    return n > 0 ? n : 1;
+}
+
+cudaError_t launch_fin(const FinArgs& a, cudaStream_t st)
+{
+    if (a.ncand <= 0) return cudaSuccess;
+    const int grid = (a.ncand + 7) / 8;
+    fin_kernel<<<grid, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace c2

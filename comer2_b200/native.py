@@ -1,0 +1,248 @@
+"""ctypes binding of the C ABI in ``include/comer2_b200.h``.
+
+The shared library is built in-tree (``comer2_b200/_lib/libcomer2_b200.so``,
+see ``build.py``).  There is no fallback: if the library cannot be loaded,
+every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from .params import SearchParams
+from .synth import ProfileSet
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libcomer2_b200.so")
+
+C2_OK = 0
+STATUS_NAMES = {0: "C2_OK", 1: "C2_ERR_ARG", 2: "C2_ERR_CUDA", 3: "C2_ERR_NOMEM", 4: "C2_ERR_STATE",
+                5: "C2_ERR_CAPACITY", 6: "C2_ERR_DEVICE"}
+
+# every symbol include/comer2_b200.h declares
+EXPORTS = [
+    "c2_create", "c2_destroy", "c2_last_error", "c2_upload_db", "c2_set_query", "c2_run_phase1",
+    "c2_get_phase1", "c2_run_finalize", "c2_get_finalize", "c2_get_thresholds", "c2_set_stream", "c2_sync",
+    "c2_launch_count",
+]
+
+_fp = C.POINTER(C.c_float)
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class c2_params(C.Structure):
+    _fields_ = [
+        ("ungapped_lambda", C.c_float), ("ungapped_K", C.c_float), ("ungapped_H", C.c_float),
+        ("gapped_lambda", C.c_float), ("gapped_K", C.c_float), ("gapped_H", C.c_float),
+        ("gapped_alpha", C.c_float), ("gapped_beta", C.c_float),
+        ("eval", C.c_float), ("ssswgt", C.c_float), ("cvswgt", C.c_float), ("minpp", C.c_float),
+        ("mapaln", C.c_int32), ("x_uninf", C.c_int32), ("ssemodel", C.c_int32),
+        ("ssss", _fp), ("ssss_card", C.c_int32),
+        ("cvs2s_keys", _fp), ("cvs2s_values", _fp), ("cvs2s_card", C.c_int32), ("cvs2s_shift", C.c_int32),
+        ("sse_nn_weights", _fp), ("n_sse_nn_weights", C.c_int32),
+    ]
+
+
+class c2_profiles(C.Structure):
+    _fields_ = [
+        ("nprofiles", C.c_int32), ("npositions", C.c_int64),
+        ("lengths", _i32p), ("offsets", _i64p), ("bkg", _fp), ("eno", _fp), ("trn", _fp),
+        ("trg", _fp), ("cv", _fp), ("cvprior", _fp), ("cvnorm2", _fp), ("ss", _fp),
+        ("ssstate", _u8p), ("aa", _u8p),
+    ]
+
+
+class c2_p1_result(C.Structure):
+    _fields_ = [("best", C.c_float), ("coords", C.c_uint32)]
+
+
+class c2_dp_result(C.Structure):
+    _fields_ = [("score", C.c_float), ("profile", C.c_int32), ("psts", C.c_int32),
+                ("beg", C.c_uint32), ("end", C.c_uint32), ("passed", C.c_int32)]
+
+
+_lib: Optional[C.CDLL] = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load the CUDA library (raises OSError when it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError("comer2_b200 CUDA library not built: %s (run comer2_b200/build.py)" % path)
+    lib = C.CDLL(path)
+    P = C.POINTER
+    lib.c2_create.argtypes = [C.c_int, P(c2_params), P(C.c_void_p)]
+    lib.c2_destroy.argtypes = [C.c_void_p]
+    lib.c2_last_error.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
+    lib.c2_upload_db.argtypes = [C.c_void_p, P(c2_profiles), C.c_uint64, C.c_uint64]
+    lib.c2_set_query.argtypes = [C.c_void_p, P(c2_profiles)]
+    lib.c2_run_phase1.argtypes = [C.c_void_p]
+    lib.c2_get_phase1.argtypes = [C.c_void_p, P(c2_p1_result), C.c_int32]
+    lib.c2_run_finalize.argtypes = [C.c_void_p, P(C.c_int32)]
+    lib.c2_get_finalize.argtypes = [C.c_void_p, P(c2_dp_result), C.c_int32]
+    lib.c2_get_thresholds.argtypes = [C.c_void_p, P(C.c_float), P(C.c_float)]
+    lib.c2_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    lib.c2_sync.argtypes = [C.c_void_p]
+    lib.c2_launch_count.argtypes = [C.c_void_p, P(C.c_uint64)]
+    for n in EXPORTS:
+        getattr(lib, n).restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray, t):
+    return a.ctypes.data_as(t)
+
+
+class _Keep:
+    """Holds numpy arrays alive while a ctypes struct points into them."""
+
+    def __init__(self):
+        self.arrs = []
+
+    def f32(self, x):
+        a = np.ascontiguousarray(x, np.float32)
+        self.arrs.append(a)
+        return _ptr(a, _fp)
+
+    def i32(self, x):
+        a = np.ascontiguousarray(x, np.int32)
+        self.arrs.append(a)
+        return _ptr(a, _i32p)
+
+    def i64(self, x):
+        a = np.ascontiguousarray(x, np.int64)
+        self.arrs.append(a)
+        return _ptr(a, _i64p)
+
+    def u8(self, x):
+        a = np.ascontiguousarray(x, np.uint8)
+        self.arrs.append(a)
+        return _ptr(a, _u8p)
+
+
+def make_params(p: SearchParams, keep: _Keep) -> c2_params:
+    s = c2_params()
+    for k in ("ungapped_lambda", "ungapped_K", "ungapped_H", "gapped_lambda", "gapped_K", "gapped_H",
+              "gapped_alpha", "gapped_beta", "eval", "ssswgt", "cvswgt", "minpp"):
+        setattr(s, k, float(getattr(p, k)))
+    s.mapaln, s.x_uninf, s.ssemodel = int(p.mapaln), int(p.x_uninf), int(p.ssemodel)
+    s.ssss = keep.f32(p.ssss.reshape(-1))
+    s.ssss_card = int(p.ssss_card)
+    s.cvs2s_keys = keep.f32(p.cvs2s_keys)
+    s.cvs2s_values = keep.f32(p.cvs2s_values)
+    s.cvs2s_card = int(p.cvs2s_card)
+    s.cvs2s_shift = int(p.cvs2s_shift)
+    s.sse_nn_weights = keep.f32(p.sse_nn_weights)
+    s.n_sse_nn_weights = int(p.sse_nn_weights.shape[0])
+    return s
+
+
+def make_profiles(ps: ProfileSet, keep: _Keep) -> c2_profiles:
+    s = c2_profiles()
+    s.nprofiles = ps.nprofiles
+    s.npositions = ps.npositions
+    s.lengths = keep.i32(ps.lengths)
+    s.offsets = keep.i64(ps.offsets)
+    s.bkg = keep.f32(ps.bkg)
+    s.eno = keep.f32(ps.eno)
+    s.trn = keep.f32(ps.trn)
+    s.trg = keep.f32(ps.trg)
+    s.cv = keep.f32(ps.cv)
+    s.cvprior = keep.f32(ps.cvprior)
+    s.cvnorm2 = keep.f32(ps.cvnorm2)
+    s.ss = keep.f32(ps.ss)
+    s.ssstate = keep.u8(ps.ssstate)
+    s.aa = keep.u8(ps.aa)
+    return s
+
+
+class C2Error(RuntimeError):
+    pass
+
+
+class Handle:
+    """One search context on one GPU (wraps a ``c2_handle``)."""
+
+    def __init__(self, params: SearchParams, device: int = 0):
+        self.lib = load()
+        self._keep = _Keep()
+        self.params = params
+        self._h = C.c_void_p()
+        sp = make_params(params, self._keep)
+        st = self.lib.c2_create(device, C.byref(sp), C.byref(self._h))
+        if st != C2_OK:
+            raise C2Error("c2_create failed: %s" % STATUS_NAMES.get(st, st))
+        self.nprof = 0
+
+    def _ck(self, st, what):
+        if st != C2_OK:
+            buf = C.create_string_buffer(512)
+            self.lib.c2_last_error(self._h, buf, 512)
+            raise C2Error("%s: %s: %s" % (what, STATUS_NAMES.get(st, st), buf.value.decode()))
+
+    def close(self):
+        if self._h:
+            self.lib.c2_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload_db(self, db: ProfileSet, total_positions: int = 0, total_profiles: int = 0):
+        k = _Keep()
+        s = make_profiles(db, k)
+        self._ck(self.lib.c2_upload_db(self._h, C.byref(s), total_positions, total_profiles), "c2_upload_db")
+        self.nprof = db.nprofiles
+
+    def set_query(self, q: ProfileSet):
+        k = _Keep()
+        s = make_profiles(q, k)
+        self._ck(self.lib.c2_set_query(self._h, C.byref(s)), "c2_set_query")
+
+    def thresholds(self):
+        a, b = C.c_float(), C.c_float()
+        self._ck(self.lib.c2_get_thresholds(self._h, C.byref(a), C.byref(b)), "c2_get_thresholds")
+        return a.value, b.value
+
+    def run_phase1(self):
+        self._ck(self.lib.c2_run_phase1(self._h), "c2_run_phase1")
+
+    def set_stream(self, stream_ptr: int):
+        """Issue work on a caller-owned cudaStream_t (e.g. torch.cuda.current_stream().cuda_stream)."""
+        self._ck(self.lib.c2_set_stream(self._h, C.c_void_p(stream_ptr)), "c2_set_stream")
+
+    def sync(self):
+        self._ck(self.lib.c2_sync(self._h), "c2_sync")
+
+    def phase1(self):
+        out = (c2_p1_result * self.nprof)()
+        self._ck(self.lib.c2_get_phase1(self._h, out, self.nprof), "c2_get_phase1")
+        arr = np.frombuffer(out, dtype=np.dtype([("best", np.float32), ("coords", np.uint32)]), count=self.nprof)
+        return arr["best"].copy(), arr["coords"].copy()
+
+    def run_finalize(self) -> int:
+        n = C.c_int32()
+        self._ck(self.lib.c2_run_finalize(self._h, C.byref(n)), "c2_run_finalize")
+        return n.value
+
+    def finalize(self, n: int):
+        out = (c2_dp_result * max(n, 1))()
+        self._ck(self.lib.c2_get_finalize(self._h, out, n), "c2_get_finalize")
+        dt = np.dtype([("score", np.float32), ("profile", np.int32), ("psts", np.int32),
+                       ("beg", np.uint32), ("end", np.uint32), ("passed", np.int32)])
+        return np.frombuffer(out, dtype=dt, count=n).copy()
+
+    def launch_count(self) -> int:
+        n = C.c_uint64()
+        self._ck(self.lib.c2_launch_count(self._h, C.byref(n)), "c2_launch_count")
+        return n.value

@@ -1,0 +1,162 @@
+/*
+ * comer2_b200.h -- C ABI of the B200 implementation of the COMER2 search hot
+ * path (profile-profile scores, Viterbi ranking DP, E-value statistics and
+ * MAP alignment).
+ *
+ * The reference has no plugin API for this path; its boundary is the C++
+ * class CuBatchProcessing (src/libmycu/cupro/CuBatchProcessing.cuh:47-244),
+ * driven by DevCommThread (src/libmycu/cualn/DevCommThread.cpp:155-165,296-356).
+ * Each entry point below names the reference call it replaces.
+ *
+ * Conventions: plain C types, pointers and sizes only; every call returns a
+ * c2_status; a handle is used by one host thread at a time; the last error
+ * text of a handle is available through c2_last_error().  No call traps or
+ * aborts: device-side problems come back as status codes.
+ */
+#ifndef COMER2_B200_H
+#define COMER2_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    C2_OK = 0,
+    C2_ERR_ARG = 1,        /* invalid argument or inconsistent sizes */
+    C2_ERR_CUDA = 2,       /* a CUDA runtime call failed */
+    C2_ERR_NOMEM = 3,      /* device or host allocation failed */
+    C2_ERR_STATE = 4,      /* call out of order (e.g. search before upload) */
+    C2_ERR_CAPACITY = 5,   /* a size exceeds a compiled limit */
+    C2_ERR_DEVICE = 6      /* a kernel reported an error status */
+} c2_status;
+
+/* Search parameters: comer.par constants, option values and score tables.
+ * Replaces the Configuration[] / MOptions / SSSScores / CVS2Scores state the
+ * reference passes to CuBatchProcessing's constructor and CuDeviceMemory
+ * (CuBatchProcessing.cuh:51-60, CuDeviceMemory.cuh:640-760). */
+typedef struct {
+    float ungapped_lambda, ungapped_K, ungapped_H;        /* [UNGAPPED]  */
+    float gapped_lambda, gapped_K, gapped_H;             /* [GAPPED_A_1] */
+    float gapped_alpha, gapped_beta;
+    float eval;            /* EVAL */
+    float ssswgt;          /* SSSWGT */
+    float cvswgt;          /* CVSWGT */
+    float minpp;           /* MINPP */
+    int32_t mapaln;        /* MAPALN */
+    int32_t x_uninf;       /* X_UNINF */
+    int32_t ssemodel;      /* SSEMODEL */
+    const float* ssss;     /* SS score table, ssss_card x ssss_card, symmetric */
+    int32_t ssss_card;
+    const float* cvs2s_keys;    /* smoothed CV score map: keys, step 0.5 */
+    const float* cvs2s_values;  /* values */
+    int32_t cvs2s_card;
+    int32_t cvs2s_shift;        /* number of negative keys */
+    const float* sse_nn_weights;  /* SS18 model weights + adjustment constants */
+    int32_t n_sse_nn_weights;
+} c2_params;
+
+/* A set of profiles in structure-of-arrays form over concatenated positions
+ * (the field set of PM2DVectorFields, src/libmycu/cupro/PM2DVectorFields.h:48-81).
+ * trn holds nprofiles + npositions rows of 7 log-space transition values
+ * (MM MI MD IM II DM DD; IM..DD scaled by 0.4, log 0 = -32768): row
+ * offsets[k] + k + i holds the transitions into position i of profile k. */
+typedef struct {
+    int32_t nprofiles;
+    int64_t npositions;
+    const int32_t* lengths;   /* [nprofiles] */
+    const int64_t* offsets;   /* [nprofiles] first position of each profile */
+    const float* bkg;         /* [nprofiles][20] background probabilities */
+    const float* eno;         /* [nprofiles] effective number of observations */
+    const float* trn;         /* [npositions + nprofiles][7] */
+    const float* trg;         /* [npositions][20] target probabilities */
+    const float* cv;          /* [npositions][19] context vectors */
+    const float* cvprior;     /* [npositions] */
+    const float* cvnorm2;     /* [npositions] */
+    const float* ss;          /* [npositions][3] SS probabilities C,E,H */
+    const uint8_t* ssstate;   /* [npositions] 'C','E','H' */
+    const uint8_t* aa;        /* [npositions] residue letters */
+} c2_profiles;
+
+/* Per-pair result of phase 1 (Viterbi ranking DP). */
+typedef struct {
+    float best;          /* maximum MM score over the pair's DP matrix */
+    uint32_t coords;     /* (x << 16) | y of the maximum, x = db, y = query */
+} c2_p1_result;
+
+/* Per-pair result of the DP finalisation (one record per pair whose phase-1
+ * maximum exceeds the score threshold).  Layout of the reference's phase-1
+ * output section (TDP2OutputAlnData dp2oadScore..dp2oadEndCoords,
+ * src/libmycu/cuss/CuBatchSS_com.h:45-53). */
+typedef struct {
+    float score;         /* max + sgn(c/2) sqrt(|c/2|) with the correlation c */
+    int32_t profile;     /* db profile index */
+    int32_t psts;        /* number of positive substitution scores on the path */
+    uint32_t beg;        /* (x << 16) | y, 1-based beginning of the path */
+    uint32_t end;        /* (x << 16) | y of the maximum */
+    int32_t passed;      /* score > threshold */
+} c2_dp_result;
+
+typedef struct c2_handle c2_handle;
+
+/* Create a handle on a device; replaces CuBatchProcessing's constructor and
+ * CuDeviceMemory's table caching (CuDeviceMemory.cu:640-760). */
+c2_status c2_create(int device, const c2_params* params, c2_handle** out);
+
+/* Release all device and host resources of a handle. */
+c2_status c2_destroy(c2_handle* h);
+
+/* Copy the handle's last error message into buf (always NUL-terminated). */
+c2_status c2_last_error(const c2_handle* h, char* buf, size_t bufsize);
+
+/* Upload (and repack for the device) a database; replaces
+ * CuBatchProcessing::TransferCPMData (CuBatchProcessing.cuh:79-82) and
+ * SetDbDetails(db_len, nseqs) (:73).  db_total_positions/profiles describe
+ * the whole database (for the threshold and search space); 0 means "this
+ * upload is the whole database". */
+c2_status c2_upload_db(c2_handle* h, const c2_profiles* db,
+                       uint64_t db_total_positions, uint64_t db_total_profiles);
+
+/* Set the query profile (profile 0 of q); replaces SetQueryLen and the query
+ * part of ProcessScoreMatrix (CuBatchProcessing.cuh:87-99).  Computes the
+ * score threshold and log E threshold as JobDispatcher::CalculateScoreThreshold
+ * (src/libmycu/cualn/JobDispatcher.cpp:809-860). */
+c2_status c2_set_query(c2_handle* h, const c2_profiles* q);
+
+/* Run phase 1 (fused score matrix + Viterbi DP max) of the current query over
+ * the uploaded database on the device, asynchronously on the handle's stream;
+ * results stay on the device.  Replaces ComputeScoreMatrixDevice +
+ * PerformCompleteDynProgDevice's DP launches (CuBatchProcessing.cu:324-372). */
+c2_status c2_run_phase1(c2_handle* h);
+
+/* Wait for the handle's stream and copy phase-1 results, one per db profile. */
+c2_status c2_get_phase1(c2_handle* h, c2_p1_result* out, int32_t n);
+
+/* Run the DP finalisation (traceback, correlation score, pass decision) for
+ * the pairs whose phase-1 maximum exceeds the threshold; replaces
+ * FinalizeDP/FinalizeDPPro (src/libmycu/cudp/CuBatchDP_final.cu:55-396).
+ * Returns the number of finalised pairs in *ncand. */
+c2_status c2_run_finalize(c2_handle* h, int32_t* ncand);
+
+/* Copy finalisation records (in ascending profile order). */
+c2_status c2_get_finalize(c2_handle* h, c2_dp_result* out, int32_t n);
+
+/* Thresholds computed for the current query. */
+c2_status c2_get_thresholds(const c2_handle* h, float* scorethld, float* logevthld);
+
+/* Make the handle issue its work on a caller-owned CUDA stream (a
+ * cudaStream_t passed as void*; NULL restores the handle's own stream). */
+c2_status c2_set_stream(c2_handle* h, void* stream);
+
+/* Synchronize the handle's stream. */
+c2_status c2_sync(c2_handle* h);
+
+/* Number of kernel launches issued by the handle since creation. */
+c2_status c2_launch_count(const c2_handle* h, uint64_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

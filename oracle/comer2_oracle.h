@@ -1,0 +1,57 @@
+/*
+ * comer2_oracle.h -- CPU oracle of the COMER2 search hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the reference's
+ * algorithm (minmarg/comer2, src/libmycu/...), used by tests/, by
+ * __graft_entry__.smoke() and by bench.py's CPU-baseline leg as the checker.
+ * The product (comer2_b200) never links or calls it.
+ *
+ * The same source builds twice: REAL=float (liborc32.so) follows the
+ * reference's float operation order, REAL=double (liborc64.so) is the FP64
+ * error reference.  CUDA fast intrinsics (__logf, __fdividef) are replaced by
+ * the C library's IEEE functions, so the float build differs from the
+ * reference's device results by rounding only.
+ *
+ * Parity pinning: the reference has no tests, fixtures or golden vectors for
+ * this path (its tree holds none); see tests/golden/ for the fixtures this
+ * oracle is pinned to.
+ */
+#ifndef COMER2_ORACLE_H
+#define COMER2_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    float ssswgt, cvswgt;
+    int mapaln;                 /* MAPALN option: 1 -> init shift 0.002, no prior rounding */
+    const float* ssss;          /* card x card symmetric SS score table */
+    int ssss_card;
+    const float* cvkeys;        /* smoothed CV map keys [cvcard] */
+    const float* cvvals;        /* smoothed CV map values [cvcard] */
+    int cvcard, cvshift;
+    /* context-vector constants (orc_cv_constants) */
+    float cv_lokappa0, cv_pownu0, cv_cterm;
+} orc_params;
+
+typedef struct {
+    int len;
+    float eno;
+    const float* bkg;           /* [20] */
+    const float* trn;           /* [(len+1)*7]: row i = transitions into position i */
+    const float* trg;           /* [len*20] */
+    const float* cv;            /* [len*19] */
+    const float* cvprior;       /* [len] */
+    const float* cvnorm2;       /* [len] */
+    const float* ss;            /* [len*3] C,E,H */
+    const unsigned char* aa;    /* [len] */
+} orc_profile;
+
+/* btck codes of the reference (src/libmycu/cudp/CuBatchDP_com.h:99-104) */
+enum { ORC_STOP = 0, ORC_LEFT = 1, ORC_UP = 2, ORC_DIAG = 3 };
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,74 @@
+"""Host-side parameter parsing, smoothing and the C-ABI surface (CPU only)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from comer2_b200 import params as P
+from comer2_b200 import synth as S
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_default_tables(params):
+    assert params.ssss.shape == (30, 30)
+    assert np.array_equal(params.ssss, params.ssss.T)
+    assert params.cvs2s_card == 93 and params.cvs2s_shift == 5
+    assert np.all(np.diff(params.cvs2s_keys) > 0)
+    assert params.cvs2s_keys[params.cvs2s_shift] == 0.0
+    assert len(params.sse_nn_weights) == 93
+    assert (params.ssswgt, params.cvswgt, params.mapaln, params.eval) == (np.float32(0.12), np.float32(0.15), 1, 10.0)
+
+
+def test_cvs2s_smoothing_running_mean():
+    keys = [-1.0, -0.5, 0.0, 0.5, 1.0, 1.5, 2.0]
+    vals = [1.0, 2.0, 3.0, 4.0, 5.0, 6.0, P.CVS2S_PLUS]
+    k, v, shift = P.smooth_cvs2s(keys, vals)
+    assert shift == 2
+    # first full window (5 values) mean = 3, assigned to the first three entries
+    assert v[0] == v[1] == v[2] == np.float32(3.0)
+    # next window (2..6) mean = 4 for index 3; the '+' tail takes the last mean
+    assert v[3] == np.float32(4.0)
+    assert v[4] == v[5] == v[6] == np.float32(4.0)
+
+
+def test_cvs2s_inserts_missing_keys():
+    keys = [0.0, 0.5, 1.5, 2.0, 2.5, 3.0]
+    vals = [1.0, 1.0, 1.0, 1.0, 1.0, 1.0]
+    k, v, shift = P.smooth_cvs2s(keys, vals)
+    assert list(k) == [0.0, 0.5, 1.0, 1.5, 2.0, 2.5, 3.0]
+    assert np.all(v == np.float32(1.0))
+
+
+def test_parse_ssss_layout():
+    txt = "ssss= 0 +1\n0000 11\nCardinality = 3\n 1\n 2 3\n 4 5 6\n"
+    card, tri = P.parse_ssss(txt)
+    m = P.ssss_full(card, tri)
+    assert m.tolist() == [[1, 2, 4], [2, 3, 5], [4, 5, 6]]
+
+
+def test_synth_quantisation():
+    rng = np.random.default_rng(0)
+    ps = S.random_profiles(rng, [40, 30])
+    assert ps.trg_int.sum(1).tolist() == [10000] * 70
+    assert (ps.trg_int >= 1).all()
+    t = ps.trn_int
+    assert (t[:, 0:3].sum(1) == 10000).all() and (t[:, 3:5].sum(1) == 10000).all() and (t[:, 5:7].sum(1) == 10000).all()
+    # working values as the text reader computes them
+    assert np.allclose(ps.trn[:, :3], np.log(t[:, :3] / 10000.0), atol=1e-6)
+    assert np.allclose(ps.trn[:, 3:], 0.4 * np.log(t[:, 3:] / 10000.0), atol=1e-6)
+    assert ps.trn.shape[0] == ps.npositions + ps.nprofiles
+
+
+def test_library_exports_header_symbols():
+    """The built C-ABI library exports every function include/comer2_b200.h declares."""
+    from comer2_b200 import native
+    hdr = open(os.path.join(ROOT, "include", "comer2_b200.h")).read()
+    declared = sorted(set(re.findall(r"\b(c2_[a-z0-9_]+)\s*\(", hdr)))
+    assert declared, "no declarations found"
+    lib = ctypes.CDLL(native.LIB_PATH)
+    missing = [n for n in declared if not hasattr(lib, n)]
+    assert not missing, missing
+    assert sorted(native.EXPORTS) == declared
