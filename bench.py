@@ -1,0 +1,287 @@
+"""Benchmark of the COMER2 search hot path on B200.
+
+Workload: one query profile of length 400 against 100,000 database profiles
+(lengths lognormal, median 200, sigma 0.6, clipped to [30, 2000]; 2% planted
+homologs), seeded synthetic data (no public profile database is used).  One
+step = one complete search: fused score + Viterbi DP over all pairs, DP
+finalisation, statistics and E-values, MAP alignment of the hits.
+
+  value : GCUPS = L_q * sum(L_d) / step time, database and query resident in
+          HBM, timed with CUDA events on the launching stream;
+  e2e   : the same metric through the C ABI with host buffers: query upload,
+          the search, and the hits (records and alignments) back to the host.
+
+With --impl reference the line reports the CPU implementation of the same
+method (the C restatement, float, one thread per host core) on a bounded
+sample of the same workload; the reference has no CPU search path of its own.
+Multi-GPU runs (torchrun) give every rank its own database of the same size
+(weak scaling, no collective on the data path); times are the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GCUPS (score+DP+MAP)"
+UNIT = "GCUPS"
+WORKLOAD = "1 query L=400 vs 100000 db profiles LN(200,0.6)[30,2000], 2% planted homologs"
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic_per_position():
+    """DRAM bytes per db position of the phase-1 kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "p1_kernel_traffic.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            return float(json.load(fh)["dram_bytes_per_db_position"])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[3 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def _max_over_ranks(x, world, backend):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if backend == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_port_gcups(w, params, seconds=12.0, threads=None):
+    """The C restatement (float, one thread per host core) on a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle_py import Oracle
+    threads = threads or os.cpu_count()
+    orc = Oracle(params, 32)
+    q = orc.profile(w.queries[0])
+    Lq = int(w.queries[0].lengths[0])
+    rng = np.random.default_rng(123)
+    order = rng.permutation(w.db.nprofiles)
+    # calibrate on a small sample, then size the timed sample to ~`seconds`
+    cal = order[:200]
+    t0 = time.perf_counter()
+    orc.batch_phase1(q, w.db, cal, threads, 1e9)
+    dt = time.perf_counter() - t0
+    rate = Lq * float(w.db.lengths[cal].sum()) / max(dt, 1e-6)
+    want = rate * seconds
+    lens = w.db.lengths[order].astype(np.float64) * Lq
+    n = int(np.searchsorted(np.cumsum(lens), want)) + 1
+    ks = order[:max(1, min(n, w.db.nprofiles))]
+    cells = Lq * float(w.db.lengths[ks].sum())
+    t0 = time.perf_counter()
+    orc.batch_phase1(q, w.db, ks, threads, 0.0)
+    dt = time.perf_counter() - t0
+    return cells / dt / 1e9, threads, "%d of %d db profiles (%.3g cells), phase 1 + DP finalisation" % (
+        len(ks), w.db.nprofiles, cells)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="database size factor (1.0 = 100k profiles)")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    args = ap.parse_args()
+    world, rank, local = _dist()
+    from comer2_b200 import params as P, synth as S
+    prm = P.load_default()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        w = S.config(1, seed=0, scale=args.scale)
+        vals = []
+        thr = samp = None
+        for _ in range(max(1, args.steps)):
+            g, thr, samp = cpu_port_gcups(w, prm, seconds=args.cpu_seconds / max(1, args.steps))
+            vals.append(g)
+        v = float(np.median(vals))
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32",
+                "data": "synthetic", "config": {"workload": WORKLOAD, "scale": args.scale},
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": samp},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "note": "the reference has no CPU search path; this is the C restatement of its method"}
+        print(json.dumps(line))
+        return
+
+    import torch
+    backend = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl"
+        torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    from comer2_b200.native import Handle
+
+    w = S.config(1, seed=rank, scale=args.scale)
+    q = w.queries[0]
+    Lq = int(q.lengths[0])
+    cells = Lq * int(w.db.lengths.sum())
+    h = Handle(prm, local)
+    st = torch.cuda.Stream()
+    h.set_stream(st.cuda_stream)
+    t0 = time.perf_counter()
+    h.upload_db(w.db)
+    upload_s = time.perf_counter() - t0
+
+    def device_step():
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        with torch.cuda.stream(st):
+            e[0].record(st)
+            h.run_phase1()
+            e[1].record(st)
+            h.run_finalize()
+            h.run_stats()
+            nh = h.run_map()
+            e[2].record(st)
+        e[2].synchronize()
+        return e[0].elapsed_time(e[2]), e[0].elapsed_time(e[1]), nh
+
+    h.set_query(q)
+    for _ in range(args.warmup):
+        device_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    l0 = h.launch_count()
+    tot, p1, nh = [], [], 0
+    for _ in range(args.steps):
+        a, b, nh = device_step()
+        tot.append(a)
+        p1.append(b)
+    torch.cuda.synchronize()
+    launches = h.launch_count() - l0
+    if world > 1:
+        torch.distributed.barrier()
+    ms = _max_over_ranks(float(np.mean(tot)), world, backend)
+    p1ms = _max_over_ranks(float(np.mean(p1)), world, backend)
+    # e2e: host buffers through the C ABI (query upload + search + hits back)
+    e2e = []
+    hits = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hits = h.search(q)
+        torch.cuda.synchronize()
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    clocks = clk.stop()
+    e2e_ms = _max_over_ranks(float(np.mean(e2e)), world, backend)
+    nprof = w.db.nprofiles
+    h2d = Lq * (64 + 6) * 4 + (Lq + 1) * 7 * 4 + 2 * Lq + 20 * 4
+    d2h = nprof * 4 + sum(5 * (x["alnlen"] + 1) for x in hits) + len(hits) * 80
+    hbm_peak, peak_kind = _peaks()
+    npos = int(w.db.lengths.sum())
+    alg_bytes = 209.0 * npos                      # FP32 profile fields streamed per query pass
+    achieved = alg_bytes / (p1ms * 1e-3) / 1e9
+    tpp = _traffic_per_position()
+    line = {
+        "metric": METRIC, "value": world * cells / (ms * 1e-3) / 1e9, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cells_per_gpu": cells, "db_profiles": nprof, "db_positions": npos,
+                   "scale": args.scale, "l2": "inputs larger than L2 (db records %.1f GB)" % (npos * 224 / 1e9),
+                   "parallelism": "db replicas, one per GPU" if world > 1 else "single GPU"},
+        "e2e": {"value": world * cells / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "hits": len(hits), "homologs_found": int(sum(1 for x in hits if x["profile"] in set(w.homologs.tolist()))),
+        "stage_ms": {"phase1": p1ms, "finalize+stats+map": ms - p1ms},
+        "roofline": {"kernel": "p1_kernel (fused score + Viterbi DP)", "bound": "hbm",
+                     "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                     "peak_kind": peak_kind,
+                     "traffic": (tpp * npos) if tpp else None,
+                     "note": "algorithmic bytes = 209 B x db positions per query pass; the FP32 kernel is "
+                             "issue/latency bound, not HBM bound"},
+        "clocks": clocks,
+        "db_upload_s": upload_s,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            g, thr, samp = cpu_port_gcups(w, prm, seconds=args.cpu_seconds)
+            line["cpu_baseline"] = {"value": g, "unit": UNIT, "cores": thr, "kind": "port", "sample": samp}
+        except Exception as ex:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                    "sample": "failed: %s" % ex}
+    if rank == 0:
+        print(json.dumps(line))
+    h.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

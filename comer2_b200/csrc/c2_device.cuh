@@ -47,6 +47,10 @@ struct ScoreConsts {
 
 constexpr int P1_WARPS = 8;               // warps per CTA of the DP kernels
 constexpr int MAX_SSSS_CARD = 32;
+// db record staging ring of the phase-1 kernel: 2 chunks of 8 columns
+constexpr int REC_CHUNK = 8, REC_CHUNK_LOG = 3, REC_SLOTS = 16;
+// shared memory per warp: score ring [32][32], SS row table [32][32], record ring
+constexpr int P1_WARP_FLOATS = 32 * 32 + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE;
 constexpr int MAX_CVCARD = 256;
 
 struct P1Args {
@@ -71,6 +75,7 @@ struct P1Args {
     const long long* cand_off;  // byte offsets into btck / float offsets into smat
     signed char* btck;          // [L][Lq] per candidate (column-major)
     float* smat;                // [L][Lq] per candidate
+    float* mmat;                // [L][Lq] per candidate: modular scores
     int* status;                // device error word (0 = ok)
 };
 

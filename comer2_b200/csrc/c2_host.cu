@@ -17,8 +17,12 @@
 
 #include "../../include/comer2_b200.h"
 #include "c2_device.cuh"
+#include "c2_stats.cuh"
 
 namespace c2 {
+cudaError_t launch_stats(const StatsArgs& a, cudaStream_t st);
+cudaError_t launch_map(const MapArgs& a, const float* qtrn, const float* dtrn, const float* qcf, int grid,
+                       int* counter, cudaStream_t st, int* nlaunch);
 size_t p1_smem_bytes(int cvcard);
 cudaError_t launch_p1(const P1Args& a, const float* qbkg, bool tb, int grid, cudaStream_t st);
 int p1_blocks_per_sm(int cvcard);
@@ -68,14 +72,16 @@ struct c2_handle {
     int Lmax = 0;
     std::vector<int32_t> h_plen;
     std::vector<int64_t> h_poff;
-    DevBuf<float> d_drec, d_pbkg;
+    DevBuf<float> d_drec, d_pbkg, d_dtrn, d_peno;
     DevBuf<int> d_plen, d_order;
     DevBuf<long long> d_poff;
+    DevBuf<unsigned char> d_daa, d_dss;
     // query
     int Lq = 0;
     float qeno = 0.f;
     std::vector<float> h_qrec;
-    DevBuf<float> d_qrec, d_qbkg;
+    DevBuf<float> d_qrec, d_qbkg, d_qtrn, d_qcf;
+    DevBuf<unsigned char> d_qaa, d_qss;
     float scorethld = 0.f, logevthld = 0.f;
     unsigned long long searchspace = 0, deltalen = 0;
     // phase 1
@@ -91,10 +97,26 @@ struct c2_handle {
     DevBuf<int> d_cand_prof;
     DevBuf<long long> d_cand_off;
     DevBuf<signed char> d_btck;
-    DevBuf<float> d_smat;
+    DevBuf<float> d_smat, d_mmat;
     DevBuf<float> d_fscore;
     DevBuf<int> d_fpsts, d_fpassed;
     DevBuf<unsigned> d_fbeg, d_fend;
+    std::vector<float> h_fscore;
+    std::vector<int> h_fpassed;
+    // statistics
+    int npass = 0;
+    std::vector<int> h_p2;          // passed pair -> candidate index
+    DevBuf<int> d_p2;
+    DevBuf<float> d_stats;
+    std::vector<float> h_stats;
+    // MAP
+    int nmap = 0;
+    std::vector<int> h_mapcand, h_mappass;
+    DevBuf<int> d_mapcand, d_mappass, d_alninfo;
+    DevBuf<float> d_fb, d_pairf;
+    DevBuf<unsigned> d_pairc;
+    DevBuf<char> d_aln;
+    int alnstride = 0;
 };
 
 static c2_status fail(c2_handle* h, c2_status st, const char* fmt, ...)
@@ -137,6 +159,75 @@ static void cv_constants(float* lokappa0, float* pownu0, float* cterm)
 }
 
 static inline float hmax(float a, float b) { return a < b ? b : a; }
+
+// Schraudolph (1999) exponential and its inverse as the MAP kernels evaluate
+// them (fused multiply-add), for the host-side boundary states
+static inline float host_fexp(float x)
+{
+    if (!(-16.f < x)) return 0.f;
+    const int i = (int)fmaf(12102203.16f, x, 1064631197.0f);
+    float f;
+    memcpy(&f, &i, 4);
+    return f;
+}
+static inline float host_flog(float x)
+{
+    if (!(3.8e-11f < x)) return -99.f;
+    int i;
+    memcpy(&i, &x, 4);
+    return (float)(i - 1064631197) * 8.2629582959339e-08f;
+}
+static inline float host_lse2(float a, float b)
+{
+    const float mx = hmax(a, b);
+    return host_flog(host_fexp(a - mx) + host_fexp(b - mx)) + mx;
+}
+
+// Gertz (2005) length adjustment for the effective search space, float
+// arithmetic as AbstractScoreMatrix::ComputeLengthAdjustment
+// (src/libpro/srcsco/AbstractScoreMatrix.cpp:303-380)
+static void length_adjustment(float lambda, float K, float alpha, float beta, size_t m, uint64_t n, size_t N,
+                              unsigned long long* searchspace, unsigned long long* deltalen)
+{
+    *searchspace = (unsigned long long)m * n;
+    *deltalen = 0;
+    if (lambda <= 0.0f || K <= 0.0f || N < 1) return;
+    const int maxit = 20;
+    const float logK = logf(K);
+    const float alratio = alpha / lambda;
+    const float max_mn = (float)((m > n) ? m : n);
+    float length = 0.0f, min_length = 0.0f, max_length = 0.0f, nxt_length = 0.0f;
+    float sspace = 0.0f, space2 = 0.0f;
+    bool converged = false;
+    const float a = (float)N;
+    const float b = (float)(n + m * N);
+    const float c = (float)(m * n) - max_mn / K;
+    if (c < 0.0f) return;
+    max_length = 2.0f * c / (b + sqrtf(b * b - 4.0f * a * c));
+    for (int j = 0; j < maxit; j++) {
+        length = nxt_length;
+        sspace = (m - length) * (n - N * length);
+        nxt_length = alratio * (logK + logf(sspace)) + beta;
+        if (length <= nxt_length) {
+            min_length = length;
+            if (nxt_length - length <= 1.0f) { converged = true; break; }
+            if (min_length == max_length) break;
+        } else
+            max_length = length;
+        if (nxt_length < min_length || max_length < nxt_length)
+            nxt_length = (!j) ? max_length : (min_length + max_length) * 0.5f;
+    }
+    if (converged) {
+        length = ceilf(min_length);
+        if (length <= max_length) {
+            space2 = (m - length) * (n - N * length);
+            nxt_length = alratio * (logK + logf(space2)) + beta;
+            if (length <= nxt_length) { min_length = length; sspace = space2; }
+        }
+    }
+    *searchspace = (unsigned long long)sspace;
+    *deltalen = (unsigned long long)min_length;
+}
 
 // ---------------------------------------------------------------------------
 extern "C" c2_status c2_create(int device, const c2_params* p, c2_handle** out)
@@ -297,6 +388,16 @@ extern "C" c2_status c2_upload_db(c2_handle* h, const c2_profiles* d, uint64_t t
     CK(cudaMemcpy(h->d_plen.p, d->lengths, (size_t)P * 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->d_order.p, order.data(), (size_t)P * 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->d_poff.p, poff.data(), (size_t)P * 8, cudaMemcpyHostToDevice));
+    // raw transitions, residues, SS states and ENOs for the statistics and MAP stages
+    if (h->d_dtrn.ensure((size_t)(N + P) * 7) || h->d_daa.ensure((size_t)N) || h->d_dss.ensure((size_t)N) ||
+        h->d_peno.ensure((size_t)P))
+        return fail(h, C2_ERR_NOMEM, "device allocation of db side arrays failed");
+    CK(cudaMemcpy(h->d_dtrn.p, d->trn, (size_t)(N + P) * 7 * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_daa.p, d->aa, (size_t)N, cudaMemcpyHostToDevice));
+    if (d->ssstate) CK(cudaMemcpy(h->d_dss.p, d->ssstate, (size_t)N, cudaMemcpyHostToDevice));
+    else CK(cudaMemset(h->d_dss.p, ' ', (size_t)N));
+    if (d->eno) CK(cudaMemcpy(h->d_peno.p, d->eno, (size_t)P * 4, cudaMemcpyHostToDevice));
+    else CK(cudaMemset(h->d_peno.p, 0, (size_t)P * 4));
     // strip-boundary scratch: per warp slot, two rows of 5 states
     const int lm = (h->Lmax + 31) & ~31;
     h->botstride = 10LL * lm;
@@ -348,7 +449,39 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
         return fail(h, C2_ERR_NOMEM, "query allocation failed");
     CK(cudaMemcpyAsync(h->d_qrec.p, h->h_qrec.data(), h->h_qrec.size() * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_qbkg.p, q->bkg, NAA * 4, cudaMemcpyHostToDevice, h->stream));
+    // MAP forward: column -1 states of the query rows (log-sum-exp form of the
+    // Viterbi boundary; src/libmycu/cumapdp/CuBatchMAPDP_fwd.cu:72-478)
+    {
+        std::vector<float> qcf((size_t)Lq * 6, 0.f);
+        float pMI = 0.f, pIM = 0.f, pDN = 0.f;
+        for (int r = 0; r < Lq; r++) {
+            float t[7];
+            trn_of(q, 0, r, t);
+            const float L0 = -99.f;
+            float uMM = 0.f, uMI = L0, uDN = L0;
+            if (r % 32 != 0) { uMI = pMI; uDN = pDN; }
+            const float mi = host_lse2((uMM + t[TMM]) + L0, (uMI + t[TMM]) + L0);
+            float im;
+            if (r % 32 == 0) im = host_lse2((0.f + t[TMI]) + L0, (L0 + t[TII]) + L0);
+            else im = host_lse2((0.f + t[TMI]) + L0, ((((0.f + t[TMI]) + L0) + t[TII]) + L0));
+            const float dn = host_lse2(uMM + t[TMD], uDN + t[TDD]);
+            float* c = qcf.data() + (size_t)r * 6;
+            c[0] = mi; c[1] = im; c[2] = dn;
+            c[3] = pMI; c[4] = pIM; c[5] = pDN;
+            pMI = mi; pIM = im; pDN = dn;
+        }
+        if (h->d_qcf.ensure(qcf.size()) || h->d_qtrn.ensure((size_t)(Lq + 1) * 7) || h->d_qaa.ensure(Lq) ||
+            h->d_qss.ensure(Lq))
+            return fail(h, C2_ERR_NOMEM, "query side arrays allocation failed");
+        CK(cudaMemcpyAsync(h->d_qcf.p, qcf.data(), qcf.size() * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->d_qtrn.p, q->trn, (size_t)(Lq + 1) * 7 * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->d_qaa.p, q->aa, (size_t)Lq, cudaMemcpyHostToDevice, h->stream));
+        if (q->ssstate) CK(cudaMemcpyAsync(h->d_qss.p, q->ssstate, (size_t)Lq, cudaMemcpyHostToDevice, h->stream));
+        else CK(cudaMemsetAsync(h->d_qss.p, ' ', (size_t)Lq, h->stream));
+    }
     CK(cudaStreamSynchronize(h->stream));
+    length_adjustment(h->prm.gapped_lambda, h->prm.gapped_K, h->prm.gapped_alpha, h->prm.gapped_beta,
+                      (size_t)Lq, h->total_pos, (size_t)h->total_prof, &h->searchspace, &h->deltalen);
     // thresholds: JobDispatcher::CalculateScoreThreshold (JobDispatcher.cpp:809-860)
     {
         size_t sspace = (size_t)Lq * (size_t)h->total_pos;
@@ -461,7 +594,7 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     if (h->ncand == 0) return C2_OK;
     const int nc = h->ncand;
     if (h->d_cand_prof.ensure(nc) || h->d_cand_off.ensure(nc) || h->d_btck.ensure((size_t)acc) ||
-        h->d_smat.ensure((size_t)acc) || h->d_fscore.ensure(nc) || h->d_fpsts.ensure(nc) ||
+        h->d_smat.ensure((size_t)acc) || h->d_mmat.ensure((size_t)acc) || h->d_fscore.ensure(nc) || h->d_fpsts.ensure(nc) ||
         h->d_fpassed.ensure(nc) || h->d_fbeg.ensure(nc) || h->d_fend.ensure(nc))
         return fail(h, C2_ERR_NOMEM, "finalisation scratch for %d pairs (%lld cells) failed", nc, acc);
     CK(cudaMemcpyAsync(h->d_cand_prof.p, h->h_cand.data(), (size_t)nc * 4, cudaMemcpyHostToDevice, h->stream));
@@ -473,6 +606,7 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     a.cand_off = h->d_cand_off.p;
     a.btck = h->d_btck.p;
     a.smat = h->d_smat.p;
+    a.mmat = h->d_mmat.p;
     CK(cudaMemsetAsync(h->d_counter.p, 0, sizeof(int), h->stream));
     const int grid = std::min(h->grid, (nc + P1_WARPS - 1) / P1_WARPS);
     CK(launch_p1(a, h->d_qbkg.p, true, grid, h->stream));
@@ -530,5 +664,209 @@ extern "C" c2_status c2_launch_count(const c2_handle* h, uint64_t* n)
 {
     if (!h || !n) return C2_ERR_ARG;
     *n = h->launches;
+    return C2_OK;
+}
+
+extern "C" c2_status c2_get_search_space(const c2_handle* h, uint64_t* ss, uint64_t* dl)
+{
+    if (!h || !ss || !dl) return C2_ERR_ARG;
+    *ss = h->searchspace;
+    *dl = h->deltalen;
+    return C2_OK;
+}
+
+extern "C" c2_status c2_run_stats(c2_handle* h, int32_t* npassed)
+{
+    if (!h || !npassed) return C2_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    int stw = 0;
+    CK(cudaMemcpy(&stw, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (stw != 0) return fail(h, C2_ERR_DEVICE, "device status %d (traceback DP disagrees with phase 1)", stw);
+    const int nc = h->ncand;
+    h->h_p2.clear();
+    h->h_fscore.assign(nc, 0.f);
+    h->h_fpassed.assign(nc, 0);
+    if (nc > 0) {
+        CK(cudaMemcpy(h->h_fpassed.data(), h->d_fpassed.p, (size_t)nc * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(h->h_fscore.data(), h->d_fscore.p, (size_t)nc * 4, cudaMemcpyDeviceToHost));
+    }
+    for (int c = 0; c < nc; c++)
+        if (h->h_fpassed[c]) h->h_p2.push_back(c);
+    h->npass = (int)h->h_p2.size();
+    *npassed = h->npass;
+    if (h->npass == 0) return C2_OK;
+    if (h->d_p2.ensure(h->npass) || h->d_stats.ensure((size_t)h->npass * STATS_NOUT))
+        return fail(h, C2_ERR_NOMEM, "statistics buffers for %d pairs failed", h->npass);
+    CK(cudaMemcpyAsync(h->d_p2.p, h->h_p2.data(), (size_t)h->npass * 4, cudaMemcpyHostToDevice, h->stream));
+    StatsArgs a;
+    memset(&a, 0, sizeof a);
+    a.Lq = h->Lq;
+    a.npass = h->npass;
+    a.p2_cand = h->d_p2.p;
+    a.cand_prof = h->d_cand_prof.p;
+    a.cand_off = h->d_cand_off.p;
+    a.plen = h->d_plen.p;
+    a.poff = h->d_poff.p;
+    a.peno = h->d_peno.p;
+    a.qaa = h->d_qaa.p;
+    a.daa = h->d_daa.p;
+    a.smat = h->d_smat.p;
+    a.fscore = h->d_fscore.p;
+    a.fpsts = h->d_fpsts.p;
+    a.nnw = h->d_nnw.p;
+    a.ssemodel = h->prm.ssemodel;
+    a.xuninf = h->prm.x_uninf;
+    a.qeno = h->qeno;
+    a.searchspace = (float)h->searchspace;
+    a.reflambda = h->prm.ungapped_lambda;
+    a.refK = h->prm.ungapped_K;
+    a.expglambda = h->prm.gapped_lambda;
+    a.expgK = h->prm.gapped_K;
+    a.out = h->d_stats.p;
+    if (!a.nnw || h->nnw.size() < 93) return fail(h, C2_ERR_ARG, "SS18 model weights missing (93 values needed)");
+    CK(launch_stats(a, h->stream));
+    h->launches++;
+    return C2_OK;
+}
+
+extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
+{
+    if (!h || !nhits) return C2_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    h->h_stats.assign((size_t)h->npass * STATS_NOUT, 0.f);
+    if (h->npass > 0)
+        CK(cudaMemcpy(h->h_stats.data(), h->d_stats.p, h->h_stats.size() * 4, cudaMemcpyDeviceToHost));
+    h->h_mapcand.clear();
+    h->h_mappass.clear();
+    for (int i = 0; i < h->npass; i++)
+        if (!(h->logevthld < h->h_stats[(size_t)i * STATS_NOUT + ST_LOGE])) {  // MAP stage skips logE > threshold
+            h->h_mapcand.push_back(h->h_p2[i]);
+            h->h_mappass.push_back(i);
+        }
+    h->nmap = (int)h->h_mapcand.size();
+    *nhits = h->nmap;
+    if (h->nmap == 0) return C2_OK;
+    const int nm = h->nmap;
+    long long cells = 0;
+    for (int c : h->h_mapcand) cells += (long long)h->Lq * h->h_plen[h->h_cand[c]];
+    (void)cells;
+    h->alnstride = h->Lq + h->Lmax + 1;
+    size_t fbn = h->d_smat.n;   // same layout as the candidates' score matrices
+    if (h->d_mapcand.ensure(nm) || h->d_mappass.ensure(nm) || h->d_fb.ensure(fbn) || h->d_pairf.ensure((size_t)nm * 4) ||
+        h->d_pairc.ensure(nm) || h->d_alninfo.ensure((size_t)nm * 8) || h->d_aln.ensure((size_t)nm * 5 * h->alnstride))
+        return fail(h, C2_ERR_NOMEM, "MAP buffers for %d pairs failed", nm);
+    CK(cudaMemcpyAsync(h->d_mapcand.p, h->h_mapcand.data(), (size_t)nm * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_mappass.p, h->h_mappass.data(), (size_t)nm * 4, cudaMemcpyHostToDevice, h->stream));
+    MapArgs a;
+    memset(&a, 0, sizeof a);
+    a.Lq = h->Lq;
+    a.nmap = nm;
+    a.map_cand = h->d_mapcand.p;
+    a.map_pass = h->d_mappass.p;
+    a.cand_prof = h->d_cand_prof.p;
+    a.cand_off = h->d_cand_off.p;
+    a.plen = h->d_plen.p;
+    a.poff = h->d_poff.p;
+    a.smat = h->d_smat.p;
+    a.mmat = h->d_mmat.p;
+    a.stats = h->d_stats.p;
+    a.fb = h->d_fb.p;
+    a.btck = h->d_btck.p;
+    a.pairf = h->d_pairf.p;
+    a.pairc = h->d_pairc.p;
+    a.bot = h->d_bot.p;
+    a.botstride = h->botstride;
+    a.counter = h->d_counter.p;
+    a.minpp = h->prm.minpp;
+    a.modscores = (h->prm.ssswgt > 0.f || h->prm.cvswgt > 0.f) ? 1 : 0;
+    a.qaa = h->d_qaa.p;
+    a.qss = h->d_qss.p;
+    a.daa = h->d_daa.p;
+    a.dss = h->d_dss.p;
+    a.aln_info = h->d_alninfo.p;
+    a.aln = h->d_aln.p;
+    a.alnstride = h->alnstride;
+    int nl = 0;
+    // the MAP sweeps run 4 warps per CTA, one boundary slot each: stay within
+    // the grid x P1_WARPS slots of the strip-boundary scratch
+    const int grid = h->grid * P1_WARPS / 4;
+    CK(launch_map(a, h->d_qtrn.p, h->d_dtrn.p, h->d_qcf.p, grid, h->d_counter.p, h->stream, &nl));
+    h->launches += nl;
+    return C2_OK;
+}
+
+extern "C" c2_status c2_get_hits(c2_handle* h, c2_hit* hits, int32_t n, char* alns, size_t* aln_bytes)
+{
+    if (!h || !aln_bytes) return C2_ERR_ARG;
+    CK(cudaStreamSynchronize(h->stream));
+    const int nm = h->nmap;
+    const size_t per = (size_t)5 * h->alnstride;
+    std::vector<int> info((size_t)nm * 8);
+    if (nm > 0) CK(cudaMemcpy(info.data(), h->d_alninfo.p, info.size() * 4, cudaMemcpyDeviceToHost));
+    size_t need = 0;
+    for (int m = 0; m < nm; m++) need += (size_t)5 * (info[(size_t)m * 8] + 1);
+    if (!alns || !hits) {
+        *aln_bytes = need;
+        return (hits || alns) ? C2_ERR_ARG : C2_OK;
+    }
+    if (n < nm || *aln_bytes < need) return fail(h, C2_ERR_ARG, "output buffers too small (%d hits, %zu bytes)", nm, need);
+    std::vector<char> raw((size_t)nm * per);
+    if (nm > 0) CK(cudaMemcpy(raw.data(), h->d_aln.p, raw.size(), cudaMemcpyDeviceToHost));
+    std::vector<int> order(nm);
+    std::iota(order.begin(), order.end(), 0);
+    auto logE = [&](int m) { return h->h_stats[(size_t)h->h_mappass[m] * STATS_NOUT + ST_LOGE]; };
+    auto prof = [&](int m) { return h->h_cand[h->h_mapcand[m]]; };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const float ex = logE(x), ey = logE(y);
+        if (ex != ey) return ex < ey;
+        return prof(x) < prof(y);
+    });
+    size_t pos = 0;
+    for (int i = 0; i < nm; i++) {
+        const int m = order[i];
+        const float* st = &h->h_stats[(size_t)h->h_mappass[m] * STATS_NOUT];
+        const int* in = &info[(size_t)m * 8];
+        c2_hit& o = hits[i];
+        o.profile = prof(m);
+        o.score = h->h_fscore[h->h_mapcand[m]];
+        o.logE = st[ST_LOGE];
+        o.logEpA = st[ST_LOGEPA];
+        o.lambda = st[ST_LAMBDA];
+        o.K = st[ST_K];
+        o.lambda_est = st[ST_LAMBDA_EST];
+        o.K_est = st[ST_K_EST];
+        o.E = st[ST_E];
+        o.H = st[ST_H];
+        o.smin = (int32_t)st[ST_MIN];
+        o.smax = (int32_t)st[ST_MAX];
+        o.alnlen = in[0];
+        o.idts = in[1];
+        o.psts = in[2];
+        o.gaps = in[3];
+        o.beg = (uint32_t)in[4];
+        o.end = (uint32_t)in[5];
+        o.aln_offset = (int64_t)pos;
+        for (int r = 0; r < 5; r++) {
+            const char* src = raw.data() + (size_t)m * per + (size_t)r * h->alnstride;
+            memcpy(alns + pos, src, (size_t)in[0]);
+            alns[pos + in[0]] = 0;
+            pos += (size_t)in[0] + 1;
+        }
+    }
+    return C2_OK;
+}
+
+extern "C" c2_status c2_search(c2_handle* h, const c2_profiles* q, int32_t* nhits)
+{
+    if (!h || !q || !nhits) return C2_ERR_ARG;
+    c2_status st;
+    int32_t n = 0;
+    if ((st = c2_set_query(h, q)) != C2_OK) return st;
+    if ((st = c2_run_phase1(h)) != C2_OK) return st;
+    if ((st = c2_run_finalize(h, &n)) != C2_OK) return st;
+    if ((st = c2_run_stats(h, &n)) != C2_OK) return st;
+    if ((st = c2_run_map(h, nhits)) != C2_OK) return st;
     return C2_OK;
 }

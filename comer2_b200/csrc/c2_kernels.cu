@@ -53,36 +53,38 @@ struct RowOps {
 
 __device__ __forceinline__ float cell_score(const RowOps& R, const float4* __restrict__ rp,
                                             const float* __restrict__ U, const float* __restrict__ cvtab,
-                                            const ScoreConsts& sc, int lane, float& aa_out)
+                                            const ScoreConsts& sc, int lane, float& mod_out)
 {
     float4 v;
-    // aa term
-    float s = 0.f;
+    // aa term (two accumulators shorten the dependent FMA chain)
+    float s = 0.f, s2 = 0.f;
 #pragma unroll
     for (int i = 0; i < 5; i++) {
-        v = __ldg(rp + i);
+        v = rp[i];
         s = fmaf(R.Qt[4 * i + 0], v.x, s);
-        s = fmaf(R.Qt[4 * i + 1], v.y, s);
+        s2 = fmaf(R.Qt[4 * i + 1], v.y, s2);
         s = fmaf(R.Qt[4 * i + 2], v.z, s);
-        s = fmaf(R.Qt[4 * i + 3], v.w, s);
+        s2 = fmaf(R.Qt[4 * i + 3], v.w, s2);
     }
+    s += s2;
     const float s0 = __logf(s) - sc.shift;
     // CV term: dot product over [20,39), then (cq)(cd) - (dot+1/kappa0)^2
-    float dot = 0.f;
+    float dot = 0.f, dot2 = 0.f;
 #pragma unroll
     for (int i = 5; i < 10; i++) {
-        v = __ldg(rp + i);
+        v = rp[i];
         const int b = 4 * i - DR_CV;
         dot = fmaf(R.qcv[b + 0], v.x, dot);
-        dot = fmaf(R.qcv[b + 1], v.y, dot);
+        dot2 = fmaf(R.qcv[b + 1], v.y, dot2);
         dot = fmaf(R.qcv[b + 2], v.z, dot);
-        if (b + 3 < NCV) dot = fmaf(R.qcv[b + 3], v.w, dot);
+        if (b + 3 < NCV) dot2 = fmaf(R.qcv[b + 3], v.w, dot2);
     }
+    dot += dot2;
     const float cd = v.w;  // DR_CN = 39
-    v = __ldg(rp + 10);    // 40 prior, 41..43 ss
+    v = rp[10];            // 40 prior, 41..43 ss
     const float pd = v.x;
     const float ds0 = v.y, ds1 = v.z, ds2 = v.w;
-    const float4 v11 = __ldg(rp + 11);  // 44 ss idx, 45 hd
+    const float4 v11 = rp[11];  // 44 ss idx, 45 hd
     dot += sc.lokappa0;
     float det = R.cq * cd - dot * dot;
     float cvs = sc.cterm + sc.pownu0 * __logf(det) - R.pq - pd;
@@ -105,11 +107,39 @@ __device__ __forceinline__ float cell_score(const RowOps& R, const float4* __res
         ss -= 0.05f;
         ss *= sc.ssswgt;
     }
-    aa_out = s0;
-    return s0 + (ss + cvm);
+    const float add = ss + cvm;
+    mod_out = add - 0.5f * sc.cvswgt;   // modular score of the MAP stage
+    return s0 + add;
 }
 
 struct St5 { float MM, MI, IM, DN, ND; };
+
+// asynchronous global->shared copies (cp.async, 16 B each)
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Stage the records of columns [REC_CHUNK*m, REC_CHUNK*(m+1)) (clipped to L)
+// into ring slots; records of consecutive columns are contiguous in HBM, so a
+// chunk is one contiguous range copied by all lanes in 16-byte pieces.  Every
+// call commits one group (possibly empty) so that wait_group counts stay aligned.
+__device__ __forceinline__ void stage_chunk(float* rec, const float* __restrict__ dr, int m, int L, int lane)
+{
+    const int c0 = m * REC_CHUNK;
+    const int nc = min(REC_CHUNK, L - c0);
+    if (nc > 0) {
+        const int n16 = nc * (DR_STRIDE / 4);
+        float* dst = rec + (c0 & (REC_SLOTS - 1)) * DR_STRIDE;
+        const float* src = dr + (long long)c0 * DR_STRIDE;
+        for (int i = lane; i < n16; i += 32) cp_async16(dst + 4 * i, src + 4 * i);
+    }
+    cp_async_commit();
+}
 
 template <bool TB>
 __global__ void __launch_bounds__(P1_WARPS * 32, 2)
@@ -120,9 +150,10 @@ p1_kernel(P1Args a, const float* __restrict__ qbkg)
     const int cvcard = a.sc.cvcard;
     const int card = a.sc.ssss_card;
     float* cvtab = smem;                                      // [cvcard][32]
-    float* wb = smem + cvcard * 32 + wid * (32 * 32 + MAX_SSSS_CARD * 32);
+    float* wb = smem + cvcard * 32 + wid * P1_WARP_FLOATS;
     float* ring = wb;                                         // [32][32]
     float* U = wb + 32 * 32;                                  // [card][32]
+    float* rec = U + MAX_SSSS_CARD * 32;                      // [REC_SLOTS][DR_STRIDE] db records
     for (int i = threadIdx.x; i < cvcard * 32; i += blockDim.x) cvtab[i] = a.cvvals[i >> 5];
     __syncthreads();
 
@@ -205,19 +236,34 @@ p1_kernel(P1Args a, const float* __restrict__ qbkg)
             }
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             const int nsteps = L + 31;
+            // db column records are staged into shared memory one chunk ahead
+            stage_chunk(rec, dr, 0, L, lane);
+            stage_chunk(rec, dr, 1, L, lane);
             for (int k = 0; k < nsteps; k++) {
+                if ((k & (REC_CHUNK - 1)) == 0 && k < L) {
+                    cp_async_wait_1();
+                    __syncwarp();
+                }
                 // ---- score stage: column k for every lane's row
                 float tc[7];
                 if (k < L) {
-                    const float4* rp = reinterpret_cast<const float4*>(dr + (long long)k * DR_STRIDE);
-                    float aa;
-                    float S = cell_score(R, rp, U, cvtab, sc, lane, aa);
+                    const float4* rp = reinterpret_cast<const float4*>(rec + (k & (REC_SLOTS - 1)) * DR_STRIDE);
+                    float mod;
+                    float S = cell_score(R, rp, U, cvtab, sc, lane, mod);
                     if (!act) S = -9.f;
                     ring[(k & 31) * 32 + lane] = S;
-                    if (TB && act) smt[(long long)k * Lq + r] = S;
-                    const float4 ta = __ldg(rp + 12), tb = __ldg(rp + 13);
+                    if (TB && act) {
+                        smt[(long long)k * Lq + r] = S;
+                        a.mmat[a.cand_off[item] + (long long)k * Lq + r] = mod;
+                    }
+                    const float4 ta = rp[12], tb = rp[13];
                     tc[0] = ta.x; tc[1] = ta.y; tc[2] = ta.z; tc[3] = ta.w;
                     tc[4] = tb.x; tc[5] = tb.y; tc[6] = tb.z;
+                    if ((k & (REC_CHUNK - 1)) == REC_CHUNK - 1) {
+                        // chunk fully read by every lane: refill its slots two chunks ahead
+                        __syncwarp();
+                        stage_chunk(rec, dr, (k >> REC_CHUNK_LOG) + 2, L, lane);
+                    }
                 } else {
 #pragma unroll
                     for (int i = 0; i < 7; i++) tc[i] = LOG0;
@@ -293,6 +339,7 @@ p1_kernel(P1Args a, const float* __restrict__ qbkg)
                 mine = nw;
                 upp = up;
             }
+            cp_async_wait_all();
             float* t = botr; botr = botw; botw = t;
             __syncwarp();
         }
@@ -400,7 +447,7 @@ __global__ void __launch_bounds__(256) fin_kernel(FinArgs a)
 // launchers (host)
 size_t p1_smem_bytes(int cvcard)
 {
-    return (size_t)(cvcard * 32 + P1_WARPS * (32 * 32 + MAX_SSSS_CARD * 32)) * sizeof(float);
+    return (size_t)(cvcard * 32 + P1_WARPS * P1_WARP_FLOATS) * sizeof(float);
 }
 
 cudaError_t launch_p1(const P1Args& a, const float* qbkg, bool tb, int grid, cudaStream_t st)

@@ -25,7 +25,7 @@ STATUS_NAMES = {0: "C2_OK", 1: "C2_ERR_ARG", 2: "C2_ERR_CUDA", 3: "C2_ERR_NOMEM"
 EXPORTS = [
     "c2_create", "c2_destroy", "c2_last_error", "c2_upload_db", "c2_set_query", "c2_run_phase1",
     "c2_get_phase1", "c2_run_finalize", "c2_get_finalize", "c2_get_thresholds", "c2_set_stream", "c2_sync",
-    "c2_launch_count",
+    "c2_launch_count", "c2_run_stats", "c2_run_map", "c2_get_hits", "c2_search", "c2_get_search_space",
 ]
 
 _fp = C.POINTER(C.c_float)
@@ -65,6 +65,14 @@ class c2_dp_result(C.Structure):
                 ("beg", C.c_uint32), ("end", C.c_uint32), ("passed", C.c_int32)]
 
 
+class c2_hit(C.Structure):
+    _fields_ = [("profile", C.c_int32), ("score", C.c_float), ("logE", C.c_float), ("logEpA", C.c_float),
+                ("lambda_", C.c_float), ("K", C.c_float), ("lambda_est", C.c_float), ("K_est", C.c_float),
+                ("E", C.c_float), ("H", C.c_float), ("smin", C.c_int32), ("smax", C.c_int32),
+                ("psts", C.c_int32), ("idts", C.c_int32), ("gaps", C.c_int32), ("alnlen", C.c_int32),
+                ("beg", C.c_uint32), ("end", C.c_uint32), ("aln_offset", C.c_int64)]
+
+
 _lib: Optional[C.CDLL] = None
 
 
@@ -90,6 +98,11 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.c2_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     lib.c2_sync.argtypes = [C.c_void_p]
     lib.c2_launch_count.argtypes = [C.c_void_p, P(C.c_uint64)]
+    lib.c2_run_stats.argtypes = [C.c_void_p, P(C.c_int32)]
+    lib.c2_run_map.argtypes = [C.c_void_p, P(C.c_int32)]
+    lib.c2_get_hits.argtypes = [C.c_void_p, P(c2_hit), C.c_int32, C.c_char_p, P(C.c_size_t)]
+    lib.c2_search.argtypes = [C.c_void_p, P(c2_profiles), P(C.c_int32)]
+    lib.c2_get_search_space.argtypes = [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]
     for n in EXPORTS:
         getattr(lib, n).restype = C.c_int
     _lib = lib
@@ -241,6 +254,47 @@ class Handle:
         dt = np.dtype([("score", np.float32), ("profile", np.int32), ("psts", np.int32),
                        ("beg", np.uint32), ("end", np.uint32), ("passed", np.int32)])
         return np.frombuffer(out, dtype=dt, count=n).copy()
+
+    def run_stats(self) -> int:
+        n = C.c_int32()
+        self._ck(self.lib.c2_run_stats(self._h, C.byref(n)), "c2_run_stats")
+        return n.value
+
+    def run_map(self) -> int:
+        n = C.c_int32()
+        self._ck(self.lib.c2_run_map(self._h, C.byref(n)), "c2_run_map")
+        return n.value
+
+    def search_space(self):
+        a, b = C.c_uint64(), C.c_uint64()
+        self._ck(self.lib.c2_get_search_space(self._h, C.byref(a), C.byref(b)), "c2_get_search_space")
+        return a.value, b.value
+
+    def hits(self, n: int):
+        """The current hits as a list of dicts (sorted by log E-value), with alignment strings."""
+        sz = C.c_size_t(0)
+        self._ck(self.lib.c2_get_hits(self._h, None, 0, None, C.byref(sz)), "c2_get_hits(size)")
+        arr = (c2_hit * max(n, 1))()
+        buf = C.create_string_buffer(max(sz.value, 1))
+        self._ck(self.lib.c2_get_hits(self._h, arr, n, buf, C.byref(sz)), "c2_get_hits")
+        raw = buf.raw
+        out = []
+        for i in range(n):
+            h = arr[i]
+            d = {k: getattr(h, k) for k, _ in c2_hit._fields_}
+            o = d.pop("aln_offset")
+            L = d["alnlen"]
+            d["strings"] = [raw[o + r * (L + 1):o + r * (L + 1) + L].decode() for r in range(5)]
+            out.append(d)
+        return out
+
+    def search(self, q: ProfileSet):
+        """Complete search of query q over the uploaded database; returns the hits."""
+        k = _Keep()
+        s = make_profiles(q, k)
+        n = C.c_int32()
+        self._ck(self.lib.c2_search(self._h, C.byref(s), C.byref(n)), "c2_search")
+        return self.hits(n.value)
 
     def launch_count(self) -> int:
         n = C.c_uint64()

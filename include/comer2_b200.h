@@ -99,6 +99,30 @@ typedef struct {
     int32_t passed;      /* score > threshold */
 } c2_dp_result;
 
+/* One reported hit: a db profile whose log E-value is within the threshold,
+ * with its statistics and MAP alignment.  The fields are those of the
+ * reference's TDP2OutputAlnData record (src/libmycu/cuss/CuBatchSS_com.h:45-78)
+ * after FinalizeMAPDP_MAP, which replaces psts, beg and end with the MAP
+ * alignment's values (src/libmycu/cumapdp/CuBatchMAPDP_map_final.cu:318-330). */
+typedef struct {
+    int32_t profile;     /* db profile index */
+    float score;         /* DP score */
+    float logE;          /* log E-value (SS18 model) */
+    float logEpA;        /* log E-value of the pair alone */
+    float lambda, K;     /* computed ungapped lambda and K of the pair's scores */
+    float lambda_est, K_est;  /* derived gapped lambda and K */
+    float E, H;          /* expected score and relative entropy */
+    int32_t smin, smax;  /* score range */
+    int32_t psts;        /* positive, non-identical aligned pairs of the MAP alignment */
+    int32_t idts;        /* identities */
+    int32_t gaps;        /* gap positions */
+    int32_t alnlen;      /* alignment length */
+    uint32_t beg;        /* (x << 16) | y, 1-based beginning */
+    uint32_t end;        /* (x << 16) | y, 0-based end */
+    int64_t aln_offset;  /* offset of the 5 NUL-terminated strings (query, middle,
+                            target, query SS, target SS) in the alignment buffer */
+} c2_hit;
+
 typedef struct c2_handle c2_handle;
 
 /* Create a handle on a device; replaces CuBatchProcessing's constructor and
@@ -142,6 +166,32 @@ c2_status c2_run_finalize(c2_handle* h, int32_t* ncand);
 
 /* Copy finalisation records (in ascending profile order). */
 c2_status c2_get_finalize(c2_handle* h, c2_dp_result* out, int32_t n);
+
+/* Compute the statistics and E-values of the finalised pairs whose score
+ * exceeds the threshold; replaces CuBatchSS::CalculateAlnStatisticsDevice
+ * (src/libmycu/cuss/CuBatchSS.cu:196-265).  *npassed receives their number. */
+c2_status c2_run_stats(c2_handle* h, int32_t* npassed);
+
+/* MAP-align the pairs whose log E-value is within the threshold; replaces
+ * CuBatchMAPDP::PerformCompleteMAPDynProgDevice (CuBatchMAPDP.cu:150-513).
+ * *nhits receives the number of hits. */
+c2_status c2_run_map(c2_handle* h, int32_t* nhits);
+
+/* Copy the hits, sorted by log E-value (then profile index), and their
+ * alignment strings.  alns may be NULL to query the required size, which is
+ * returned in *aln_bytes; n must be at least the number of hits. */
+c2_status c2_get_hits(c2_handle* h, c2_hit* hits, int32_t n, char* alns, size_t* aln_bytes);
+
+/* One complete search of a query over the uploaded database: set the query,
+ * phase 1, finalisation, statistics and MAP alignment; replaces
+ * CuBatchProcessing::ProcessScoreMatrix (CuBatchProcessing.cuh:87-99).
+ * *nhits receives the number of hits; copy them with c2_get_hits. */
+c2_status c2_search(c2_handle* h, const c2_profiles* query, int32_t* nhits);
+
+/* Effective search space and length adjustment used for the current query
+ * (AbstractScoreMatrix::ComputeLengthAdjustment,
+ * src/libpro/srcsco/AbstractScoreMatrix.cpp:247-380). */
+c2_status c2_get_search_space(const c2_handle* h, uint64_t* searchspace, uint64_t* deltalen);
 
 /* Thresholds computed for the current query. */
 c2_status c2_get_thresholds(const c2_handle* h, float* scorethld, float* logevthld);

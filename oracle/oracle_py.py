@@ -39,6 +39,27 @@ class orc_profile(C.Structure):
                 ("cv", _fp), ("cvprior", _fp), ("cvnorm2", _fp), ("ss", _fp), ("aa", _u8p)]
 
 
+class orc_stats_in(C.Structure):
+    _fields_ = [("ssemodel", C.c_int), ("nq", C.c_int), ("nd", C.c_int), ("qeno", C.c_float),
+                ("deno", C.c_float), ("searchspace", C.c_float), ("reflambda", C.c_float),
+                ("refK", C.c_float), ("expglambda", C.c_float), ("expgK", C.c_float),
+                ("nnw", _fp), ("score", C.c_float), ("psts", C.c_float)]
+
+
+def _stats_out(rt):
+    class orc_stats_out(C.Structure):
+        _fields_ = [(n, rt) for n in ("min", "max", "E", "H", "lambda_", "K", "lambda_est", "K_est",
+                                      "logE", "logEpA", "mu", "scale")]
+    return orc_stats_out
+
+
+def _map_out(rt):
+    class orc_map_out(C.Structure):
+        _fields_ = [("logZ", rt), ("maxF", rt), ("mapmax", rt)] + [
+            (n, C.c_int) for n in ("endx", "endy", "begx", "begy", "alnlen", "idts", "psts", "gaps")]
+    return orc_map_out
+
+
 class Oracle:
     """One oracle variant: bits=32 (float) or bits=64 (double)."""
 
@@ -65,6 +86,18 @@ class Oracle:
         L.orc_length_adjustment.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, C.c_size_t,
                                             C.c_ulonglong, C.c_size_t, C.POINTER(C.c_ulonglong),
                                             C.POINTER(C.c_ulonglong)]
+        self.StatsOut = _stats_out(self.crt)
+        self.MapOut = _map_out(self.crt)
+        L.orc_stats.argtypes = [C.POINTER(orc_stats_in), rp, _u8p, _u8p, C.c_int, C.POINTER(self.StatsOut)]
+        L.orc_map.argtypes = [C.POINTER(orc_profile), C.POINTER(orc_profile), rp, rp, self.crt, self.crt,
+                              C.c_int, _u8p, _u8p, rp, C.c_char_p, C.POINTER(self.MapOut)]
+        L.orc_set_map_exact.argtypes = [C.c_int]
+        L.orc_lbetainc.argtypes = [self.crt] * 3
+        L.orc_lbetainc.restype = self.crt
+        L.orc_lgammainc_Q.argtypes = [self.crt] * 2
+        L.orc_lgammainc_Q.restype = self.crt
+        L.orc_batch_phase1.argtypes = [C.POINTER(orc_params), C.POINTER(orc_profile), C.POINTER(orc_profile),
+                                       C.c_int, C.c_int, self.crt, rp, rp]
         self._keep = []
         self.params = params
         self.P = self._make_params(params)
@@ -151,6 +184,68 @@ class Oracle:
             sc, ps, bx, by = self.finalize(S, bt, best, x, y)
             out.update(score=sc, psts=ps, begx=bx, begy=by)
         return out
+
+    def stats(self, S, qaa, daa, score, psts, qeno, deno, searchspace, xuninf=1):
+        """Statistics of one passed pair; S is the pair's [nq, nd] score matrix."""
+        p = self.params
+        S = np.ascontiguousarray(S, self.rt)
+        nq, nd = S.shape
+        si = orc_stats_in(int(p.ssemodel), nq, nd, float(qeno), float(deno), float(searchspace),
+                          float(p.ungapped_lambda), float(p.ungapped_K), float(p.gapped_lambda),
+                          float(p.gapped_K), self._f32(p.sse_nn_weights), float(score), float(psts))
+        qa = np.ascontiguousarray(qaa, np.uint8)
+        da = np.ascontiguousarray(daa, np.uint8)
+        o = self.StatsOut()
+        self.lib.orc_stats(C.byref(si), S.ctypes.data_as(C.POINTER(self.crt)), qa.ctypes.data_as(_u8p),
+                           da.ctypes.data_as(_u8p), xuninf, C.byref(o))
+        return {k: getattr(o, k) for k, _ in o._fields_}
+
+    def map(self, q, d, S, MOD, logepa, qss=None, dss=None, exact=False, with_post=False):
+        """MAP alignment of one pair: dict with logZ, coordinates, counts and strings."""
+        p = self.params
+        S = np.ascontiguousarray(S, self.rt)
+        MOD = np.ascontiguousarray(MOD, self.rt)
+        nq, nd = S.shape
+        post = np.zeros((nq, nd), self.rt) if with_post else None
+        cap = nq + nd + 1
+        aln = C.create_string_buffer(5 * cap)
+        keep = []
+
+        def u8(a):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, np.uint8)
+            keep.append(a)
+            return a.ctypes.data_as(_u8p)
+
+        self.lib.orc_set_map_exact(1 if exact else 0)
+        o = self.MapOut()
+        rp = C.POINTER(self.crt)
+        self.lib.orc_map(C.byref(q), C.byref(d), S.ctypes.data_as(rp), MOD.ctypes.data_as(rp), logepa,
+                         float(p.minpp), 1, u8(qss), u8(dss), post.ctypes.data_as(rp) if with_post else None,
+                         aln, C.byref(o))
+        self.lib.orc_set_map_exact(0)
+        out = {k: getattr(o, k) for k, _ in o._fields_}
+        raw = aln.raw
+        out["strings"] = [raw[r * cap:r * cap + out["alnlen"]].decode() for r in range(5)]
+        if with_post:
+            out["post"] = post
+        return out
+
+    def batch_phase1(self, q, db, ks, nthreads, thld):
+        """Phase 1 + finalisation of query q against db profiles ks on nthreads host threads."""
+        profs = (orc_profile * len(ks))()
+        keep = []
+        for i, k in enumerate(ks):
+            pr = self.profile(db, int(k))
+            keep.append(pr)
+            profs[i] = pr
+        best = np.zeros(len(ks), self.rt)
+        score = np.zeros(len(ks), self.rt)
+        rp = C.POINTER(self.crt)
+        self.lib.orc_batch_phase1(C.byref(self.P), C.byref(q), profs, len(ks), int(nthreads), thld,
+                                  best.ctypes.data_as(rp), score.ctypes.data_as(rp))
+        return best, score
 
     def score_threshold(self, nq, dbsize, eval_, gK, glambda):
         a, b = C.c_float(), C.c_float()

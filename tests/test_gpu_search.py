@@ -1,0 +1,115 @@
+"""GPU parity of the complete search (phase 1, finalisation, statistics, MAP)
+against the CPU oracle, through the C ABI.
+
+Tolerances: DP scores 1e-4 relative, log E-values 1e-3 absolute, hit lists
+identical, MAP alignment strings identical.  A context-vector score near a
+map-bin edge can round differently on the two sides (one cell moves by one
+table step, ~0.01); pairs affected that way are counted and must be rare.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from comer2_b200 import synth as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_search(orc, prm, w, searchspace, thld, logevthld):
+    """The oracle's hit list: {profile: record}."""
+    q = w.queries[0]
+    qo = orc.profile(q)
+    out = {}
+    for k in range(w.db.nprofiles):
+        do = orc.profile(w.db, k)
+        r = orc.pair(qo, do)
+        if not (r["best"] > thld) or not (r["score"] > thld):
+            continue
+        off, nd = int(w.db.offsets[k]), int(w.db.lengths[k])
+        st = orc.stats(r["S"], q.aa, w.db.aa[off:off + nd], r["score"], r["psts"], q.eno[0], w.db.eno[k],
+                       float(searchspace), prm.x_uninf)
+        rec = {"score": r["score"], "stats": st}
+        if not (logevthld < st["logE"]):
+            m = orc.map(qo, do, r["S"], r["MOD"], st["logEpA"], qss=q.ssstate, dss=w.db.ssstate[off:off + nd])
+            rec["map"] = m
+        out[k] = rec
+    return out
+
+
+def _run(params, w):
+    from comer2_b200.native import Handle
+    h = Handle(params, 0)
+    h.upload_db(w.db)
+    hits = h.search(w.queries[0])
+    thld, logevthld = h.thresholds()
+    ss, _ = h.search_space()
+    return h, hits, thld, logevthld, ss
+
+
+@pytest.mark.parametrize("seed", [2, 9])
+def test_search_matches_oracle(params, orc32, seed):
+    w = S.config(1, seed=seed, scale=0.003)   # 300 profiles, 6 planted homologs
+    h, hits, thld, logevthld, ss = _run(params, w)
+    ref = _oracle_search(orc32, params, w, ss, thld, logevthld)
+    ref_hits = sorted(k for k, v in ref.items() if "map" in v)
+    got = sorted(int(x["profile"]) for x in hits)
+    assert got == ref_hits
+    # hits are sorted by log E-value
+    le = [x["logE"] for x in hits]
+    assert le == sorted(le)
+    flips = 0
+    for x in hits:
+        k = int(x["profile"])
+        r = ref[k]
+        st, m = r["stats"], r["map"]
+        dscore = abs(x["score"] - r["score"])
+        if dscore > 1e-4 * max(1.0, abs(r["score"])):
+            flips += 1
+            assert dscore < 0.1
+            continue
+        assert x["logE"] == pytest.approx(st["logE"], abs=1e-3), k
+        assert x["logEpA"] == pytest.approx(st["logEpA"], abs=1e-3), k
+        assert x["lambda_"] == pytest.approx(st["lambda_"], rel=1e-3, abs=1e-5), k
+        assert x["K"] == pytest.approx(st["K"], rel=1e-3, abs=1e-6), k
+        assert (x["smin"], x["smax"]) == (st["min"], st["max"])
+        assert x["strings"][:3] == m["strings"][:3], k
+        assert x["strings"][3:] == m["strings"][3:], k
+        assert (x["alnlen"], x["idts"], x["psts"], x["gaps"]) == (m["alnlen"], m["idts"], m["psts"], m["gaps"])
+        assert (x["beg"] >> 16, x["beg"] & 0xFFFF) == (m["begx"], m["begy"])
+        assert (x["end"] >> 16, x["end"] & 0xFFFF) == (m["endx"], m["endy"])
+    assert flips <= max(1, len(hits) // 20)
+    # every planted homolog is found with a small E-value
+    for k in w.homologs:
+        assert k in got
+    h.close()
+
+
+def test_search_space_matches_oracle(params, orc32):
+    w = S.config(0, seed=4, scale=0.05)
+    from comer2_b200.native import Handle
+    h = Handle(params, 0)
+    h.upload_db(w.db, total_positions=5_000_000, total_profiles=20_000)
+    h.set_query(w.queries[0])
+    ss, dl = h.search_space()
+    ref = orc32.length_adjustment(params.gapped_lambda, params.gapped_K, params.gapped_alpha,
+                                  params.gapped_beta, int(w.queries[0].lengths[0]), 5_000_000, 20_000)
+    assert (ss, dl) == ref
+    thld, le = h.thresholds()
+    rt, rl = orc32.score_threshold(int(w.queries[0].lengths[0]), 5_000_000, params.eval, params.gapped_K,
+                                   params.gapped_lambda)
+    assert thld == rt and le == rl
+    h.close()
+
+
+def test_no_hits_db(params):
+    """A database of unrelated short profiles: the search completes with few or no hits."""
+    rng = np.random.default_rng(77)
+    q = S.random_profiles(rng, [60])
+    db = S.random_profiles(rng, [40] * 30)
+    from comer2_b200.native import Handle
+    h = Handle(params, 0)
+    h.upload_db(db, total_positions=10_000_000, total_profiles=50_000)
+    hits = h.search(q)
+    assert len(hits) == 0
+    h.close()
