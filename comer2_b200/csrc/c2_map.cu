@@ -308,6 +308,10 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
             }
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             for (int k = 0; k < L + 31; k++) {
+                const int j = k - lane;         // mirrored column
+                // diagonal-successor score of column j, read before this step's
+                // write can reuse its ring slot (lane 31 reads slot (k+1)&31 = k&31)
+                const float sco = (j >= 1 && j < L) ? rin[(j - 1) & 31][lane] : MLOG0;
                 float tc[7];
                 if (k < L) {
                     const int ca = L - 1 - k;   // actual column of mirrored column k
@@ -345,10 +349,8 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
                     }
                 }
                 __syncwarp();
-                const int j = k - lane;         // mirrored column
                 S5 rt = mine, dg = upp;         // successor to the right, diagonal successor
                 if (j == 0) { rt = INIT; dg = INIT; }
-                const float sco = (j >= 1 && j < L) ? rin[(j - 1) & 31][lane] : MLOG0;
                 S5 nw;
                 nw.MM = lse5p1((dn.MI + q7[TMM]) + t7[TMI], (rt.IM + q7[TMI]) + t7[TMM], dn.DN + q7[TMD],
                                rt.ND + t7[TMD], ((dg.MM + q7[TMM]) + t7[TMM]) + sco);
