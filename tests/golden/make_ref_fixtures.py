@@ -71,9 +71,13 @@ def run(outroot):
         d = os.path.join(INP, case)
         out = os.path.join(outroot, case)
         os.makedirs(out, exist_ok=True)
+        # --dev-mem bounds the reference's device heap (its default takes all
+        # memory, which leaves none for loading its kernels' module)
+        env = dict(os.environ, CUDA_MODULE_LOADING="EAGER")
         r = subprocess.run(["timeout", "300", os.path.join(REF, "comer"), "-i", os.path.join(d, "q.pro"), "-d",
-                            os.path.join(d, "db"), "-o", out, "-p", opts, "-f", "1", "--dev-N=1"],
-                           capture_output=True, text=True)
+                            os.path.join(d, "db"), "-o", out, "-p", opts, "-f", "1", "--dev-N=1",
+                            "--dev-mem=16000"],
+                           capture_output=True, text=True, env=env)
         with open(os.path.join(out, "comer.log"), "w") as fh:
             fh.write(r.stdout + "\n---stderr---\n" + r.stderr + "\nrc=%d\n" % r.returncode)
         print(case, "rc", r.returncode)
