@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -868,5 +869,73 @@ extern "C" c2_status c2_search(c2_handle* h, const c2_profiles* q, int32_t* nhit
     if ((st = c2_run_finalize(h, &n)) != C2_OK) return st;
     if ((st = c2_run_stats(h, &n)) != C2_OK) return st;
     if ((st = c2_run_map(h, nhits)) != C2_OK) return st;
+    return C2_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Phase 1 with no allocation (no counterpart in the reference).  The same
+// p1_kernel, launched with its per-call scratch -- the work-queue counter and
+// the per-warp strip-boundary rows -- taken from a fixed file-scope device
+// array instead of handle buffers, and its results written to caller-owned
+// device memory.  For hosts that must not allocate at call time (cudaMalloc
+// and cudaFree synchronise the device and can fail under memory pressure).
+//
+// Scratch: C2_STATIC_SCRATCH_BYTES = 16 MiB; bytes [0, 256) hold the work
+// counter (zeroed by every call), the rest holds 10 x Lmax floats per warp
+// slot, Lmax being the longest db profile.  The grid shrinks to the number of
+// 8-warp blocks whose slots fit; a database whose longest profile needs more
+// than the whole array for one block (Lmax > 52,428) is rejected.
+// Every call on a device shares the one array: calls whose kernels overlap on
+// the GPU (different streams, or different handles on one device) race on it.
+// The first call on a device resolves the array's address with
+// cudaGetSymbolAddress (with that device current); make that first call
+// before any stream capture.
+namespace {
+constexpr size_t C2_STATIC_SCRATCH_BYTES = size_t(16) << 20;
+constexpr size_t C2_STATIC_HDR = 256;
+constexpr int C2_STATIC_MAXDEV = 64;
+__device__ __align__(256) unsigned char c2_static_scratch[C2_STATIC_SCRATCH_BYTES];
+void* g_static_scratch[C2_STATIC_MAXDEV] = {};
+std::mutex g_static_mu;
+}  // namespace
+
+extern "C" c2_status c2_run_phase1_static(c2_handle* h, float* d_best, uint32_t* d_coords)
+{
+    if (!h || !d_best || !d_coords) return C2_ERR_ARG;
+    if (h->nprof <= 0 || h->Lq <= 0) return fail(h, C2_ERR_STATE, "run_phase1_static needs a database and a query");
+    if (h->device < 0 || h->device >= C2_STATIC_MAXDEV)
+        return fail(h, C2_ERR_ARG, "run_phase1_static: device %d out of range", h->device);
+    CK(cudaSetDevice(h->device));
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_static_mu);
+        if (!g_static_scratch[h->device]) {
+            void* p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, c2_static_scratch);
+            if (e != cudaSuccess || !p)
+                return fail(h, C2_ERR_CUDA, "run_phase1_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+            g_static_scratch[h->device] = p;
+        }
+        base = g_static_scratch[h->device];
+    }
+    const size_t per_block = (size_t)h->botstride * sizeof(float) * P1_WARPS;
+    const size_t nblocks = (C2_STATIC_SCRATCH_BYTES - C2_STATIC_HDR) / per_block;
+    if (nblocks < 1)
+        return fail(h, C2_ERR_CAPACITY,
+                    "run_phase1_static: longest db profile (%lld positions) exceeds the static scratch limit "
+                    "(%zu positions)",
+                    h->botstride / 10, (C2_STATIC_SCRATCH_BYTES - C2_STATIC_HDR) / (10 * sizeof(float) * P1_WARPS));
+    const int grid = (int)std::min<size_t>((size_t)h->grid, nblocks);
+    P1Args a;
+    fill_p1(h, a);
+    a.nwork = h->nprof;
+    a.order = h->d_order.p;
+    a.counter = (int*)base;
+    a.bot = (float*)((char*)base + C2_STATIC_HDR);
+    a.best = d_best;
+    a.coords = d_coords;
+    CK(cudaMemsetAsync(base, 0, sizeof(int), h->stream));
+    CK(launch_p1(a, h->d_qbkg.p, false, grid, h->stream));
+    h->launches++;
     return C2_OK;
 }

@@ -26,6 +26,7 @@ EXPORTS = [
     "c2_create", "c2_destroy", "c2_last_error", "c2_upload_db", "c2_set_query", "c2_run_phase1",
     "c2_get_phase1", "c2_run_finalize", "c2_get_finalize", "c2_get_thresholds", "c2_set_stream", "c2_sync",
     "c2_launch_count", "c2_run_stats", "c2_run_map", "c2_get_hits", "c2_search", "c2_get_search_space",
+    "c2_run_phase1_static",
 ]
 
 _fp = C.POINTER(C.c_float)
@@ -103,6 +104,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.c2_get_hits.argtypes = [C.c_void_p, P(c2_hit), C.c_int32, C.c_char_p, P(C.c_size_t)]
     lib.c2_search.argtypes = [C.c_void_p, P(c2_profiles), P(C.c_int32)]
     lib.c2_get_search_space.argtypes = [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]
+    lib.c2_run_phase1_static.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     for n in EXPORTS:
         getattr(lib, n).restype = C.c_int
     _lib = lib

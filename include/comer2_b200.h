@@ -206,6 +206,18 @@ c2_status c2_sync(c2_handle* h);
 /* Number of kernel launches issued by the handle since creation. */
 c2_status c2_launch_count(const c2_handle* h, uint64_t* n);
 
+/* Phase 1 (as c2_run_phase1) that allocates nothing.  No counterpart in the
+ * reference.  Its scratch (work counter, strip-boundary rows) lives in one
+ * static 16 MiB device array per device, so the grid is limited to the 8-warp
+ * blocks whose boundary rows fit; a database whose longest profile exceeds
+ * 52,428 positions is rejected with C2_ERR_CAPACITY.  Results go to caller-owned
+ * device arrays of nprofiles entries (d_best: DP maxima, d_coords: packed
+ * (column << 16 | row) of the maximum), in the layout c2_get_phase1 reports.
+ * The array is shared by every call on the device: calls that overlap on the
+ * GPU race.  The first call on a device looks up the array's address; make it
+ * before any stream capture.  Enqueued on the handle's stream. */
+c2_status c2_run_phase1_static(c2_handle* h, float* d_best, uint32_t* d_coords);
+
 #ifdef __cplusplus
 }
 #endif

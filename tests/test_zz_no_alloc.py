@@ -1,0 +1,62 @@
+"""The allocation-free phase-1 entry point c2_run_phase1_static, through the
+C ABI: its results equal c2_run_phase1's on the same database and query, on
+two calls in a row (the second reuses the static scratch), and a database
+beyond its compiled scratch limit is refused before any launch."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from comer2_b200 import synth as S
+
+pytestmark = pytest.mark.gpu
+
+C2_ERR_CAPACITY = 5
+
+
+def _call(h, d_best, d_coords):
+    return h.lib.c2_run_phase1_static(h._h, C.c_void_p(d_best.data_ptr()), C.c_void_p(d_coords.data_ptr()))
+
+
+def test_phase1_static_matches_phase1(params):
+    import torch
+    from comer2_b200.native import Handle
+    w = S.config(1, seed=5, scale=0.002)   # 200 profiles, lengths 30..2000
+    h = Handle(params, 0)
+    h.upload_db(w.db)
+    h.set_query(w.queries[0])
+    h.run_phase1()
+    h.sync()
+    best, coords = h.phase1()
+    n = w.db.nprofiles
+    for _ in range(2):
+        d_best = torch.full((n,), -1.0, dtype=torch.float32, device="cuda:0")
+        d_coords = torch.full((n,), -1, dtype=torch.int32, device="cuda:0")
+        torch.cuda.synchronize()
+        h._ck(_call(h, d_best, d_coords), "c2_run_phase1_static")
+        h.sync()
+        got_b = d_best.cpu().numpy()
+        got_c = d_coords.cpu().numpy().view(np.uint32)
+        assert np.array_equal(got_b.view(np.uint32), best.view(np.uint32))
+        assert np.array_equal(got_c, coords)
+    h.close()
+
+
+def test_phase1_static_rejects_beyond_limit(params):
+    import torch
+    from comer2_b200.native import Handle
+    rng = np.random.default_rng(3)
+    db = S.random_profiles(rng, [52_429])   # one position beyond the 16 MiB scratch limit
+    q = S.random_profiles(rng, [40])
+    h = Handle(params, 0)
+    h.upload_db(db)
+    h.set_query(q)
+    d_best = torch.zeros(1, dtype=torch.float32, device="cuda:0")
+    d_coords = torch.zeros(1, dtype=torch.int32, device="cuda:0")
+    before = h.launch_count()
+    assert _call(h, d_best, d_coords) == C2_ERR_CAPACITY
+    buf = C.create_string_buffer(512)
+    h.lib.c2_last_error(h._h, buf, 512)
+    assert b"static scratch limit" in buf.value
+    assert h.launch_count() == before
+    h.close()
