@@ -84,15 +84,31 @@ def run(outroot):
 
 
 def collect(outroot):
+    """Summarise the reference's JSON output per case into ref_b200_outcome.json:
+    the number of reported hits, how many have a finite score and E-value, and
+    the first hits' fields."""
+    summary = {}
     for case in CASES:
-        files = [f for f in glob.glob(os.path.join(outroot, case, "*")) if not f.endswith("comer.log")]
-        res = {"case": case, "config": CASES[case], "files": {}}
-        for f in files:
-            with open(f) as fh:
-                res["files"][os.path.basename(f)] = fh.read()
-        with open(os.path.join(HERE, "ref_%s.json" % case), "w") as fh:
-            json.dump(res, fh, indent=1)
-        print("collected", case, list(res["files"]))
+        files = glob.glob(os.path.join(outroot, case, "*.json"))
+        if not files:
+            summary[case] = {"error": "no output"}
+            continue
+        t = open(files[0]).read().replace("-nan", "NaN").replace("nan", "NaN").replace("inf", "Infinity")
+        hits = json.loads(t)["comer_search"]["search_hits"]
+        recs = []
+        for h in hits:
+            r = h["hit_record"]
+            a = r["alignment"]
+            recs.append({"target": r["target_description"], "score": a["score"], "evalue": a["evalue"],
+                         "expected_score": a["expected_score"], "aln_length": a["aln_length"],
+                         "min_score": a["min_score"], "max_score": a["max_score"]})
+        import math
+        finite = sum(1 for x in recs if math.isfinite(x["score"]) and math.isfinite(x["evalue"])
+                     and abs(x["score"]) < 1e6)
+        summary[case] = {"config": CASES[case], "n_hits": len(recs), "n_finite": finite, "first": recs[:5]}
+    with open(os.path.join(HERE, "ref_b200_outcome.json"), "w") as fh:
+        json.dump(summary, fh, indent=1)
+    print(json.dumps({k: (v.get("n_hits"), v.get("n_finite")) for k, v in summary.items()}))
 
 
 if __name__ == "__main__":
