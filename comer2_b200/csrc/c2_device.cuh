@@ -77,6 +77,10 @@ struct P1Args {
     float* smat;                // [L][Lq] per candidate
     float* mmat;                // [L][Lq] per candidate: modular scores
     int* status;                // device error word (0 = ok)
+    // strip pipeline of the traceback variant
+    float* bnd;                 // per candidate at 10 x (cand_off / Lq): two last-row buffers [5][L]
+    int* prog;                  // [ncand][nstrips] finished columns per strip
+    float* tbbest;              // [ncand] DP maximum of the traceback sweep
 };
 
 struct FinArgs {
@@ -90,6 +94,8 @@ struct FinArgs {
     const float* best;
     const unsigned* coords;
     float scorethld;
+    const float* tbbest;        // [ncand] maxima of the traceback sweep (checked against best)
+    int* status;
     // outputs [ncand]
     float* score;
     int* psts;
@@ -98,4 +104,60 @@ struct FinArgs {
     int* passed;
 };
 
+}  // namespace c2
+
+// ---------------------------------------------------------------------------
+// Phase-2 sweeps (traceback DP, MAP forward/backward/MAP DP) run one strip of
+// one pair per warp: a work item is (pair m, strip s), items are handed out
+// in order from a global counter, so the item a warp waits on was taken
+// earlier by a warp that is running.  Strip s writes its last row (5 states
+// per column) to bnd[m][s & 1][5][L] and publishes the number of finished
+// columns in prog[m * nstrips + s]; strip s+1 waits for the columns it
+// prefetches.  A long pair is thus swept by up to nstrips warps at once
+// instead of one.
+namespace c2 {
+constexpr int PIPE_G = 8;                 // columns per progress update
+constexpr unsigned PIPE_SPIN = 1u << 22;  // polls before a wait gives up
+constexpr int PIPE_ERR_TIMEOUT = 3;       // device status of an abandoned wait
+
+__device__ __forceinline__ int pipe_ld_acquire(const int* p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void pipe_st_release(int* p, int v)
+{
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Warp-uniform wait until *flag >= need (lane 0 polls).  After PIPE_SPIN
+// polls it records PIPE_ERR_TIMEOUT in *status, marks the warp broken (no
+// further waits) and returns; the sweep then finishes with invalid values
+// and the host reports the status.
+__device__ __forceinline__ void pipe_wait(const int* flag, int need, int lane, int* status, bool& broken)
+{
+    if (broken) return;
+    unsigned it = 0;
+    for (;;) {
+        int ok = 0;
+        if (lane == 0) ok = pipe_ld_acquire(flag) >= need;
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (ok) break;
+        if (++it >= PIPE_SPIN) {
+            if (lane == 0 && status) atomicCAS(status, 0, PIPE_ERR_TIMEOUT);
+            broken = true;
+            break;
+        }
+        __nanosleep(128);
+    }
+    __syncwarp();
+}
+
+// producer side: lane 31 has stored column c of its strip's last row
+__device__ __forceinline__ void pipe_publish(int* flag, int c, int L)
+{
+    if (((c + 1) % PIPE_G) == 0 || c + 1 == L) pipe_st_release(flag, c + 1);
+}
 }  // namespace c2

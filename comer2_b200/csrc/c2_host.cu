@@ -99,6 +99,9 @@ struct c2_handle {
     DevBuf<long long> d_cand_off;
     DevBuf<signed char> d_btck;
     DevBuf<float> d_smat, d_mmat;
+    // strip pipeline of the phase-2 sweeps: last-row buffers, progress words
+    DevBuf<float> d_bnd, d_tbbest;
+    DevBuf<int> d_prog;
     DevBuf<float> d_fscore;
     DevBuf<int> d_fpsts, d_fpassed;
     DevBuf<unsigned> d_fbeg, d_fend;
@@ -116,6 +119,7 @@ struct c2_handle {
     DevBuf<int> d_mapcand, d_mappass, d_alninfo;
     DevBuf<float> d_fb, d_pairf;
     DevBuf<unsigned> d_pairc;
+    DevBuf<unsigned long long> d_pairk;
     DevBuf<char> d_aln;
     int alnstride = 0;
 };
@@ -140,6 +144,17 @@ static c2_status fail(c2_handle* h, c2_status st, const char* fmt, ...)
             return fail(h, C2_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
                         __FILE__, __LINE__);                                            \
     } while (0)
+
+// device status words: 2 = the traceback DP's maximum differs from phase 1,
+// 3 = a phase-2 sweep gave up waiting for the strip above it
+static const char* status_text(int st)
+{
+    switch (st) {
+    case 2: return "traceback DP disagrees with phase 1";
+    case PIPE_ERR_TIMEOUT: return "a strip wait in a phase-2 sweep timed out";
+    default: return "unknown device error";
+    }
+}
 
 // Context-vector constants exactly as _TCTXVECT computes them in float
 // (src/libpro/srcpro/TCTXVECT.cpp:26-54).
@@ -596,7 +611,9 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     const int nc = h->ncand;
     if (h->d_cand_prof.ensure(nc) || h->d_cand_off.ensure(nc) || h->d_btck.ensure((size_t)acc) ||
         h->d_smat.ensure((size_t)acc) || h->d_mmat.ensure((size_t)acc) || h->d_fscore.ensure(nc) || h->d_fpsts.ensure(nc) ||
-        h->d_fpassed.ensure(nc) || h->d_fbeg.ensure(nc) || h->d_fend.ensure(nc))
+        h->d_fpassed.ensure(nc) || h->d_fbeg.ensure(nc) || h->d_fend.ensure(nc) ||
+        h->d_bnd.ensure((size_t)(acc / h->Lq) * 10) || h->d_tbbest.ensure(nc) ||
+        h->d_prog.ensure((size_t)nc * ((h->Lq + 31) / 32)))
         return fail(h, C2_ERR_NOMEM, "finalisation scratch for %d pairs (%lld cells) failed", nc, acc);
     CK(cudaMemcpyAsync(h->d_cand_prof.p, h->h_cand.data(), (size_t)nc * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_cand_off.p, h->h_cand_off.data(), (size_t)nc * 8, cudaMemcpyHostToDevice, h->stream));
@@ -608,8 +625,15 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     a.btck = h->d_btck.p;
     a.smat = h->d_smat.p;
     a.mmat = h->d_mmat.p;
+    a.bnd = h->d_bnd.p;
+    a.prog = h->d_prog.p;
+    a.tbbest = h->d_tbbest.p;
+    const long long nitems = (long long)nc * ((h->Lq + 31) / 32);
     CK(cudaMemsetAsync(h->d_counter.p, 0, sizeof(int), h->stream));
-    const int grid = std::min(h->grid, (nc + P1_WARPS - 1) / P1_WARPS);
+    CK(cudaMemsetAsync(h->d_prog.p, 0, (size_t)nitems * sizeof(int), h->stream));
+    CK(cudaMemsetAsync(h->d_tbbest.p, 0, (size_t)nc * sizeof(float), h->stream));
+    // one warp per (candidate, strip) work item at most
+    const int grid = (int)std::min<long long>(h->grid, (nitems + P1_WARPS - 1) / P1_WARPS);
     CK(launch_p1(a, h->d_qbkg.p, true, grid, h->stream));
     h->launches++;
     FinArgs f;
@@ -623,6 +647,8 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     f.best = h->d_best.p;
     f.coords = h->d_coords.p;
     f.scorethld = h->scorethld;
+    f.tbbest = h->d_tbbest.p;
+    f.status = h->d_status.p;
     f.score = h->d_fscore.p;
     f.psts = h->d_fpsts.p;
     f.beg = h->d_fbeg.p;
@@ -639,7 +665,7 @@ extern "C" c2_status c2_get_finalize(c2_handle* h, c2_dp_result* out, int32_t n)
     CK(cudaStreamSynchronize(h->stream));
     int stw = 0;
     CK(cudaMemcpy(&stw, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (stw != 0) return fail(h, C2_ERR_DEVICE, "device status %d (traceback DP disagrees with phase 1)", stw);
+    if (stw != 0) return fail(h, C2_ERR_DEVICE, "device status %d (%s)", stw, status_text(stw));
     const int nc = h->ncand;
     if (nc == 0) return C2_OK;
     std::vector<float> sc(nc);
@@ -683,7 +709,7 @@ extern "C" c2_status c2_run_stats(c2_handle* h, int32_t* npassed)
     CK(cudaStreamSynchronize(h->stream));
     int stw = 0;
     CK(cudaMemcpy(&stw, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (stw != 0) return fail(h, C2_ERR_DEVICE, "device status %d (traceback DP disagrees with phase 1)", stw);
+    if (stw != 0) return fail(h, C2_ERR_DEVICE, "device status %d (%s)", stw, status_text(stw));
     const int nc = h->ncand;
     h->h_p2.clear();
     h->h_fscore.assign(nc, 0.f);
@@ -756,7 +782,8 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
     h->alnstride = h->Lq + h->Lmax + 1;
     size_t fbn = h->d_smat.n;   // same layout as the candidates' score matrices
     if (h->d_mapcand.ensure(nm) || h->d_mappass.ensure(nm) || h->d_fb.ensure(fbn) || h->d_pairf.ensure((size_t)nm * 4) ||
-        h->d_pairc.ensure(nm) || h->d_alninfo.ensure((size_t)nm * 8) || h->d_aln.ensure((size_t)nm * 5 * h->alnstride))
+        h->d_pairc.ensure(nm) || h->d_alninfo.ensure((size_t)nm * 8) || h->d_aln.ensure((size_t)nm * 5 * h->alnstride) ||
+        h->d_pairk.ensure(nm))
         return fail(h, C2_ERR_NOMEM, "MAP buffers for %d pairs failed", nm);
     CK(cudaMemcpyAsync(h->d_mapcand.p, h->h_mapcand.data(), (size_t)nm * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_mappass.p, h->h_mappass.data(), (size_t)nm * 4, cudaMemcpyHostToDevice, h->stream));
@@ -777,8 +804,10 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
     a.btck = h->d_btck.p;
     a.pairf = h->d_pairf.p;
     a.pairc = h->d_pairc.p;
-    a.bot = h->d_bot.p;
-    a.botstride = h->botstride;
+    a.bnd = h->d_bnd.p;
+    a.prog = h->d_prog.p;
+    a.pairk = h->d_pairk.p;
+    a.status = h->d_status.p;
     a.counter = h->d_counter.p;
     a.minpp = h->prm.minpp;
     a.modscores = (h->prm.ssswgt > 0.f || h->prm.cvswgt > 0.f) ? 1 : 0;
@@ -802,6 +831,9 @@ extern "C" c2_status c2_get_hits(c2_handle* h, c2_hit* hits, int32_t n, char* al
 {
     if (!h || !aln_bytes) return C2_ERR_ARG;
     CK(cudaStreamSynchronize(h->stream));
+    int stw = 0;
+    CK(cudaMemcpy(&stw, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (stw != 0) return fail(h, C2_ERR_DEVICE, "device status %d (%s)", stw, status_text(stw));
     const int nm = h->nmap;
     const size_t per = (size_t)5 * h->alnstride;
     std::vector<int> info((size_t)nm * 8);

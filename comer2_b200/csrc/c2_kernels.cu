@@ -18,8 +18,8 @@
 //    transitions passed down the lanes the same way;
 //  * the strip's last row is handed to the next strip through a per-warp
 //    boundary buffer (global memory, L2 resident).
-// The traceback variant (TB = true) recomputes the same DP for the pairs that
-// pass the phase-1 threshold and stores their scores and btck codes
+// The traceback variant (p1tb_kernel) recomputes the same DP for the pairs
+// that pass the phase-1 threshold and stores their scores and btck codes
 // column-major for the finalisation, statistics and MAP stages.
 #include "c2_device.cuh"
 
@@ -141,7 +141,6 @@ __device__ __forceinline__ void stage_chunk(float* rec, const float* __restrict_
     cp_async_commit();
 }
 
-template <bool TB>
 __global__ void __launch_bounds__(P1_WARPS * 32, 2)
 p1_kernel(P1Args a, const float* __restrict__ qbkg)
 {
@@ -175,12 +174,6 @@ p1_kernel(P1Args a, const float* __restrict__ qbkg)
         const float* __restrict__ dr = a.drec + off * DR_STRIDE;
         const float* __restrict__ bd = a.pbkg + (long long)p * NAA;
         const int edge = corner_edge(Lq, L);
-        signed char* bt = nullptr;
-        float* smt = nullptr;
-        if (TB) {
-            bt = a.btck + a.cand_off[item];
-            smt = a.smat + a.cand_off[item];
-        }
         float best = 0.f;
         int brow = 0x7fffffff, bcol = 0x7fffffff;
         float* botr = bot0;
@@ -252,10 +245,6 @@ p1_kernel(P1Args a, const float* __restrict__ qbkg)
                     float S = cell_score(R, rp, U, cvtab, sc, lane, mod);
                     if (!act) S = -9.f;
                     ring[(k & 31) * 32 + lane] = S;
-                    if (TB && act) {
-                        smt[(long long)k * Lq + r] = S;
-                        a.mmat[a.cand_off[item] + (long long)k * Lq + r] = mod;
-                    }
                     const float4 ta = rp[12], tb = rp[13];
                     tc[0] = ta.x; tc[1] = ta.y; tc[2] = ta.z; tc[3] = ta.w;
                     tc[4] = tb.x; tc[5] = tb.y; tc[6] = tb.z;
@@ -319,16 +308,6 @@ p1_kernel(P1Args a, const float* __restrict__ qbkg)
                 }
                 const bool valid = act && j >= 0 && j < L;
                 if (valid && nw.MM > best) { best = nw.MM; brow = r; bcol = j; }
-                if (TB && valid) {
-                    int b = BT_STOP;
-                    float mx = nw.MM;
-                    if (nw.MM != 0.f) b = BT_DIAG;
-                    if (mx < nw.MI) { mx = nw.MI; b = BT_UP; }
-                    if (mx < nw.IM) { mx = nw.IM; b = BT_LEFT; }
-                    if (mx < nw.DN) { mx = nw.DN; b = BT_UP; }
-                    if (mx < nw.ND) { b = BT_LEFT; }
-                    bt[(long long)j * Lq + r] = (signed char)b;
-                }
                 if (wr_bot && j >= 0 && j < L) {
                     botw[0 * Lmax + j] = nw.MM;
                     botw[1 * Lmax + j] = nw.MI;
@@ -355,17 +334,228 @@ p1_kernel(P1Args a, const float* __restrict__ qbkg)
         }
         if (lane == 0) {
             const unsigned xy = (best > 0.f) ? (((unsigned)bcol << 16) | ((unsigned)brow & 0xffffu)) : 0u;
-            if (TB) {
-                // consistency check against the phase-1 result of this pair
-                if (a.best[p] != best && a.status) atomicCAS(a.status, 0, 2);
-            } else {
-                a.best[p] = best;
-                a.coords[p] = xy;
-            }
+            a.best[p] = best;
+            a.coords[p] = xy;
         }
         __syncwarp();
     }
 }
+
+// Traceback variant for the candidate pairs: the same score and DP
+// arithmetic as p1_kernel, storing the score matrix, the modular scores and
+// the btck codes column-major.  Work items are (candidate, strip) as in the
+// phase-2 strip pipeline (c2_device.cuh), so a long pair is swept by several
+// warps at once; the pair maximum is collected in tbbest for the check
+// against phase 1.
+__global__ void __launch_bounds__(P1_WARPS * 32, 2)
+p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
+{
+    extern __shared__ float smem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int cvcard = a.sc.cvcard;
+    const int card = a.sc.ssss_card;
+    float* cvtab = smem;                                      // [cvcard][32]
+    float* wb = smem + cvcard * 32 + wid * P1_WARP_FLOATS;
+    float* ring = wb;                                         // [32][32]
+    float* U = wb + 32 * 32;                                  // [card][32]
+    float* rec = U + MAX_SSSS_CARD * 32;                      // [REC_SLOTS][DR_STRIDE] db records
+    for (int i = threadIdx.x; i < cvcard * 32; i += blockDim.x) cvtab[i] = a.cvvals[i >> 5];
+    __syncthreads();
+
+    const int Lq = a.Lq;
+    const int nstrips = (Lq + 31) >> 5;
+    const int nitems = a.nwork * nstrips;
+    const ScoreConsts sc = a.sc;
+    bool broken = false;
+
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.counter, 1);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= nitems) break;
+        const int cand = item / nstrips, s = item - cand * nstrips;
+        const int p = a.order[cand];
+        const int L = a.plen[p];
+        const long long off = a.poff[p];
+        const float* __restrict__ dr = a.drec + off * DR_STRIDE;
+        const float* __restrict__ bd = a.pbkg + (long long)p * NAA;
+        const int edge = corner_edge(Lq, L);
+        const long long coff = a.cand_off[cand];
+        signed char* bt = a.btck + coff;
+        float* smt = a.smat + coff;
+        float* mmt = a.mmat + coff;
+        float* bnd = a.bnd + (coff / Lq) * 10;
+        const float* botr = bnd + ((s + 1) & 1) * 5 * L;   // last row of strip s-1
+        float* botw = bnd + (s & 1) * 5 * L;
+        int* pf = a.prog + (long long)cand * nstrips;
+        float best = 0.f;
+        {
+            const int r = s * 32 + lane;
+            const bool act = r < Lq;
+            const float* __restrict__ qr = a.qrec + (long long)(act ? r : Lq - 1) * QR_STRIDE;
+            RowOps R;
+#pragma unroll
+            for (int i = 0; i < NAA; i++)
+                R.Qt[i] = __fdividef(qr[QR_TRG + i], 0.5f * (qbkg[i] + bd[i]));
+#pragma unroll
+            for (int i = 0; i < NCV; i++) R.qcv[i] = qr[QR_CV + i];
+            R.cq = qr[QR_CN];
+            R.pq = qr[QR_PRIOR];
+            R.hq = qr[QR_HQ];
+            {
+                const float q0 = qr[QR_SS], q1 = qr[QR_SS + 1], q2 = qr[QR_SS + 2];
+                const int i0 = (int)(q0 * 9.999f), i1 = 10 + (int)(q1 * 9.999f), i2 = 20 + (int)(q2 * 9.999f);
+                for (int c = 0; c < card; c++)
+                    U[c * 32 + lane] = q0 * __ldg(a.ssss + i0 * card + c) + q1 * __ldg(a.ssss + i1 * card + c) +
+                                       q2 * __ldg(a.ssss + i2 * card + c);
+            }
+            float q7[7];
+#pragma unroll
+            for (int i = 0; i < 7; i++) q7[i] = act ? qr[QR_TRN + i] : LOG0;
+            // column -1 boundary states of this row and of the row above
+            const bool z_left = (lane == 31);
+            const bool z_diag = (lane == 31 || lane == 0);
+            const St5 LB = z_left ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
+                                  : St5{0.f, qr[QR_C + 0], qr[QR_C + 1], qr[QR_C + 2], LOG0};
+            const St5 DB = z_diag ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
+                                  : St5{0.f, qr[QR_CP + 0], qr[QR_CP + 1], qr[QR_CP + 2], LOG0};
+            __syncwarp();
+
+            St5 mine = {0.f, 0.f, 0.f, 0.f, 0.f};
+            St5 upp = {0.f, 0.f, 0.f, 0.f, 0.f};
+            float t7[7];
+#pragma unroll
+            for (int i = 0; i < 7; i++) t7[i] = LOG0;
+            // strip-boundary prefetch: lane i holds column c0 + i of the row above
+            float bcur[5], bnxt[5];
+            if (s > 0) pipe_wait(pf + s - 1, min(64, L), lane, a.status, broken);
+#pragma unroll
+            for (int f = 0; f < 5; f++) {
+                bcur[f] = 0.f;
+                bnxt[f] = 0.f;
+                if (s > 0) {
+                    if (lane < L) bcur[f] = __ldcg(botr + f * L + lane);
+                    if (32 + lane < L) bnxt[f] = __ldcg(botr + f * L + 32 + lane);
+                }
+            }
+            const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
+            const int nsteps = L + 31;
+            // db column records are staged into shared memory one chunk ahead
+            stage_chunk(rec, dr, 0, L, lane);
+            stage_chunk(rec, dr, 1, L, lane);
+            for (int k = 0; k < nsteps; k++) {
+                if ((k & (REC_CHUNK - 1)) == 0 && k < L) {
+                    cp_async_wait_1();
+                    __syncwarp();
+                }
+                // ---- score stage: column k for every lane's row
+                float tc[7];
+                if (k < L) {
+                    const float4* rp = reinterpret_cast<const float4*>(rec + (k & (REC_SLOTS - 1)) * DR_STRIDE);
+                    float mod;
+                    float S = cell_score(R, rp, U, cvtab, sc, lane, mod);
+                    if (!act) S = -9.f;
+                    ring[(k & 31) * 32 + lane] = S;
+                    if (act) {
+                        smt[(long long)k * Lq + r] = S;
+                        mmt[(long long)k * Lq + r] = mod;
+                    }
+                    const float4 ta = rp[12], tb = rp[13];
+                    tc[0] = ta.x; tc[1] = ta.y; tc[2] = ta.z; tc[3] = ta.w;
+                    tc[4] = tb.x; tc[5] = tb.y; tc[6] = tb.z;
+                    if ((k & (REC_CHUNK - 1)) == REC_CHUNK - 1) {
+                        // chunk fully read by every lane: refill its slots two chunks ahead
+                        __syncwarp();
+                        stage_chunk(rec, dr, (k >> REC_CHUNK_LOG) + 2, L, lane);
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 7; i++) tc[i] = LOG0;
+                }
+                // ---- DP stage: column j = k - lane
+#pragma unroll
+                for (int i = 0; i < 7; i++) {
+                    const float x = __shfl_up_sync(FULL, t7[i], 1);
+                    t7[i] = (lane == 0) ? tc[i] : x;
+                }
+                St5 up;
+                up.MM = __shfl_up_sync(FULL, mine.MM, 1);
+                up.MI = __shfl_up_sync(FULL, mine.MI, 1);
+                up.IM = __shfl_up_sync(FULL, mine.IM, 1);
+                up.DN = __shfl_up_sync(FULL, mine.DN, 1);
+                up.ND = __shfl_up_sync(FULL, mine.ND, 1);
+                {
+                    const int src = k & 31;
+                    const float b0 = __shfl_sync(FULL, bcur[0], src);
+                    const float b1 = __shfl_sync(FULL, bcur[1], src);
+                    const float b2 = __shfl_sync(FULL, bcur[2], src);
+                    const float b3 = __shfl_sync(FULL, bcur[3], src);
+                    const float b4 = __shfl_sync(FULL, bcur[4], src);
+                    if (lane == 0) up = St5{b0, b1, b2, b3, b4};
+                    if (src == 31) {
+                        if (s > 0 && k + 33 < L) pipe_wait(pf + s - 1, min(k + 65, L), lane, a.status, broken);
+#pragma unroll
+                        for (int f = 0; f < 5; f++) {
+                            bcur[f] = bnxt[f];
+                            const int c = k + 33 + lane;
+                            bnxt[f] = (s > 0 && c < L) ? __ldcg(botr + f * L + c) : 0.f;
+                        }
+                    }
+                }
+                const int j = k - lane;
+                St5 left = mine, diag = upp;
+                if (j == 0) { left = LB; diag = DB; }
+                float S = -9.f;
+                if (j >= 0 && j < L) {
+                    S = ring[(j & 31) * 32 + lane];
+                    if (in_corner(Lq, L, edge, r, j)) S = -9.f;
+                }
+                St5 nw;
+                {
+                    float v = fmaxf((diag.MI + q7[TMM]) + t7[TIM], (diag.IM + q7[TIM]) + t7[TMM]);
+                    v = fmaxf(v, (diag.DN + q7[TDM]) + t7[TMM]);
+                    v = fmaxf(v, (diag.ND + q7[TMM]) + t7[TDM]);
+                    v = fmaxf(v, (diag.MM + q7[TMM]) + t7[TMM]);
+                    nw.MM = fmaxf(v + S, 0.f);
+                    nw.MI = fmaxf((up.MM + q7[TMM]) + t7[TMI], (up.MI + q7[TMM]) + t7[TII]);
+                    nw.IM = fmaxf((left.MM + q7[TMI]) + t7[TMM], (left.IM + q7[TII]) + t7[TMM]);
+                    nw.DN = fmaxf(up.MM + q7[TMD], up.DN + q7[TDD]);
+                    nw.ND = fmaxf(left.MM + t7[TMD], left.ND + t7[TDD]);
+                }
+                const bool valid = act && j >= 0 && j < L;
+                if (valid && nw.MM > best) best = nw.MM;
+                if (valid) {
+                    int b = BT_STOP;
+                    float mx = nw.MM;
+                    if (nw.MM != 0.f) b = BT_DIAG;
+                    if (mx < nw.MI) { mx = nw.MI; b = BT_UP; }
+                    if (mx < nw.IM) { mx = nw.IM; b = BT_LEFT; }
+                    if (mx < nw.DN) { mx = nw.DN; b = BT_UP; }
+                    if (mx < nw.ND) { b = BT_LEFT; }
+                    bt[(long long)j * Lq + r] = (signed char)b;
+                }
+                if (wr_bot && j >= 0 && j < L) {
+                    botw[0 * L + j] = nw.MM;
+                    botw[1 * L + j] = nw.MI;
+                    botw[2 * L + j] = nw.IM;
+                    botw[3 * L + j] = nw.DN;
+                    botw[4 * L + j] = nw.ND;
+                    pipe_publish(pf + s, j, L);
+                }
+                mine = nw;
+                upp = up;
+            }
+            cp_async_wait_all();
+            __syncwarp();
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) best = fmaxf(best, __shfl_xor_sync(FULL, best, o));
+        // best >= 0, so its bit pattern orders as an unsigned integer
+        if (lane == 0) atomicMax(reinterpret_cast<unsigned*>(a.tbbest + cand), __float_as_uint(best));
+        __syncwarp();
+    }
+}
+
 
 // Warp butterfly sum as the reference's FinalizeDPPro reduction
 // (src/libmycu/cudp/CuBatchDP_final.cu:254-260).
@@ -394,6 +584,8 @@ __global__ void __launch_bounds__(256) fin_kernel(FinArgs a)
     const float* sm = a.smat + a.cand_off[c];
     float* ch = cache[wid];
     const float maxsc = a.best[p];
+    // the traceback sweep must reproduce the phase-1 maximum of this pair
+    if (lane == 0 && a.tbbest[c] != maxsc && a.status) atomicCAS(a.status, 0, 2);
     const unsigned xx = a.coords[p];
     int x = (int)(xx >> 16), y = (int)(xx & 0xffff);
     int psts = 0;
@@ -454,11 +646,11 @@ cudaError_t launch_p1(const P1Args& a, const float* qbkg, bool tb, int grid, cud
 {
     const size_t sm = p1_smem_bytes(a.sc.cvcard);
     if (tb) {
-        cudaFuncSetAttribute(p1_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        p1_kernel<true><<<grid, P1_WARPS * 32, sm, st>>>(a, qbkg);
+        cudaFuncSetAttribute(p1tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        p1tb_kernel<<<grid, P1_WARPS * 32, sm, st>>>(a, qbkg);
     } else {
-        cudaFuncSetAttribute(p1_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        p1_kernel<false><<<grid, P1_WARPS * 32, sm, st>>>(a, qbkg);
+        cudaFuncSetAttribute(p1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        p1_kernel<<<grid, P1_WARPS * 32, sm, st>>>(a, qbkg);
     }
     return cudaGetLastError();
 }
@@ -467,8 +659,8 @@ int p1_blocks_per_sm(int cvcard)
 {
     int n = 0;
     const size_t sm = p1_smem_bytes(cvcard);
-    cudaFuncSetAttribute(p1_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, p1_kernel<false>, P1_WARPS * 32, sm);
+    cudaFuncSetAttribute(p1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, p1_kernel, P1_WARPS * 32, sm);
     return n > 0 ? n : 1;
 }
 

@@ -14,6 +14,8 @@
 // inverse with the reference's adjustment constant
 // (src/libmycu/cucom/myfastapproxmath.cuh:13-45), arguments below -16 giving
 // 0 and probabilities below 3.8e-11 giving -99 (_fwd.cuh:205-253).
+#include <algorithm>
+
 #include "c2_device.cuh"
 #include "c2_stats.cuh"
 
@@ -122,7 +124,8 @@ __device__ __forceinline__ float map_score(const MapArgs& a, const MapPair& P, l
 }
 
 // ---------------------------------------------------------------------------
-// forward sweep: F for every cell; F.MM stored column-major in fb
+// forward sweep: F for every cell; F.MM stored column-major in fb.  Work
+// items are (pair, strip); see the strip pipeline in c2_device.cuh.
 __global__ void __launch_bounds__(MAPW * 32) map_fwd_kernel(MapArgs a, const float* __restrict__ qtrn,
                                                       const float* __restrict__ dtrn,
                                                       const float* __restrict__ qcf)
@@ -131,25 +134,27 @@ __global__ void __launch_bounds__(MAPW * 32) map_fwd_kernel(MapArgs a, const flo
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float(*rin)[33] = rings[wid][0];
     float(*rout)[33] = rings[wid][1];
-    const long long slot = (long long)blockIdx.x * MAPW + wid;
-    const int Lmax = (int)(a.botstride / 10);
-    float* bot0 = a.bot + slot * a.botstride;
     const int Lq = a.Lq;
     const int nstrips = (Lq + 31) >> 5;
+    const int nitems = a.nmap * nstrips;
     const S5 INIT = {0.f, MLOG0, MLOG0, MLOG0, MLOG0};
+    bool broken = false;
     for (;;) {
-        int m = 0;
-        if (lane == 0) m = atomicAdd(a.counter, 1);
-        m = __shfl_sync(FULL, m, 0);
-        if (m >= a.nmap) break;
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.counter, 1);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= nitems) break;
+        const int m = item / nstrips, s = item - m * nstrips;
         const MapPair P = map_pair(a, qtrn, m);
         const int L = P.L;
         const float* __restrict__ dt0 = dtrn + P.toff;
         float* fb = a.fb + P.base;
+        float* bnd = a.bnd + (P.base / Lq) * 10;
+        const float* botr = bnd + ((s + 1) & 1) * 5 * L;   // last row of strip s-1
+        float* botw = bnd + (s & 1) * 5 * L;
+        int* pf = a.prog + (long long)m * nstrips;
         float maxF = 0.f;
-        float* botr = bot0;
-        float* botw = bot0 + 5 * Lmax;
-        for (int s = 0; s < nstrips; s++) {
+        {
             const int r = s * 32 + lane;
             const bool act = r < Lq;
             float q7[7];
@@ -164,10 +169,11 @@ __global__ void __launch_bounds__(MAPW * 32) map_fwd_kernel(MapArgs a, const flo
             for (int i = 0; i < 7; i++) t7[i] = MLOG0;
             float bcur[5], bnxt[5];
             const float binit[5] = {0.f, MLOG0, MLOG0, MLOG0, MLOG0};
+            if (s > 0) pipe_wait(pf + s - 1, min(64, L), lane, a.status, broken);
 #pragma unroll
             for (int f = 0; f < 5; f++) {
-                bcur[f] = (s > 0 && lane < L) ? botr[f * Lmax + lane] : binit[f];
-                bnxt[f] = (s > 0 && 32 + lane < L) ? botr[f * Lmax + 32 + lane] : binit[f];
+                bcur[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : binit[f];
+                bnxt[f] = (s > 0 && 32 + lane < L) ? __ldcg(botr + f * L + 32 + lane) : binit[f];
             }
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             for (int k = 0; k < L + 31; k++) {
@@ -197,11 +203,12 @@ __global__ void __launch_bounds__(MAPW * 32) map_fwd_kernel(MapArgs a, const flo
                     const float b4 = __shfl_sync(FULL, bcur[4], src);
                     if (lane == 0) up = S5{b0, b1, b2, b3, b4};
                     if (src == 31) {
+                        if (s > 0 && k + 33 < L) pipe_wait(pf + s - 1, min(k + 65, L), lane, a.status, broken);
 #pragma unroll
                         for (int f = 0; f < 5; f++) {
                             bcur[f] = bnxt[f];
                             const int cc = k + 33 + lane;
-                            bnxt[f] = (s > 0 && cc < L) ? botr[f * Lmax + cc] : binit[f];
+                            bnxt[f] = (s > 0 && cc < L) ? __ldcg(botr + f * L + cc) : binit[f];
                         }
                     }
                 }
@@ -224,8 +231,9 @@ __global__ void __launch_bounds__(MAPW * 32) map_fwd_kernel(MapArgs a, const flo
                     rout[j & 31][lane] = nw.MM;
                 }
                 if (wr_bot && j >= 0 && j < L) {
-                    botw[0 * Lmax + j] = nw.MM; botw[1 * Lmax + j] = nw.MI; botw[2 * Lmax + j] = nw.IM;
-                    botw[3 * Lmax + j] = nw.DN; botw[4 * Lmax + j] = nw.ND;
+                    botw[0 * L + j] = nw.MM; botw[1 * L + j] = nw.MI; botw[2 * L + j] = nw.IM;
+                    botw[3 * L + j] = nw.DN; botw[4 * L + j] = nw.ND;
+                    pipe_publish(pf + s, j, L);
                 }
                 mine = nw;
                 upp = up;
@@ -233,12 +241,11 @@ __global__ void __launch_bounds__(MAPW * 32) map_fwd_kernel(MapArgs a, const flo
                 if (cfl >= 0 && cfl < L && act) fb[(long long)cfl * Lq + r] = rout[cfl & 31][lane];
                 __syncwarp();
             }
-            float* t = botr; botr = botw; botw = t;
-            __syncwarp();
         }
 #pragma unroll
         for (int o = 16; o >= 1; o >>= 1) maxF = hmax(maxF, __shfl_xor_sync(FULL, maxF, o));
-        if (lane == 0) a.pairf[m * 4 + 0] = maxF;
+        // maxF >= 0, so its bit pattern orders as an unsigned integer
+        if (lane == 0) atomicMax(reinterpret_cast<unsigned*>(a.pairf + m * 4), __float_as_uint(maxF));
         __syncwarp();
     }
 }
@@ -264,7 +271,7 @@ __global__ void __launch_bounds__(256) map_z_kernel(MapArgs a)
 
 // ---------------------------------------------------------------------------
 // backward sweep on the mirrored matrix (row Lq-1-r', column L-1-j'); adds
-// B.MM to fb, giving F+B per cell
+// B.MM to fb, giving F+B per cell.  Work items are (pair, mirrored strip).
 __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const float* __restrict__ qtrn,
                                                       const float* __restrict__ dtrn)
 {
@@ -272,24 +279,26 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float(*rin)[33] = rings[wid][0];
     float(*rout)[33] = rings[wid][1];
-    const long long slot = (long long)blockIdx.x * MAPW + wid;
-    const int Lmax = (int)(a.botstride / 10);
-    float* bot0 = a.bot + slot * a.botstride;
     const int Lq = a.Lq;
     const int nstrips = (Lq + 31) >> 5;
+    const int nitems = a.nmap * nstrips;
     const S5 INIT = {0.f, MLOG0, MLOG0, MLOG0, MLOG0};
+    bool broken = false;
     for (;;) {
-        int m = 0;
-        if (lane == 0) m = atomicAdd(a.counter, 1);
-        m = __shfl_sync(FULL, m, 0);
-        if (m >= a.nmap) break;
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.counter, 1);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= nitems) break;
+        const int m = item / nstrips, s = item - m * nstrips;
         const MapPair P = map_pair(a, qtrn, m);
         const int L = P.L;
         const float* __restrict__ dt0 = dtrn + P.toff;
         float* fb = a.fb + P.base;
-        float* botr = bot0;
-        float* botw = bot0 + 5 * Lmax;
-        for (int s = 0; s < nstrips; s++) {
+        float* bnd = a.bnd + (P.base / Lq) * 10;
+        const float* botr = bnd + ((s + 1) & 1) * 5 * L;   // last row of mirrored strip s-1
+        float* botw = bnd + (s & 1) * 5 * L;
+        int* pf = a.prog + (long long)m * nstrips;
+        {
             const int rm = s * 32 + lane;       // mirrored row
             const int r = Lq - 1 - rm;          // actual row
             const bool act = rm < Lq;
@@ -301,10 +310,11 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
             for (int i = 0; i < 7; i++) t7[i] = MLOG0;
             float bcur[5], bnxt[5];
             const float binit[5] = {0.f, MLOG0, MLOG0, MLOG0, MLOG0};
+            if (s > 0) pipe_wait(pf + s - 1, min(64, L), lane, a.status, broken);
 #pragma unroll
             for (int f = 0; f < 5; f++) {
-                bcur[f] = (s > 0 && lane < L) ? botr[f * Lmax + lane] : binit[f];
-                bnxt[f] = (s > 0 && 32 + lane < L) ? botr[f * Lmax + 32 + lane] : binit[f];
+                bcur[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : binit[f];
+                bnxt[f] = (s > 0 && 32 + lane < L) ? __ldcg(botr + f * L + 32 + lane) : binit[f];
             }
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             for (int k = 0; k < L + 31; k++) {
@@ -340,11 +350,12 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
                     const float b4 = __shfl_sync(FULL, bcur[4], src);
                     if (lane == 0) dn = S5{b0, b1, b2, b3, b4};
                     if (src == 31) {
+                        if (s > 0 && k + 33 < L) pipe_wait(pf + s - 1, min(k + 65, L), lane, a.status, broken);
 #pragma unroll
                         for (int f = 0; f < 5; f++) {
                             bcur[f] = bnxt[f];
                             const int cc = k + 33 + lane;
-                            bnxt[f] = (s > 0 && cc < L) ? botr[f * Lmax + cc] : binit[f];
+                            bnxt[f] = (s > 0 && cc < L) ? __ldcg(botr + f * L + cc) : binit[f];
                         }
                     }
                 }
@@ -360,8 +371,9 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
                 nw.ND = lse2(((dg.MM + q7[TMM]) + t7[TDM]) + sco, rt.ND + t7[TDD]);
                 if (act && j >= 0 && j < L) rout[j & 31][lane] = nw.MM;
                 if (wr_bot && j >= 0 && j < L) {
-                    botw[0 * Lmax + j] = nw.MM; botw[1 * Lmax + j] = nw.MI; botw[2 * Lmax + j] = nw.IM;
-                    botw[3 * Lmax + j] = nw.DN; botw[4 * Lmax + j] = nw.ND;
+                    botw[0 * L + j] = nw.MM; botw[1 * L + j] = nw.MI; botw[2 * L + j] = nw.IM;
+                    botw[3 * L + j] = nw.DN; botw[4 * L + j] = nw.ND;
+                    pipe_publish(pf + s, j, L);
                 }
                 mine = nw;
                 upp = dn;
@@ -372,8 +384,6 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
                 }
                 __syncwarp();
             }
-            float* t = botr; botr = botw; botw = t;
-            __syncwarp();
         }
     }
 }
@@ -396,17 +406,17 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float(*rin)[33] = rings[wid];
     signed char(*bout)[33] = brings[wid];
-    const long long slot = (long long)blockIdx.x * MAPW + wid;
-    const int Lmax = (int)(a.botstride / 10);
-    float* bot0 = a.bot + slot * a.botstride;
     const int Lq = a.Lq;
     const int nstrips = (Lq + 31) >> 5;
+    const int nitems = a.nmap * nstrips;
     const float gap = a.minpp * 0.5f;
+    bool broken = false;
     for (;;) {
-        int m = 0;
-        if (lane == 0) m = atomicAdd(a.counter, 1);
-        m = __shfl_sync(FULL, m, 0);
-        if (m >= a.nmap) break;
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.counter, 1);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= nitems) break;
+        const int m = item / nstrips, s = item - m * nstrips;
         const int c = a.map_cand[m];
         const int p = a.cand_prof[c];
         const int L = a.plen[p];
@@ -415,16 +425,19 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
         signed char* bt = a.btck + base;
         const float logZ = a.pairf[m * 4 + 1];
         const int edge = corner_edge_m(Lq, L);
+        float* bnd = a.bnd + (base / Lq) * 10;
+        const float* botr = bnd + ((s + 1) & 1) * 5 * L;   // last row of strip s-1
+        float* botw = bnd + (s & 1) * 5 * L;
+        int* pf = a.prog + (long long)m * nstrips;
         float best = 0.f;
         int brow = 0x7fffffff, bcol = 0x7fffffff;
-        float* botr = bot0;
-        float* botw = bot0 + Lmax;
-        for (int s = 0; s < nstrips; s++) {
+        {
             const int r = s * 32 + lane;
             const bool act = r < Lq;
             float mine = 0.f, upp = 0.f;
-            float bcur = (s > 0 && lane < L) ? botr[lane] : 0.f;
-            float bnxt = (s > 0 && 32 + lane < L) ? botr[32 + lane] : 0.f;
+            if (s > 0) pipe_wait(pf + s - 1, min(64, L), lane, a.status, broken);
+            float bcur = (s > 0 && lane < L) ? __ldcg(botr + lane) : 0.f;
+            float bnxt = (s > 0 && 32 + lane < L) ? __ldcg(botr + 32 + lane) : 0.f;
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             for (int k = 0; k < L + 31; k++) {
                 if (k < L) rin[k & 31][lane] = act ? fb[(long long)k * Lq + r] : 0.f;
@@ -434,9 +447,10 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
                     const float b0 = __shfl_sync(FULL, bcur, src);
                     if (lane == 0) up = b0;
                     if (src == 31) {
+                        if (s > 0 && k + 33 < L) pipe_wait(pf + s - 1, min(k + 65, L), lane, a.status, broken);
                         bcur = bnxt;
                         const int cc = k + 33 + lane;
-                        bnxt = (s > 0 && cc < L) ? botr[cc] : 0.f;
+                        bnxt = (s > 0 && cc < L) ? __ldcg(botr + cc) : 0.f;
                     }
                 }
                 __syncwarp();
@@ -456,15 +470,16 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
                     if (v < left - gap) { v = left - gap; b = BT_LEFT; }
                 }
                 if (valid) bout[j & 31][lane] = (signed char)b;
-                if (wr_bot && j >= 0 && j < L) botw[j] = v;
+                if (wr_bot && j >= 0 && j < L) {
+                    botw[j] = v;
+                    pipe_publish(pf + s, j, L);
+                }
                 mine = v;
                 upp = up;
                 const int cfl = k - 31;
                 if (cfl >= 0 && cfl < L && act) bt[(long long)cfl * Lq + r] = bout[cfl & 31][lane];
                 __syncwarp();
             }
-            float* t = botr; botr = botw; botw = t;
-            __syncwarp();
         }
 #pragma unroll
         for (int o = 16; o >= 1; o >>= 1) {
@@ -475,9 +490,13 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
                 best = ob; brow = orr; bcol = oc;
             }
         }
-        if (lane == 0) {
-            a.pairf[m * 4 + 2] = best;
-            a.pairc[m] = (best > 0.f) ? (((unsigned)bcol << 16) | ((unsigned)brow & 0xffffu)) : 0u;
+        // pair maximum over strips: largest value, then smallest row, then
+        // smallest column, as one 64-bit key (best >= 0 orders by its bits)
+        if (lane == 0 && best > 0.f) {
+            const unsigned cell = ((unsigned)brow << 16) | ((unsigned)bcol & 0xffffu);
+            const unsigned long long key =
+                ((unsigned long long)__float_as_uint(best) << 32) | (unsigned long long)(0xffffffffu - cell);
+            atomicMax(a.pairk + m, key);
         }
         __syncwarp();
     }
@@ -498,7 +517,13 @@ __global__ void map_tb_kernel(MapArgs a)
     const long long base = a.cand_off[c];
     const signed char* bt = a.btck + base;
     const float* sm = a.smat + base;
-    const unsigned xx = a.pairc[m];
+    // MAP DP maximum and its cell from the packed key (0: no positive cell)
+    const unsigned long long key = a.pairk[m];
+    const float mbest = __uint_as_float((unsigned)(key >> 32));
+    const unsigned cell = 0xffffffffu - (unsigned)(key & 0xffffffffu);
+    const unsigned xx = (key != 0ull) ? (((cell & 0xffffu) << 16) | (cell >> 16)) : 0u;
+    a.pairf[m * 4 + 2] = mbest;
+    a.pairc[m] = xx;
     int x = (int)(xx >> 16), y = (int)(xx & 0xffff);
     char* o = a.aln + (size_t)m * 5 * a.alnstride;
     char *tq = o, *tm = o + a.alnstride, *tt = o + 2 * a.alnstride, *sq = o + 3 * a.alnstride,
@@ -553,15 +578,26 @@ cudaError_t launch_map(const MapArgs& a, const float* qtrn, const float* dtrn, c
                        int* counter, cudaStream_t st, int* nlaunch)
 {
     if (a.nmap <= 0) return cudaSuccess;
-    // grid = number of CTAs of MAPW warps that the boundary scratch has slots for
-    const int g = min(grid, (a.nmap + MAPW - 1) / MAPW);
+    const int nstrips = (a.Lq + 31) >> 5;
+    const long long nitems = (long long)a.nmap * nstrips;
+    // grid: persistent CTAs of MAPW warps, at most one warp per work item
+    const int g = (int)std::min<long long>(grid, (nitems + MAPW - 1) / MAPW);
+    const size_t progb = (size_t)nitems * sizeof(int);
     cudaError_t e;
-    if ((e = cudaMemsetAsync(counter, 0, sizeof(int), st)) != cudaSuccess) return e;
+    // per sweep: fresh work counter and strip progress words
+    auto reset = [&]() -> cudaError_t {
+        cudaError_t r = cudaMemsetAsync(counter, 0, sizeof(int), st);
+        if (r == cudaSuccess) r = cudaMemsetAsync(a.prog, 0, progb, st);
+        return r;
+    };
+    if ((e = cudaMemsetAsync(a.pairf, 0, (size_t)a.nmap * 4 * sizeof(float), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(a.pairk, 0, (size_t)a.nmap * sizeof(unsigned long long), st)) != cudaSuccess) return e;
+    if ((e = reset()) != cudaSuccess) return e;
     map_fwd_kernel<<<g, MAPW * 32, 0, st>>>(a, qtrn, dtrn, qcf);
     map_z_kernel<<<(a.nmap + 7) / 8, 256, 0, st>>>(a);
-    if ((e = cudaMemsetAsync(counter, 0, sizeof(int), st)) != cudaSuccess) return e;
+    if ((e = reset()) != cudaSuccess) return e;
     map_bwd_kernel<<<g, MAPW * 32, 0, st>>>(a, qtrn, dtrn);
-    if ((e = cudaMemsetAsync(counter, 0, sizeof(int), st)) != cudaSuccess) return e;
+    if ((e = reset()) != cudaSuccess) return e;
     map_dp_kernel<<<g, MAPW * 32, 0, st>>>(a);
     map_tb_kernel<<<(a.nmap + 31) / 32, 32, 0, st>>>(a);
     *nlaunch += 5;

@@ -52,8 +52,10 @@ struct MapArgs {
     signed char* btck;          // [L][Lq] per candidate: MAP traceback codes
     float* pairf;               // [nmap][4]: maxF, logZ, map max, (unused)
     unsigned* pairc;            // [nmap]: MAP end coordinates
-    float* bot;                 // per warp slot: strip boundary rows (5 x Lmax x 2)
-    long long botstride;
+    float* bnd;                 // per candidate at 10 x (cand_off / Lq): two last-row buffers [5][L]
+    int* prog;                  // [ncand][nstrips] finished columns per strip
+    unsigned long long* pairk;  // [nmap] MAP DP maximum and end cell, packed for atomicMax
+    int* status;
     int* counter;
     float minpp;
     int modscores;
