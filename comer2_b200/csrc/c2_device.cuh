@@ -52,6 +52,15 @@ constexpr int REC_CHUNK = 8, REC_CHUNK_LOG = 3, REC_SLOTS = 16;
 // shared memory per warp: score ring [32][32], SS row table [32][32], record ring
 constexpr int P1_WARP_FLOATS = 32 * 32 + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE;
 constexpr int MAX_CVCARD = 256;
+// chunked phase-1 kernel: 12 warps per CTA, one CTA per SM; per warp a score
+// ring of 64 columns x 32 rows, a transition ring of 64 columns (stride 9
+// floats: per-lane reads of different columns hit different banks), the SS
+// row table and the record staging ring
+constexpr int P1C_WARPS = 12;
+// phase-1 kernel variants of launch_p1
+enum : int { P1K_STRIP = 0, P1K_CHUNKED = 1, P1K_TRACEBACK = 2 };
+constexpr int P1C_RING = 64, P1C_TRS = 9, P1C_CVREP = 16;
+constexpr int P1C_WARP_FLOATS = P1C_RING * 32 + P1C_RING * P1C_TRS + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE;
 
 struct P1Args {
     const float* qrec;      // [Lq][QR_STRIDE]

@@ -25,8 +25,9 @@ cudaError_t launch_stats(const StatsArgs& a, cudaStream_t st);
 cudaError_t launch_map(const MapArgs& a, const float* qtrn, const float* dtrn, const float* qcf, int grid,
                        int* counter, cudaStream_t st, int* nlaunch);
 size_t p1_smem_bytes(int cvcard);
-cudaError_t launch_p1(const P1Args& a, const float* qbkg, bool tb, int grid, cudaStream_t st);
+cudaError_t launch_p1(const P1Args& a, const float* qbkg, int which, int grid, cudaStream_t st);
 int p1_blocks_per_sm(int cvcard);
+int p1c_blocks_per_sm(int cvcard);
 cudaError_t launch_fin(const FinArgs& a, cudaStream_t st);
 }  // namespace c2
 
@@ -555,7 +556,12 @@ extern "C" c2_status c2_run_phase1(c2_handle* h)
     a.nwork = h->nprof;
     a.order = h->d_order.p;
     CK(cudaMemsetAsync(h->d_counter.p, 0, sizeof(int), h->stream));
-    CK(launch_p1(a, h->d_qbkg.p, false, h->grid, h->stream));
+    // chunked kernel: one 12-warp CTA per SM, within the boundary-row slots
+    // allocated for the strip kernel's grid (h->grid x P1_WARPS)
+    int gc = h->nsm * p1c_blocks_per_sm(h->sc.cvcard);
+    if (gc < 1) return fail(h, C2_ERR_CUDA, "phase-1 kernel does not fit on an SM");
+    gc = std::min(gc, h->grid * P1_WARPS / P1C_WARPS);
+    CK(launch_p1(a, h->d_qbkg.p, P1K_CHUNKED, gc, h->stream));
     h->launches++;
     return C2_OK;
 }
@@ -634,7 +640,7 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     CK(cudaMemsetAsync(h->d_tbbest.p, 0, (size_t)nc * sizeof(float), h->stream));
     // one warp per (candidate, strip) work item at most
     const int grid = (int)std::min<long long>(h->grid, (nitems + P1_WARPS - 1) / P1_WARPS);
-    CK(launch_p1(a, h->d_qbkg.p, true, grid, h->stream));
+    CK(launch_p1(a, h->d_qbkg.p, P1K_TRACEBACK, grid, h->stream));
     h->launches++;
     FinArgs f;
     f.Lq = h->Lq;
@@ -967,7 +973,7 @@ extern "C" c2_status c2_run_phase1_static(c2_handle* h, float* d_best, uint32_t*
     a.best = d_best;
     a.coords = d_coords;
     CK(cudaMemsetAsync(base, 0, sizeof(int), h->stream));
-    CK(launch_p1(a, h->d_qbkg.p, false, grid, h->stream));
+    CK(launch_p1(a, h->d_qbkg.p, P1K_STRIP, grid, h->stream));
     h->launches++;
     return C2_OK;
 }

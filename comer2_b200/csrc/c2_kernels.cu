@@ -51,6 +51,9 @@ struct RowOps {
     float cq, pq, hq;
 };
 
+// cvtab holds each CV map value CVREP times ([cvcard][CVREP]); a lane reads
+// replica lane % CVREP so that lanes reading different entries rarely share a bank.
+template <int CVREP>
 __device__ __forceinline__ float cell_score(const RowOps& R, const float4* __restrict__ rp,
                                             const float* __restrict__ U, const float* __restrict__ cvtab,
                                             const ScoreConsts& sc, int lane, float& mod_out)
@@ -94,7 +97,7 @@ __device__ __forceinline__ float cell_score(const RowOps& R, const float4* __res
     else {
         // clamp keeps the shared-memory read in bounds for any table/argument
         const int ix = min(max(sc.cvshift + (int)rintf(2.f * cvs), 0), sc.cvcard - 1);
-        cvm = cvtab[ix * 32 + lane];
+        cvm = cvtab[ix * CVREP + (lane & (CVREP - 1))];
     }
     cvm *= sc.cvswgt;
     // SS term
@@ -242,7 +245,7 @@ p1_kernel(P1Args a, const float* __restrict__ qbkg)
                 if (k < L) {
                     const float4* rp = reinterpret_cast<const float4*>(rec + (k & (REC_SLOTS - 1)) * DR_STRIDE);
                     float mod;
-                    float S = cell_score(R, rp, U, cvtab, sc, lane, mod);
+                    float S = cell_score<32>(R, rp, U, cvtab, sc, lane, mod);
                     if (!act) S = -9.f;
                     ring[(k & 31) * 32 + lane] = S;
                     const float4 ta = rp[12], tb = rp[13];
@@ -453,7 +456,7 @@ p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
                 if (k < L) {
                     const float4* rp = reinterpret_cast<const float4*>(rec + (k & (REC_SLOTS - 1)) * DR_STRIDE);
                     float mod;
-                    float S = cell_score(R, rp, U, cvtab, sc, lane, mod);
+                    float S = cell_score<32>(R, rp, U, cvtab, sc, lane, mod);
                     if (!act) S = -9.f;
                     ring[(k & 31) * 32 + lane] = S;
                     if (act) {
@@ -557,6 +560,243 @@ p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
 }
 
 
+// ---------------------------------------------------------------------------
+// Phase 1, chunked: the same arithmetic as p1_kernel, scheduled in chunks of
+// 32 db columns.  Per chunk, every lane first scores its query row against
+// the 32 columns (independent cells: the FMA chains of consecutive columns
+// overlap), writing scores and the columns' DP transitions to shared-memory
+// rings; then the warp advances the anti-diagonal wavefront by 32 steps.
+// Wavefront steps whose 32 cells all lie inside the matrix (every chunk but
+// the first and the last ones of a strip) run without bounds checks.
+struct DPLane {
+    St5 mine, upp;           // own state at the previous step, up-state of the previous step
+    float q7[7];             // row transitions
+    float bcur[5], bnxt[5];  // row above the strip: columns [32m, 32m+32) and the next 32
+    float best;
+    int kbest;
+};
+
+template <bool CHECK>
+__device__ __forceinline__ void p1c_steps(DPLane& D, int k0, int k1, int lane, int L, bool act, int cA, int cB,
+                                          const float* __restrict__ ring, const float* __restrict__ trn,
+                                          const St5& LB, const St5& DB, bool wr_bot, float* __restrict__ botw,
+                                          int Lmax)
+{
+#pragma unroll 4
+    for (int k = k0; k < k1; k++) {
+        const int j = k - lane;
+        const int slot = j & (P1C_RING - 1);
+        float S = ring[slot * 32 + lane];
+        if (j <= cA || j >= cB) S = -9.f;   // corner cells (CellYXinCorners)
+        float t7[7];
+#pragma unroll
+        for (int i = 0; i < 7; i++) t7[i] = trn[slot * P1C_TRS + i];
+        St5 up;
+        up.MM = __shfl_up_sync(FULL, D.mine.MM, 1);
+        up.MI = __shfl_up_sync(FULL, D.mine.MI, 1);
+        up.IM = __shfl_up_sync(FULL, D.mine.IM, 1);
+        up.DN = __shfl_up_sync(FULL, D.mine.DN, 1);
+        up.ND = __shfl_up_sync(FULL, D.mine.ND, 1);
+        {
+            // row above the strip at column k (lane 0's column)
+            const int src = k & 31;
+            const float b0 = __shfl_sync(FULL, D.bcur[0], src);
+            const float b1 = __shfl_sync(FULL, D.bcur[1], src);
+            const float b2 = __shfl_sync(FULL, D.bcur[2], src);
+            const float b3 = __shfl_sync(FULL, D.bcur[3], src);
+            const float b4 = __shfl_sync(FULL, D.bcur[4], src);
+            if (lane == 0) up = St5{b0, b1, b2, b3, b4};
+        }
+        St5 left = D.mine, diag = D.upp;
+        if (CHECK && j == 0) { left = LB; diag = DB; }
+        const float* q7 = D.q7;
+        St5 nw;
+        {
+            float v = fmaxf((diag.MI + q7[TMM]) + t7[TIM], (diag.IM + q7[TIM]) + t7[TMM]);
+            v = fmaxf(v, (diag.DN + q7[TDM]) + t7[TMM]);
+            v = fmaxf(v, (diag.ND + q7[TMM]) + t7[TDM]);
+            v = fmaxf(v, (diag.MM + q7[TMM]) + t7[TMM]);
+            nw.MM = fmaxf(v + S, 0.f);
+            nw.MI = fmaxf((up.MM + q7[TMM]) + t7[TMI], (up.MI + q7[TMM]) + t7[TII]);
+            nw.IM = fmaxf((left.MM + q7[TMI]) + t7[TMM], (left.IM + q7[TII]) + t7[TMM]);
+            nw.DN = fmaxf(up.MM + q7[TMD], up.DN + q7[TDD]);
+            nw.ND = fmaxf(left.MM + t7[TMD], left.ND + t7[TDD]);
+        }
+        const bool inm = !CHECK || (j >= 0 && j < L);
+        if (act && inm && nw.MM > D.best) { D.best = nw.MM; D.kbest = k; }
+        if (wr_bot && inm) {
+            botw[0 * Lmax + j] = nw.MM;
+            botw[1 * Lmax + j] = nw.MI;
+            botw[2 * Lmax + j] = nw.IM;
+            botw[3 * Lmax + j] = nw.DN;
+            botw[4 * Lmax + j] = nw.ND;
+        }
+        D.mine = nw;
+        D.upp = up;
+    }
+}
+
+__global__ void __launch_bounds__(P1C_WARPS * 32, 1)
+p1c_kernel(P1Args a, const float* __restrict__ qbkg)
+{
+    extern __shared__ float smem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int cvcard = a.sc.cvcard;
+    const int card = a.sc.ssss_card;
+    float* cvtab = smem;                                      // [cvcard][P1C_CVREP]
+    float* wb = smem + cvcard * P1C_CVREP + wid * P1C_WARP_FLOATS;
+    float* ring = wb;                                         // [P1C_RING][32] scores
+    float* trn = ring + P1C_RING * 32;                        // [P1C_RING][P1C_TRS] transitions
+    float* U = trn + P1C_RING * P1C_TRS;                      // [card][32]
+    float* rec = U + MAX_SSSS_CARD * 32;                      // [REC_SLOTS][DR_STRIDE] db records
+    for (int i = threadIdx.x; i < cvcard * P1C_CVREP; i += blockDim.x) cvtab[i] = a.cvvals[i / P1C_CVREP];
+    __syncthreads();
+
+    const long long slotw = (long long)blockIdx.x * P1C_WARPS + wid;
+    const int Lmax = (int)(a.botstride / 10);
+    float* bot0 = a.bot + slotw * a.botstride;
+    const int Lq = a.Lq;
+    const int nstrips = (Lq + 31) >> 5;
+    const ScoreConsts sc = a.sc;
+
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.counter, 1);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= a.nwork) break;
+        const int p = a.order[item];
+        const int L = a.plen[p];
+        const long long off = a.poff[p];
+        const float* __restrict__ dr = a.drec + off * DR_STRIDE;
+        const float* __restrict__ bd = a.pbkg + (long long)p * NAA;
+        const int edge = corner_edge(Lq, L);
+        float* botr = bot0;
+        float* botw = bot0 + 5 * Lmax;
+        float pbest = 0.f;
+        int prow = 0x7fffffff, pcol = 0x7fffffff;
+
+        for (int s = 0; s < nstrips; s++) {
+            const int r = s * 32 + lane;
+            const bool act = r < Lq;
+            const float* __restrict__ qr = a.qrec + (long long)(act ? r : Lq - 1) * QR_STRIDE;
+            RowOps R;
+#pragma unroll
+            for (int i = 0; i < NAA; i++)
+                R.Qt[i] = __fdividef(qr[QR_TRG + i], 0.5f * (qbkg[i] + bd[i]));
+#pragma unroll
+            for (int i = 0; i < NCV; i++) R.qcv[i] = qr[QR_CV + i];
+            R.cq = qr[QR_CN];
+            R.pq = qr[QR_PRIOR];
+            R.hq = qr[QR_HQ];
+            {
+                const float q0 = qr[QR_SS], q1 = qr[QR_SS + 1], q2 = qr[QR_SS + 2];
+                const int i0 = (int)(q0 * 9.999f), i1 = 10 + (int)(q1 * 9.999f), i2 = 20 + (int)(q2 * 9.999f);
+                for (int c = 0; c < card; c++)
+                    U[c * 32 + lane] = q0 * __ldg(a.ssss + i0 * card + c) + q1 * __ldg(a.ssss + i1 * card + c) +
+                                       q2 * __ldg(a.ssss + i2 * card + c);
+            }
+            DPLane D;
+#pragma unroll
+            for (int i = 0; i < 7; i++) D.q7[i] = act ? qr[QR_TRN + i] : LOG0;
+            // column -1 boundary states of this row and of the row above
+            const bool z_left = (lane == 31);
+            const bool z_diag = (lane == 31 || lane == 0);
+            const St5 LB = z_left ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
+                                  : St5{0.f, qr[QR_C + 0], qr[QR_C + 1], qr[QR_C + 2], LOG0};
+            const St5 DB = z_diag ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
+                                  : St5{0.f, qr[QR_CP + 0], qr[QR_CP + 1], qr[QR_CP + 2], LOG0};
+            // corner cells of this row: j <= cA or j >= cB
+            const int cA = (Lq <= r + edge) ? edge + r - Lq : -1;
+            const int cB = (r < edge) ? L - edge + r : 0x7fffffff;
+            D.mine = St5{0.f, 0.f, 0.f, 0.f, 0.f};
+            D.upp = D.mine;
+            D.best = 0.f;
+            D.kbest = 0;
+#pragma unroll
+            for (int f = 0; f < 5; f++) {
+                D.bcur[f] = 0.f;
+                D.bnxt[f] = 0.f;
+                if (s > 0) {
+                    if (lane < L) D.bcur[f] = botr[f * Lmax + lane];
+                    if (32 + lane < L) D.bnxt[f] = botr[f * Lmax + 32 + lane];
+                }
+            }
+            const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
+            __syncwarp();
+            stage_chunk(rec, dr, 0, L, lane);
+            stage_chunk(rec, dr, 1, L, lane);
+            const int nch = (L + 31) >> 5;        // chunks holding columns
+            const int kend = L + 31;              // wavefront steps of the strip
+            for (int m = 0; 32 * m < kend; m++) {
+                // ---- score stage: columns [32m, min(32m + 32, L))
+                if (m < nch) {
+                    const int c0 = 32 * m, c1 = min(c0 + 32, L);
+                    for (int c = c0; c < c1; c++) {
+                        if ((c & (REC_CHUNK - 1)) == 0) {
+                            cp_async_wait_1();
+                            __syncwarp();
+                        }
+                        const float* rc = rec + (c & (REC_SLOTS - 1)) * DR_STRIDE;
+                        float mod;
+                        float Sc = cell_score<P1C_CVREP>(R, reinterpret_cast<const float4*>(rc), U, cvtab, sc, lane, mod);
+                        (void)mod;
+                        const int slot = c & (P1C_RING - 1);
+                        ring[slot * 32 + lane] = Sc;
+                        if (lane < 7) trn[slot * P1C_TRS + lane] = rc[DR_TRN + lane];
+                        if ((c & (REC_CHUNK - 1)) == REC_CHUNK - 1) {
+                            // group fully read by every lane: refill its slots two groups ahead
+                            __syncwarp();
+                            stage_chunk(rec, dr, (c >> REC_CHUNK_LOG) + 2, L, lane);
+                        }
+                    }
+                }
+                __syncwarp();
+                // ---- DP stage: wavefront steps [32m, 32m + 32)
+                const int k0 = 32 * m, k1 = min(k0 + 32, kend);
+                if (m >= 1 && k0 + 31 < L && k1 == k0 + 32)
+                    p1c_steps<false>(D, k0, k1, lane, L, act, cA, cB, ring, trn, LB, DB, wr_bot, botw, Lmax);
+                else
+                    p1c_steps<true>(D, k0, k1, lane, L, act, cA, cB, ring, trn, LB, DB, wr_bot, botw, Lmax);
+                // next 32 columns of the row above the strip
+#pragma unroll
+                for (int f = 0; f < 5; f++) {
+                    D.bcur[f] = D.bnxt[f];
+                    const int cc = k0 + 64 + lane;
+                    D.bnxt[f] = (s > 0 && cc < L) ? botr[f * Lmax + cc] : 0.f;
+                }
+                __syncwarp();
+            }
+            cp_async_wait_all();
+            // this strip's maximum: largest score, then smallest row, then smallest column
+            {
+                float b = D.best;
+                int rr = (D.best > 0.f) ? r : 0x7fffffff;
+                int cc = (D.best > 0.f) ? D.kbest - lane : 0x7fffffff;
+                if (b > pbest || (b == pbest && (rr < prow || (rr == prow && cc < pcol)))) {
+                    pbest = b; prow = rr; pcol = cc;
+                }
+            }
+            float* t = botr; botr = botw; botw = t;
+            __syncwarp();
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            const float ob = __shfl_xor_sync(FULL, pbest, o);
+            const int orr = __shfl_xor_sync(FULL, prow, o);
+            const int oc = __shfl_xor_sync(FULL, pcol, o);
+            if (ob > pbest || (ob == pbest && (orr < prow || (orr == prow && oc < pcol)))) {
+                pbest = ob; prow = orr; pcol = oc;
+            }
+        }
+        if (lane == 0) {
+            const unsigned xy = (pbest > 0.f) ? (((unsigned)pcol << 16) | ((unsigned)prow & 0xffffu)) : 0u;
+            a.best[p] = pbest;
+            a.coords[p] = xy;
+        }
+        __syncwarp();
+    }
+}
+
 // Warp butterfly sum as the reference's FinalizeDPPro reduction
 // (src/libmycu/cudp/CuBatchDP_final.cu:254-260).
 __device__ __forceinline__ float warp_butterfly(float v)
@@ -637,15 +877,35 @@ __global__ void __launch_bounds__(256) fin_kernel(FinArgs a)
 
 // ---------------------------------------------------------------------------
 // launchers (host)
+size_t p1c_smem_bytes(int cvcard)
+{
+    return (size_t)(cvcard * P1C_CVREP + P1C_WARPS * P1C_WARP_FLOATS) * sizeof(float);
+}
+
+int p1c_blocks_per_sm(int cvcard)
+{
+    int n = 0;
+    const size_t sm = p1c_smem_bytes(cvcard);
+    cudaFuncSetAttribute(p1c_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, p1c_kernel, P1C_WARPS * 32, sm);
+    return n;
+}
+
 size_t p1_smem_bytes(int cvcard)
 {
     return (size_t)(cvcard * 32 + P1_WARPS * P1_WARP_FLOATS) * sizeof(float);
 }
 
-cudaError_t launch_p1(const P1Args& a, const float* qbkg, bool tb, int grid, cudaStream_t st)
+cudaError_t launch_p1(const P1Args& a, const float* qbkg, int which, int grid, cudaStream_t st)
 {
+    if (which == P1K_CHUNKED) {
+        const size_t sm = p1c_smem_bytes(a.sc.cvcard);
+        cudaFuncSetAttribute(p1c_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        p1c_kernel<<<grid, P1C_WARPS * 32, sm, st>>>(a, qbkg);
+        return cudaGetLastError();
+    }
     const size_t sm = p1_smem_bytes(a.sc.cvcard);
-    if (tb) {
+    if (which == P1K_TRACEBACK) {
         cudaFuncSetAttribute(p1tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         p1tb_kernel<<<grid, P1_WARPS * 32, sm, st>>>(a, qbkg);
     } else {
