@@ -52,15 +52,17 @@ constexpr int REC_CHUNK = 8, REC_CHUNK_LOG = 3, REC_SLOTS = 16;
 // shared memory per warp: score ring [32][32], SS row table [32][32], record ring
 constexpr int P1_WARP_FLOATS = 32 * 32 + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE;
 constexpr int MAX_CVCARD = 256;
-// chunked phase-1 kernel: 12 warps per CTA, one CTA per SM; per warp a score
-// ring of 64 columns x 32 rows, a transition ring of 64 columns (stride 9
-// floats: per-lane reads of different columns hit different banks), the SS
-// row table and the record staging ring
-constexpr int P1C_WARPS = 12;
+// chunked phase-1 kernel: 11 warps per CTA, one CTA per SM; per warp a score
+// ring of 64 columns x 32 rows, a transition ring of 64 columns (stride 12
+// floats: the two 16-byte reads of 8 lanes at consecutive columns cover 32
+// distinct banks), the SS row table, the record staging ring and the row
+// above the strip for the current chunk ([32][8])
+constexpr int P1C_WARPS = 11;
 // phase-1 kernel variants of launch_p1
 enum : int { P1K_STRIP = 0, P1K_CHUNKED = 1, P1K_TRACEBACK = 2 };
-constexpr int P1C_RING = 64, P1C_TRS = 9, P1C_CVREP = 16;
-constexpr int P1C_WARP_FLOATS = P1C_RING * 32 + P1C_RING * P1C_TRS + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE;
+constexpr int P1C_RING = 64, P1C_TRS = 12, P1C_CVREP = 16;
+constexpr int P1C_WARP_FLOATS =
+    P1C_RING * 32 + P1C_RING * P1C_TRS + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE + 32 * 8;
 
 struct P1Args {
     const float* qrec;      // [Lq][QR_STRIDE]

@@ -556,7 +556,7 @@ extern "C" c2_status c2_run_phase1(c2_handle* h)
     a.nwork = h->nprof;
     a.order = h->d_order.p;
     CK(cudaMemsetAsync(h->d_counter.p, 0, sizeof(int), h->stream));
-    // chunked kernel: one 12-warp CTA per SM, within the boundary-row slots
+    // chunked kernel: one CTA of P1C_WARPS warps per SM, within the boundary-row slots
     // allocated for the strip kernel's grid (h->grid x P1_WARPS)
     int gc = h->nsm * p1c_blocks_per_sm(h->sc.cvcard);
     if (gc < 1) return fail(h, C2_ERR_CUDA, "phase-1 kernel does not fit on an SM");

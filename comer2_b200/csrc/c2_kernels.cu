@@ -571,7 +571,7 @@ p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
 struct DPLane {
     St5 mine, upp;           // own state at the previous step, up-state of the previous step
     float q7[7];             // row transitions
-    float bcur[5], bnxt[5];  // row above the strip: columns [32m, 32m+32) and the next 32
+    float bnxt[5];           // row above the strip: columns [32m+32, 32m+64) (lane i: column 32m+32+i)
     float best;
     int kbest;
 };
@@ -579,8 +579,8 @@ struct DPLane {
 template <bool CHECK>
 __device__ __forceinline__ void p1c_steps(DPLane& D, int k0, int k1, int lane, int L, bool act, int cA, int cB,
                                           const float* __restrict__ ring, const float* __restrict__ trn,
-                                          const St5& LB, const St5& DB, bool wr_bot, float* __restrict__ botw,
-                                          int Lmax)
+                                          const float* __restrict__ bnd, const St5& LB, const St5& DB, bool wr_bot,
+                                          float* __restrict__ botw, int Lmax)
 {
 #pragma unroll 4
     for (int k = k0; k < k1; k++) {
@@ -589,8 +589,12 @@ __device__ __forceinline__ void p1c_steps(DPLane& D, int k0, int k1, int lane, i
         float S = ring[slot * 32 + lane];
         if (j <= cA || j >= cB) S = -9.f;   // corner cells (CellYXinCorners)
         float t7[7];
-#pragma unroll
-        for (int i = 0; i < 7; i++) t7[i] = trn[slot * P1C_TRS + i];
+        {
+            const float4 ta = *reinterpret_cast<const float4*>(trn + slot * P1C_TRS);
+            const float4 tb = *reinterpret_cast<const float4*>(trn + slot * P1C_TRS + 4);
+            t7[0] = ta.x; t7[1] = ta.y; t7[2] = ta.z; t7[3] = ta.w;
+            t7[4] = tb.x; t7[5] = tb.y; t7[6] = tb.z;
+        }
         St5 up;
         up.MM = __shfl_up_sync(FULL, D.mine.MM, 1);
         up.MI = __shfl_up_sync(FULL, D.mine.MI, 1);
@@ -598,14 +602,10 @@ __device__ __forceinline__ void p1c_steps(DPLane& D, int k0, int k1, int lane, i
         up.DN = __shfl_up_sync(FULL, D.mine.DN, 1);
         up.ND = __shfl_up_sync(FULL, D.mine.ND, 1);
         {
-            // row above the strip at column k (lane 0's column)
-            const int src = k & 31;
-            const float b0 = __shfl_sync(FULL, D.bcur[0], src);
-            const float b1 = __shfl_sync(FULL, D.bcur[1], src);
-            const float b2 = __shfl_sync(FULL, D.bcur[2], src);
-            const float b3 = __shfl_sync(FULL, D.bcur[3], src);
-            const float b4 = __shfl_sync(FULL, D.bcur[4], src);
-            if (lane == 0) up = St5{b0, b1, b2, b3, b4};
+            // row above the strip at column k (lane 0's column), broadcast reads
+            const float4 ba = *reinterpret_cast<const float4*>(bnd + (k & 31) * 8);
+            const float b4 = bnd[(k & 31) * 8 + 4];
+            if (lane == 0) up = St5{ba.x, ba.y, ba.z, ba.w, b4};
         }
         St5 left = D.mine, diag = D.upp;
         if (CHECK && j == 0) { left = LB; diag = DB; }
@@ -649,6 +649,7 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
     float* trn = ring + P1C_RING * 32;                        // [P1C_RING][P1C_TRS] transitions
     float* U = trn + P1C_RING * P1C_TRS;                      // [card][32]
     float* rec = U + MAX_SSSS_CARD * 32;                      // [REC_SLOTS][DR_STRIDE] db records
+    float* bnd = rec + REC_SLOTS * DR_STRIDE;                 // [32][8] row above the strip
     for (int i = threadIdx.x; i < cvcard * P1C_CVREP; i += blockDim.x) cvtab[i] = a.cvvals[i / P1C_CVREP];
     __syncthreads();
 
@@ -712,17 +713,21 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
             D.upp = D.mine;
             D.best = 0.f;
             D.kbest = 0;
+            float bc[5];
 #pragma unroll
             for (int f = 0; f < 5; f++) {
-                D.bcur[f] = 0.f;
+                bc[f] = 0.f;
                 D.bnxt[f] = 0.f;
                 if (s > 0) {
-                    if (lane < L) D.bcur[f] = botr[f * Lmax + lane];
+                    if (lane < L) bc[f] = botr[f * Lmax + lane];
                     if (32 + lane < L) D.bnxt[f] = botr[f * Lmax + 32 + lane];
                 }
             }
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             __syncwarp();
+            // columns [0, 32) of the row above, lane i holding column i
+            *reinterpret_cast<float4*>(bnd + lane * 8) = make_float4(bc[0], bc[1], bc[2], bc[3]);
+            bnd[lane * 8 + 4] = bc[4];
             stage_chunk(rec, dr, 0, L, lane);
             stage_chunk(rec, dr, 1, L, lane);
             const int nch = (L + 31) >> 5;        // chunks holding columns
@@ -754,13 +759,15 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
                 // ---- DP stage: wavefront steps [32m, 32m + 32)
                 const int k0 = 32 * m, k1 = min(k0 + 32, kend);
                 if (m >= 1 && k0 + 31 < L && k1 == k0 + 32)
-                    p1c_steps<false>(D, k0, k1, lane, L, act, cA, cB, ring, trn, LB, DB, wr_bot, botw, Lmax);
+                    p1c_steps<false>(D, k0, k1, lane, L, act, cA, cB, ring, trn, bnd, LB, DB, wr_bot, botw, Lmax);
                 else
-                    p1c_steps<true>(D, k0, k1, lane, L, act, cA, cB, ring, trn, LB, DB, wr_bot, botw, Lmax);
+                    p1c_steps<true>(D, k0, k1, lane, L, act, cA, cB, ring, trn, bnd, LB, DB, wr_bot, botw, Lmax);
+                __syncwarp();
                 // next 32 columns of the row above the strip
+                *reinterpret_cast<float4*>(bnd + lane * 8) = make_float4(D.bnxt[0], D.bnxt[1], D.bnxt[2], D.bnxt[3]);
+                bnd[lane * 8 + 4] = D.bnxt[4];
 #pragma unroll
                 for (int f = 0; f < 5; f++) {
-                    D.bcur[f] = D.bnxt[f];
                     const int cc = k0 + 64 + lane;
                     D.bnxt[f] = (s > 0 && cc < L) ? botr[f * Lmax + cc] : 0.f;
                 }

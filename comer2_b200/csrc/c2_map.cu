@@ -176,11 +176,20 @@ __global__ void __launch_bounds__(MAPW * 32) map_fwd_kernel(MapArgs a, const flo
                 bnxt[f] = (s > 0 && 32 + lane < L) ? __ldcg(botr + f * L + 32 + lane) : binit[f];
             }
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
+            // column k's score and transitions are loaded one step ahead
+            float nsc = act ? map_score(a, P, r) : MLOG0;
+            float ntc[7];
+            trn_fwd(dt0, 0, L, ntc);
             for (int k = 0; k < L + 31; k++) {
                 float tc[7];
                 if (k < L) {
-                    rin[k & 31][lane] = act ? map_score(a, P, (long long)k * Lq + r) : MLOG0;
-                    trn_fwd(dt0, k, L, tc);
+                    rin[k & 31][lane] = nsc;
+#pragma unroll
+                    for (int i = 0; i < 7; i++) tc[i] = ntc[i];
+                    if (k + 1 < L) {
+                        nsc = act ? map_score(a, P, (long long)(k + 1) * Lq + r) : MLOG0;
+                        trn_fwd(dt0, k + 1, L, ntc);
+                    }
                 } else {
 #pragma unroll
                     for (int i = 0; i < 7; i++) tc[i] = MLOG0;
@@ -317,6 +326,13 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
                 bnxt[f] = (s > 0 && 32 + lane < L) ? __ldcg(botr + f * L + 32 + lane) : binit[f];
             }
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
+            const bool hasdn = act && r + 1 < Lq;
+            // loads of mirrored column k (diagonal-successor score, transitions,
+            // and the F value to add B to) are issued one step ahead
+            float nsc = hasdn ? map_score(a, P, (long long)(L - 1) * Lq + r + 1) : MLOG0;
+            float ntc[7];
+            trn_bwd(dt0, L - 1, L, ntc);
+            float nfb = act ? fb[(long long)(L - 1) * Lq + r] : 0.f;
             for (int k = 0; k < L + 31; k++) {
                 const int j = k - lane;         // mirrored column
                 // diagonal-successor score of column j, read before this step's
@@ -324,10 +340,15 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
                 const float sco = (j >= 1 && j < L) ? rin[(j - 1) & 31][lane] : MLOG0;
                 float tc[7];
                 if (k < L) {
-                    const int ca = L - 1 - k;   // actual column of mirrored column k
                     // score of the diagonal successor of mirrored column k+1
-                    rin[k & 31][lane] = (act && r + 1 < Lq) ? map_score(a, P, (long long)ca * Lq + r + 1) : MLOG0;
-                    trn_bwd(dt0, ca, L, tc);
+                    rin[k & 31][lane] = nsc;
+#pragma unroll
+                    for (int i = 0; i < 7; i++) tc[i] = ntc[i];
+                    if (k + 1 < L) {
+                        const int ca1 = L - 2 - k;   // actual column of mirrored column k+1
+                        nsc = hasdn ? map_score(a, P, (long long)ca1 * Lq + r + 1) : MLOG0;
+                        trn_bwd(dt0, ca1, L, ntc);
+                    }
                 } else {
 #pragma unroll
                     for (int i = 0; i < 7; i++) tc[i] = MLOG0;
@@ -379,8 +400,8 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
                 upp = dn;
                 const int cfl = k - 31;
                 if (cfl >= 0 && cfl < L && act) {
-                    const long long idx = (long long)(L - 1 - cfl) * Lq + r;
-                    fb[idx] = fb[idx] + rout[cfl & 31][lane];
+                    fb[(long long)(L - 1 - cfl) * Lq + r] = nfb + rout[cfl & 31][lane];
+                    if (cfl + 1 < L) nfb = fb[(long long)(L - 2 - cfl) * Lq + r];
                 }
                 __syncwarp();
             }
@@ -439,8 +460,12 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
             float bcur = (s > 0 && lane < L) ? __ldcg(botr + lane) : 0.f;
             float bnxt = (s > 0 && 32 + lane < L) ? __ldcg(botr + 32 + lane) : 0.f;
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
+            float nfb = act ? fb[r] : 0.f;   // column k is loaded one step ahead
             for (int k = 0; k < L + 31; k++) {
-                if (k < L) rin[k & 31][lane] = act ? fb[(long long)k * Lq + r] : 0.f;
+                if (k < L) {
+                    rin[k & 31][lane] = nfb;
+                    if (k + 1 < L) nfb = act ? fb[(long long)(k + 1) * Lq + r] : 0.f;
+                }
                 float up = __shfl_up_sync(FULL, mine, 1);
                 {
                     const int src = k & 31;
