@@ -150,6 +150,8 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="database size factor (1.0 = 100k profiles)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    ap.add_argument("--score-mode", default="bf16", choices=["fp32", "bf16"],
+                    help="phase-1 score contractions: FP32 CUDA cores or split-BF16 tensor cores")
     args = ap.parse_args()
     world, rank, local = _dist()
     from comer2_b200 import params as P, synth as S
@@ -190,6 +192,8 @@ def main():
     Lq = int(q.lengths[0])
     cells = Lq * int(w.db.lengths.sum())
     h = Handle(prm, local)
+    from comer2_b200.native import SCORE_BF16_TC, SCORE_FP32
+    h.set_score_mode(SCORE_BF16_TC if args.score_mode == "bf16" else SCORE_FP32)
     st = torch.cuda.Stream()
     h.set_stream(st.cuda_stream)
     t0 = time.perf_counter()

@@ -52,6 +52,24 @@ constexpr int REC_CHUNK = 8, REC_CHUNK_LOG = 3, REC_SLOTS = 16;
 // shared memory per warp: score ring [32][32], SS row table [32][32], record ring
 constexpr int P1_WARP_FLOATS = 32 * 32 + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE;
 constexpr int MAX_CVCARD = 256;
+// Tensor-core (BF16 split) phase-1 kernel.  The three contractions of a cell
+// score -- amino acids (K = 20), context vectors (K = 19) and the SS table
+// (K = card <= 32, the db side a 3-hot vector of SS probabilities) -- run as
+// mma.sync m16n8k16 BF16 products with FP32 accumulation, each operand split
+// into hi + lo BF16 parts (x = hi + lo + O(2^-17 x)) and hi*hi + hi*lo +
+// lo*hi accumulated.  db operands (B, k16 x n8 fragments) are packed once per
+// database in the fragment order of the 32 lanes, 8 db columns per tile:
+//   tcdb[tile][dot 3][ktile 2][split 2][lane 32][2 words]
+// with every profile padded to a multiple of 32 columns; query operands (A,
+// m16 x k16) per query: qa[strip][mtile 2][dot 2: cv, ss][ktile 2][split 2]
+// [lane 32][4 words] and the unscaled amino-acid rows qaa[strip][mtile 2]
+// [ktile 2][lane 32][8 floats] (scaled per pair by 1 / (0.5 (bq + bd))).
+// Per db position the DP and the score epilogue also read a column record
+// cold[pos][P1C_TRS]: transitions 0..6, pad, cvnorm, CV prior, P(H) + 0.1, pad.
+constexpr int TC_TILE_WORDS = 3 * 2 * 2 * 32 * 2;
+constexpr int TC_QA_WORDS = 2 * 2 * 2 * 2 * 32 * 4;   // per strip
+constexpr int TC_QAA_FLOATS = 2 * 2 * 32 * 8;         // per strip
+enum : int { CO_CD = 8, CO_PD = 9, CO_HD = 10 };
 // chunked phase-1 kernel: 11 warps per CTA, one CTA per SM; per warp a score
 // ring of 64 columns x 32 rows, a transition ring of 64 columns (stride 12
 // floats: the two 16-byte reads of 8 lanes at consecutive columns cover 32
@@ -59,10 +77,17 @@ constexpr int MAX_CVCARD = 256;
 // above the strip for the current chunk ([32][8])
 constexpr int P1C_WARPS = 11;
 // phase-1 kernel variants of launch_p1
-enum : int { P1K_STRIP = 0, P1K_CHUNKED = 1, P1K_TRACEBACK = 2 };
+enum : int { P1K_STRIP = 0, P1K_CHUNKED = 1, P1K_TRACEBACK = 2, P1K_TENSOR = 3 };
 constexpr int P1C_RING = 64, P1C_TRS = 12, P1C_CVREP = 16;
 constexpr int P1C_WARP_FLOATS =
     P1C_RING * 32 + P1C_RING * P1C_TRS + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE + 32 * 8;
+// tensor-core kernel: score ring of 64 columns with 36 floats per column (the
+// fragment-layout writes and the per-lane wavefront reads are both free of
+// bank conflicts), a column-record ring of 4 chunks, the row above the strip
+// and the pair-scaled amino-acid A fragments of the strip ([mt][kt][split][lane][4])
+constexpr int P1T_WARPS = 11;
+constexpr int P1T_RLD = 36, P1T_CRING = 128;
+constexpr int P1T_WARP_FLOATS = P1C_RING * P1T_RLD + P1T_CRING * P1C_TRS + 32 * 8 + 2 * 2 * 2 * 32 * 4;
 
 struct P1Args {
     const float* qrec;      // [Lq][QR_STRIDE]
@@ -91,7 +116,13 @@ struct P1Args {
     // strip pipeline of the traceback variant
     float* bnd;                 // per candidate at 10 x (cand_off / Lq): two last-row buffers [5][L]
     int* prog;                  // [ncand][nstrips] finished columns per strip
-    float* tbbest;              // [ncand] DP maximum of the traceback sweep
+    unsigned long long* tbkey;  // [ncand] maximum of the traceback sweep and its cell, packed
+    // tensor-core operands (P1K_TENSOR)
+    const unsigned* tcdb;       // db B fragments
+    const long long* ttile;     // [nprof] first tile of each profile
+    const float* cold;          // [npos][P1C_TRS] column records
+    const unsigned* qa;         // query A fragments (cv, ss)
+    const float* qaa;           // query amino-acid rows in fragment order
 };
 
 struct FinArgs {
@@ -105,7 +136,8 @@ struct FinArgs {
     const float* best;
     const unsigned* coords;
     float scorethld;
-    const float* tbbest;        // [ncand] maxima of the traceback sweep (checked against best)
+    const unsigned long long* tbkey;  // [ncand] maxima of the traceback sweep and their cells
+    float tol;                  // allowed |phase-1 maximum - traceback maximum| (0: identical)
     int* status;
     // outputs [ncand]
     float* score;

@@ -28,6 +28,9 @@ size_t p1_smem_bytes(int cvcard);
 cudaError_t launch_p1(const P1Args& a, const float* qbkg, int which, int grid, cudaStream_t st);
 int p1_blocks_per_sm(int cvcard);
 int p1c_blocks_per_sm(int cvcard);
+int p1t_blocks_per_sm(int cvcard);
+cudaError_t launch_tc_pack(const float* drec, const long long* poff, const int* plen, const long long* ttile,
+                           int nprof, unsigned* tcdb, float* cold, cudaStream_t st);
 cudaError_t launch_fin(const FinArgs& a, cudaStream_t st);
 }  // namespace c2
 
@@ -61,6 +64,8 @@ struct c2_handle {
     uint64_t launches = 0;
     int nsm = 0;
     int grid = 0;
+    int score_mode = C2_SCORE_FP32;   // phase-1 score arithmetic (c2_set_score_mode)
+    bool tc_ready = false;            // db operands of the tensor-core path packed
     // parameters
     c2_params prm{};
     std::vector<float> ssss, cvkeys, cvvals, nnw;
@@ -101,7 +106,12 @@ struct c2_handle {
     DevBuf<signed char> d_btck;
     DevBuf<float> d_smat, d_mmat;
     // strip pipeline of the phase-2 sweeps: last-row buffers, progress words
-    DevBuf<float> d_bnd, d_tbbest;
+    DevBuf<float> d_bnd;
+    DevBuf<unsigned long long> d_tbkey;
+    // tensor-core score operands
+    DevBuf<unsigned> d_tcdb, d_qa;
+    DevBuf<long long> d_ttile;
+    DevBuf<float> d_cold, d_qaaf;
     DevBuf<int> d_prog;
     DevBuf<float> d_fscore;
     DevBuf<int> d_fpsts, d_fpassed;
@@ -352,6 +362,27 @@ static inline void trn_of(const c2_profiles* d, int k, int i, float* t7)
     t7[TIM] = a[3]; t7[TII] = b[4]; t7[TDM] = a[5]; t7[TDD] = a[6];
 }
 
+// candidate margin and traceback tolerance of the BF16 score mode (relative)
+constexpr float C2_TC_MARGIN = 2e-3f;
+constexpr float C2_TC_TOL = 2e-3f;
+
+// BF16 round to nearest even, as the device conversion does
+static inline uint32_t bf16_rn_bits(float x)
+{
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return 0x7fc0u;   // NaN
+    return (u + 0x7fffu + ((u >> 16) & 1u)) >> 16;
+}
+
+static inline float bf16_to_f(uint32_t b)
+{
+    const uint32_t u = b << 16;
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
 static inline int ss_index(int state, float prb) { return state * 10 + (int)(prb * 9.999f); }
 
 extern "C" c2_status c2_upload_db(c2_handle* h, const c2_profiles* d, uint64_t tot_pos, uint64_t tot_prof)
@@ -421,6 +452,7 @@ extern "C" c2_status c2_upload_db(c2_handle* h, const c2_profiles* d, uint64_t t
     if (h->d_bot.ensure((size_t)h->grid * P1_WARPS * h->botstride))
         return fail(h, C2_ERR_NOMEM, "strip-boundary scratch allocation failed");
     h->Lq = 0;
+    h->tc_ready = false;
     return C2_OK;
 }
 
@@ -464,6 +496,57 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
     }
     if (h->d_qrec.ensure(h->h_qrec.size()) || h->d_qbkg.ensure(NAA))
         return fail(h, C2_ERR_NOMEM, "query allocation failed");
+    // tensor-core query operands (layouts in c2_device.cuh): context vectors
+    // and SS row tables U[r][c] = sum_s p_q(s) T[idx_q(s)][c] as split BF16 A
+    // fragments, amino-acid rows unscaled in fragment order
+    {
+        const int ns = (Lq + 31) / 32;
+        const int card = h->sc.ssss_card;
+        std::vector<float> U((size_t)Lq * 32, 0.f);
+        for (int r = 0; r < Lq; r++) {
+            const float* s3 = q->ss + (size_t)r * NSS;
+            const int i0 = (int)(s3[0] * 9.999f), i1 = 10 + (int)(s3[1] * 9.999f), i2 = 20 + (int)(s3[2] * 9.999f);
+            for (int c = 0; c < card; c++)
+                U[(size_t)r * 32 + c] = s3[0] * h->ssss[(size_t)i0 * card + c] + s3[1] * h->ssss[(size_t)i1 * card + c] +
+                                        s3[2] * h->ssss[(size_t)i2 * card + c];
+        }
+        auto aval = [&](int d, int r, int k) -> float {
+            if (r >= Lq) return 0.f;
+            if (d == 0) return k < NCV ? q->cv[(size_t)r * NCV + k] : 0.f;
+            return k < card ? U[(size_t)r * 32 + k] : 0.f;
+        };
+        std::vector<uint32_t> qa((size_t)ns * TC_QA_WORDS, 0u);
+        std::vector<float> qaa((size_t)ns * TC_QAA_FLOATS, 0.f);
+        for (int s = 0; s < ns; s++)
+            for (int mt = 0; mt < 2; mt++)
+                for (int kt = 0; kt < 2; kt++)
+                    for (int lane = 0; lane < 32; lane++) {
+                        const int g = lane >> 2, qq = lane & 3;
+                        for (int d = 0; d < 2; d++)
+                            for (int w = 0; w < 4; w++) {
+                                const int r = 32 * s + 16 * mt + g + ((w & 1) ? 8 : 0);
+                                const int k = 16 * kt + 2 * qq + ((w >> 1) ? 8 : 0);
+                                const float x0 = aval(d, r, k), x1 = aval(d, r, k + 1);
+                                const uint32_t h0 = bf16_rn_bits(x0), h1 = bf16_rn_bits(x1);
+                                const uint32_t l0 = bf16_rn_bits(x0 - bf16_to_f(h0));
+                                const uint32_t l1 = bf16_rn_bits(x1 - bf16_to_f(h1));
+                                const size_t base = (size_t)(((s * 2 + mt) * 2 + d) * 2 + kt) * 2;
+                                qa[((base + 0) * 32 + lane) * 4 + w] = h0 | (h1 << 16);
+                                qa[((base + 1) * 32 + lane) * 4 + w] = l0 | (l1 << 16);
+                            }
+                        for (int e = 0; e < 8; e++) {
+                            const int r = 32 * s + 16 * mt + g + (((e >> 1) & 1) << 3);
+                            const int k = 16 * kt + 2 * qq + (e & 1) + ((e >> 2) << 3);
+                            qaa[((size_t)((s * 2 + mt) * 2 + kt) * 32 + lane) * 8 + e] =
+                                (r < Lq && k < NAA) ? q->trg[(size_t)r * NAA + k] : 0.f;
+                        }
+                    }
+        if (h->d_qa.ensure(qa.size()) || h->d_qaaf.ensure(qaa.size()))
+            return fail(h, C2_ERR_NOMEM, "query operand allocation failed");
+        CK(cudaMemcpyAsync(h->d_qa.p, qa.data(), qa.size() * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->d_qaaf.p, qaa.data(), qaa.size() * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
     CK(cudaMemcpyAsync(h->d_qrec.p, h->h_qrec.data(), h->h_qrec.size() * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_qbkg.p, q->bkg, NAA * 4, cudaMemcpyHostToDevice, h->stream));
     // MAP forward: column -1 states of the query rows (log-sum-exp form of the
@@ -526,6 +609,36 @@ extern "C" c2_status c2_get_thresholds(const c2_handle* h, float* s, float* le)
     return C2_OK;
 }
 
+// Pack the db operands of the tensor-core path (once per database).
+static c2_status tc_prepare_db(c2_handle* h)
+{
+    if (h->tc_ready) return C2_OK;
+    std::vector<long long> tt(h->nprof);
+    long long ntiles = 0;
+    for (int k = 0; k < h->nprof; k++) {
+        tt[k] = ntiles;
+        ntiles += (long long)((h->h_plen[k] + 31) / 32) * 4;
+    }
+    if (h->d_ttile.ensure(h->nprof) || h->d_tcdb.ensure((size_t)ntiles * TC_TILE_WORDS) ||
+        h->d_cold.ensure((size_t)h->npos * P1C_TRS))
+        return fail(h, C2_ERR_NOMEM, "tensor-core db operands (%lld tiles) allocation failed", ntiles);
+    CK(cudaMemcpyAsync(h->d_ttile.p, tt.data(), (size_t)h->nprof * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(launch_tc_pack(h->d_drec.p, h->d_poff.p, h->d_plen.p, h->d_ttile.p, h->nprof, h->d_tcdb.p, h->d_cold.p,
+                      h->stream));
+    h->launches++;
+    CK(cudaStreamSynchronize(h->stream));
+    h->tc_ready = true;
+    return C2_OK;
+}
+
+extern "C" c2_status c2_set_score_mode(c2_handle* h, int32_t mode)
+{
+    if (!h) return C2_ERR_ARG;
+    if (mode != C2_SCORE_FP32 && mode != C2_SCORE_BF16_TC) return fail(h, C2_ERR_ARG, "unknown score mode %d", mode);
+    h->score_mode = mode;
+    return C2_OK;
+}
+
 static void fill_p1(c2_handle* h, P1Args& a)
 {
     memset(&a, 0, sizeof a);
@@ -556,6 +669,21 @@ extern "C" c2_status c2_run_phase1(c2_handle* h)
     a.nwork = h->nprof;
     a.order = h->d_order.p;
     CK(cudaMemsetAsync(h->d_counter.p, 0, sizeof(int), h->stream));
+    if (h->score_mode == C2_SCORE_BF16_TC) {
+        c2_status st = tc_prepare_db(h);
+        if (st != C2_OK) return st;
+        a.tcdb = h->d_tcdb.p;
+        a.ttile = h->d_ttile.p;
+        a.cold = h->d_cold.p;
+        a.qa = h->d_qa.p;
+        a.qaa = h->d_qaaf.p;
+        int gt = h->nsm * p1t_blocks_per_sm(h->sc.cvcard);
+        if (gt < 1) return fail(h, C2_ERR_CUDA, "tensor-core phase-1 kernel does not fit on an SM");
+        gt = std::min(gt, h->grid * P1_WARPS / P1T_WARPS);
+        CK(launch_p1(a, h->d_qbkg.p, P1K_TENSOR, gt, h->stream));
+        h->launches++;
+        return C2_OK;
+    }
     // chunked kernel: one CTA of P1C_WARPS warps per SM, within the boundary-row slots
     // allocated for the strip kernel's grid (h->grid x P1_WARPS)
     int gc = h->nsm * p1c_blocks_per_sm(h->sc.cvcard);
@@ -604,8 +732,14 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     h->h_cand.clear();
     h->h_cand_off.clear();
     long long acc = 0;
+    // FinalizeDPPro: maxsc <= scorethld -> not passed.  With BF16 phase-1
+    // scores the candidate cut is lowered by a margin far above their error;
+    // the FP32 traceback sweep then applies the exact cut (fin_kernel).
+    const float cut = (h->score_mode == C2_SCORE_FP32)
+                          ? h->scorethld
+                          : h->scorethld - C2_TC_MARGIN * std::max(1.0f, std::fabs(h->scorethld));
     for (int k = 0; k < h->nprof; k++) {
-        if (b[k] > h->scorethld) {  // FinalizeDPPro: maxsc <= scorethld -> not passed
+        if (b[k] > cut) {
             h->h_cand.push_back(k);
             h->h_cand_off.push_back(acc);
             acc += (long long)h->Lq * h->h_plen[k];
@@ -618,7 +752,7 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     if (h->d_cand_prof.ensure(nc) || h->d_cand_off.ensure(nc) || h->d_btck.ensure((size_t)acc) ||
         h->d_smat.ensure((size_t)acc) || h->d_mmat.ensure((size_t)acc) || h->d_fscore.ensure(nc) || h->d_fpsts.ensure(nc) ||
         h->d_fpassed.ensure(nc) || h->d_fbeg.ensure(nc) || h->d_fend.ensure(nc) ||
-        h->d_bnd.ensure((size_t)(acc / h->Lq) * 10) || h->d_tbbest.ensure(nc) ||
+        h->d_bnd.ensure((size_t)(acc / h->Lq) * 10) || h->d_tbkey.ensure(nc) ||
         h->d_prog.ensure((size_t)nc * ((h->Lq + 31) / 32)))
         return fail(h, C2_ERR_NOMEM, "finalisation scratch for %d pairs (%lld cells) failed", nc, acc);
     CK(cudaMemcpyAsync(h->d_cand_prof.p, h->h_cand.data(), (size_t)nc * 4, cudaMemcpyHostToDevice, h->stream));
@@ -633,11 +767,11 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     a.mmat = h->d_mmat.p;
     a.bnd = h->d_bnd.p;
     a.prog = h->d_prog.p;
-    a.tbbest = h->d_tbbest.p;
+    a.tbkey = h->d_tbkey.p;
     const long long nitems = (long long)nc * ((h->Lq + 31) / 32);
     CK(cudaMemsetAsync(h->d_counter.p, 0, sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_prog.p, 0, (size_t)nitems * sizeof(int), h->stream));
-    CK(cudaMemsetAsync(h->d_tbbest.p, 0, (size_t)nc * sizeof(float), h->stream));
+    CK(cudaMemsetAsync(h->d_tbkey.p, 0, (size_t)nc * sizeof(unsigned long long), h->stream));
     // one warp per (candidate, strip) work item at most
     const int grid = (int)std::min<long long>(h->grid, (nitems + P1_WARPS - 1) / P1_WARPS);
     CK(launch_p1(a, h->d_qbkg.p, P1K_TRACEBACK, grid, h->stream));
@@ -653,7 +787,9 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     f.best = h->d_best.p;
     f.coords = h->d_coords.p;
     f.scorethld = h->scorethld;
-    f.tbbest = h->d_tbbest.p;
+    f.tbkey = h->d_tbkey.p;
+    // BF16 phase-1 maxima differ from the FP32 traceback sweep by rounding only
+    f.tol = (h->score_mode == C2_SCORE_FP32) ? 0.f : C2_TC_TOL;
     f.status = h->d_status.p;
     f.score = h->d_fscore.p;
     f.psts = h->d_fpsts.p;

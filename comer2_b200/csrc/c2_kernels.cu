@@ -21,6 +21,8 @@
 // The traceback variant (p1tb_kernel) recomputes the same DP for the pairs
 // that pass the phase-1 threshold and stores their scores and btck codes
 // column-major for the finalisation, statistics and MAP stages.
+#include <cuda_bf16.h>
+
 #include "c2_device.cuh"
 
 namespace c2 {
@@ -348,7 +350,7 @@ p1_kernel(P1Args a, const float* __restrict__ qbkg)
 // arithmetic as p1_kernel, storing the score matrix, the modular scores and
 // the btck codes column-major.  Work items are (candidate, strip) as in the
 // phase-2 strip pipeline (c2_device.cuh), so a long pair is swept by several
-// warps at once; the pair maximum is collected in tbbest for the check
+// warps at once; the pair maximum and its cell are collected in tbkey for the check
 // against phase 1.
 __global__ void __launch_bounds__(P1_WARPS * 32, 2)
 p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
@@ -392,6 +394,8 @@ p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
         float* botw = bnd + (s & 1) * 5 * L;
         int* pf = a.prog + (long long)cand * nstrips;
         float best = 0.f;
+        int bcol = 0x7fffffff;
+        int brow = 0x7fffffff;
         {
             const int r = s * 32 + lane;
             const bool act = r < Lq;
@@ -526,7 +530,7 @@ p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
                     nw.ND = fmaxf(left.MM + t7[TMD], left.ND + t7[TDD]);
                 }
                 const bool valid = act && j >= 0 && j < L;
-                if (valid && nw.MM > best) best = nw.MM;
+                if (valid && nw.MM > best) { best = nw.MM; bcol = j; }
                 if (valid) {
                     int b = BT_STOP;
                     float mx = nw.MM;
@@ -551,10 +555,23 @@ p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
             cp_async_wait_all();
             __syncwarp();
         }
+        if (best > 0.f) brow = s * 32 + lane;
 #pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) best = fmaxf(best, __shfl_xor_sync(FULL, best, o));
-        // best >= 0, so its bit pattern orders as an unsigned integer
-        if (lane == 0) atomicMax(reinterpret_cast<unsigned*>(a.tbbest + cand), __float_as_uint(best));
+        for (int o = 16; o >= 1; o >>= 1) {
+            const float ob = __shfl_xor_sync(FULL, best, o);
+            const int orr = __shfl_xor_sync(FULL, brow, o);
+            const int oc = __shfl_xor_sync(FULL, bcol, o);
+            if (ob > best || (ob == best && (orr < brow || (orr == brow && oc < bcol)))) {
+                best = ob; brow = orr; bcol = oc;
+            }
+        }
+        // pair maximum over strips: largest value, then smallest row, then
+        // smallest column, as one 64-bit key (best >= 0 orders by its bits)
+        if (lane == 0 && best > 0.f) {
+            const unsigned cell = ((unsigned)brow << 16) | ((unsigned)bcol & 0xffffu);
+            atomicMax(a.tbkey + cand,
+                      ((unsigned long long)__float_as_uint(best) << 32) | (unsigned long long)(0xffffffffu - cell));
+        }
         __syncwarp();
     }
 }
@@ -576,7 +593,9 @@ struct DPLane {
     int kbest;
 };
 
-template <bool CHECK>
+// RLD: floats per column of the score ring; TMASK: slot mask of the
+// transition ring (stride P1C_TRS floats per column)
+template <bool CHECK, int RLD = 32, int TMASK = P1C_RING - 1>
 __device__ __forceinline__ void p1c_steps(DPLane& D, int k0, int k1, int lane, int L, bool act, int cA, int cB,
                                           const float* __restrict__ ring, const float* __restrict__ trn,
                                           const float* __restrict__ bnd, const St5& LB, const St5& DB, bool wr_bot,
@@ -586,12 +605,13 @@ __device__ __forceinline__ void p1c_steps(DPLane& D, int k0, int k1, int lane, i
     for (int k = k0; k < k1; k++) {
         const int j = k - lane;
         const int slot = j & (P1C_RING - 1);
-        float S = ring[slot * 32 + lane];
+        float S = ring[slot * RLD + lane];
         if (j <= cA || j >= cB) S = -9.f;   // corner cells (CellYXinCorners)
         float t7[7];
         {
-            const float4 ta = *reinterpret_cast<const float4*>(trn + slot * P1C_TRS);
-            const float4 tb = *reinterpret_cast<const float4*>(trn + slot * P1C_TRS + 4);
+            const int ts = (j & TMASK) * P1C_TRS;
+            const float4 ta = *reinterpret_cast<const float4*>(trn + ts);
+            const float4 tb = *reinterpret_cast<const float4*>(trn + ts + 4);
             t7[0] = ta.x; t7[1] = ta.y; t7[2] = ta.z; t7[3] = ta.w;
             t7[4] = tb.x; t7[5] = tb.y; t7[6] = tb.z;
         }
@@ -804,6 +824,373 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core score path (layouts in c2_device.cuh).
+
+__device__ __forceinline__ unsigned bf16_bits(float x)
+{
+    return (unsigned)__bfloat16_as_ushort(__float2bfloat16_rn(x));
+}
+
+// hi and lo BF16 parts of x: hi = bf16(x), lo = bf16(x - hi)
+__device__ __forceinline__ void bf16_split(float x, unsigned& hi, unsigned& lo)
+{
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    hi = (unsigned)__bfloat16_as_ushort(h);
+    lo = bf16_bits(x - __bfloat162float(h));
+}
+
+// D += A * B, m16n8k16, BF16 inputs, FP32 accumulation
+__device__ __forceinline__ void mma_bf16(float* d, const unsigned* a, unsigned b0, unsigned b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Pack the db operands of one profile per CTA (4 warps over its 8-column
+// tiles) and its column records.
+__global__ void __launch_bounds__(128) tc_pack_kernel(const float* __restrict__ drec, const long long* __restrict__ poff,
+                                                      const int* __restrict__ plen, const long long* __restrict__ ttile,
+                                                      unsigned* __restrict__ tcdb, float* __restrict__ cold)
+{
+    const int p = blockIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int L = plen[p];
+    const long long off = poff[p];
+    const int ntiles = ((L + 31) >> 5) * 4;
+    const int g = lane >> 2, q = lane & 3;
+    for (int t = wid; t < ntiles; t += 4) {
+        const int col = 8 * t + g;
+        const bool valid = col < L;
+        const float* rc = drec + (off + (valid ? col : 0)) * DR_STRIDE;
+        const int pk = __float_as_int(rc[DR_SSIDX]);
+        const int i0 = pk & 0xff, i1 = (pk >> 8) & 0xff, i2 = (pk >> 16) & 0xff;
+        unsigned* out = tcdb + (ttile[p] + t) * (long long)TC_TILE_WORDS;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+#pragma unroll
+            for (int kt = 0; kt < 2; kt++) {
+                float v[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const int k = 16 * kt + 2 * q + (e & 1) + (e >> 1) * 8;
+                    float x = 0.f;
+                    if (valid) {
+                        if (d == 0) x = (k < NAA) ? rc[DR_TRG + k] : 0.f;
+                        else if (d == 1) x = (k < NCV) ? rc[DR_CV + k] : 0.f;
+                        else x = (k == i0) ? rc[DR_SS] : (k == i1) ? rc[DR_SS + 1] : (k == i2) ? rc[DR_SS + 2] : 0.f;
+                    }
+                    v[e] = x;
+                }
+                unsigned h[4], l[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) bf16_split(v[e], h[e], l[e]);
+                unsigned* o = out + ((d * 2 + kt) * 2) * 64 + lane * 2;
+                o[0] = h[0] | (h[1] << 16);
+                o[1] = h[2] | (h[3] << 16);
+                o[64] = l[0] | (l[1] << 16);
+                o[65] = l[2] | (l[3] << 16);
+            }
+        }
+    }
+    for (int c = threadIdx.x; c < L; c += blockDim.x) {
+        const float* rc = drec + (off + c) * DR_STRIDE;
+        float* o = cold + (off + c) * P1C_TRS;
+#pragma unroll
+        for (int i = 0; i < 7; i++) o[i] = rc[DR_TRN + i];
+        o[7] = 0.f;
+        o[CO_CD] = rc[DR_CN];
+        o[CO_PD] = rc[DR_PRIOR];
+        o[CO_HD] = rc[DR_HD];
+        o[11] = 0.f;
+    }
+}
+
+// Score epilogue of one cell from its three contractions (same arithmetic as
+// cell_score after the dot products)
+template <int CVREP>
+__device__ __forceinline__ float tc_epilogue(float daa, float dcv, float dss, float cq, float pq, float hq, float cd,
+                                             float pd, float hd, const float* __restrict__ cvtab,
+                                             const ScoreConsts& sc, int lane)
+{
+    const float s0 = __logf(daa) - sc.shift;
+    const float dot = dcv + sc.lokappa0;
+    const float det = cq * cd - dot * dot;
+    const float cvs = sc.cterm + sc.pownu0 * __logf(det) - pq - pd;
+    float cvm;
+    if (cvs <= sc.cvkey_first) cvm = sc.cvval_first;
+    else if (sc.cvkey_last <= cvs) cvm = sc.cvval_last;
+    else {
+        const int ix = min(max(sc.cvshift + (int)rintf(2.f * cvs), 0), sc.cvcard - 1);
+        cvm = cvtab[ix * CVREP + (lane & (CVREP - 1))];
+    }
+    cvm *= sc.cvswgt;
+    float ss = dss;
+    if (-99.f < ss) {
+        ss += hq * hd * 0.1111111f;
+        ss -= 0.05f;
+        ss *= sc.ssswgt;
+    }
+    return s0 + (ss + cvm);
+}
+
+// Stage the column records of chunk m (32 columns) into the column ring
+__device__ __forceinline__ void stage_cols(float* cring, const float* __restrict__ cold, int m, int L, int lane)
+{
+    const int c0 = 32 * m;
+    const int nc = min(32, L - c0);
+    if (nc > 0) {
+        float* dst = cring + (c0 & (P1T_CRING - 1)) * P1C_TRS;
+        const float* src = cold + (long long)c0 * P1C_TRS;
+        for (int i = lane; i < nc * (P1C_TRS / 4); i += 32) cp_async16(dst + 4 * i, src + 4 * i);
+    }
+    cp_async_commit();
+}
+
+// Phase 1 with the score contractions on the tensor cores: per 32-column
+// chunk the warp computes the 32 x 32 score tile with mma.sync (fragment
+// layout: lane (g, q) holds rows g, g + 8 of each 16-row tile and columns
+// 2q, 2q + 1 of each 8-column tile), applies the epilogue per cell, writes the
+// scores into the ring, then advances the same wavefront DP as p1c_kernel.
+__global__ void __launch_bounds__(P1T_WARPS * 32, 1)
+p1t_kernel(P1Args a, const float* __restrict__ qbkg)
+{
+    extern __shared__ float smem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int cvcard = a.sc.cvcard;
+    float* cvtab = smem;                                      // [cvcard][P1C_CVREP]
+    float* wb = smem + cvcard * P1C_CVREP + wid * P1T_WARP_FLOATS;
+    float* ring = wb;                                         // [P1C_RING][P1T_RLD] scores
+    float* cring = ring + P1C_RING * P1T_RLD;                 // [P1T_CRING][P1C_TRS] column records
+    float* bnd = cring + P1T_CRING * P1C_TRS;                 // [32][8] row above the strip
+    uint4* aas = reinterpret_cast<uint4*>(bnd + 32 * 8);      // [mt][kt][split][lane] amino-acid A fragments
+    for (int i = threadIdx.x; i < cvcard * P1C_CVREP; i += blockDim.x) cvtab[i] = a.cvvals[i / P1C_CVREP];
+    __syncthreads();
+
+    const long long slotw = (long long)blockIdx.x * P1T_WARPS + wid;
+    const int Lmax = (int)(a.botstride / 10);
+    float* bot0 = a.bot + slotw * a.botstride;
+    const int Lq = a.Lq;
+    const int nstrips = (Lq + 31) >> 5;
+    const ScoreConsts sc = a.sc;
+    const int g = lane >> 2, q = lane & 3;
+
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.counter, 1);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= a.nwork) break;
+        const int p = a.order[item];
+        const int L = a.plen[p];
+        const long long off = a.poff[p];
+        const float* __restrict__ cold = a.cold + off * P1C_TRS;
+        const unsigned* __restrict__ tb0 = a.tcdb + a.ttile[p] * (long long)TC_TILE_WORDS;
+        const float* __restrict__ bd = a.pbkg + (long long)p * NAA;
+        const int edge = corner_edge(Lq, L);
+        float* botr = bot0;
+        float* botw = bot0 + 5 * Lmax;
+        float pbest = 0.f;
+        int prow = 0x7fffffff, pcol = 0x7fffffff;
+
+        for (int s = 0; s < nstrips; s++) {
+            const int r = s * 32 + lane;
+            const bool act = r < Lq;
+            const float* __restrict__ qr = a.qrec + (long long)(act ? r : Lq - 1) * QR_STRIDE;
+            // amino-acid A fragments of this strip, scaled for the pair and split
+            // into shared memory (q(a) / (0.5 (bq(a) + bd(a))), as cell_score's Qt)
+            __syncwarp();
+#pragma unroll
+            for (int kt = 0; kt < 2; kt++) {
+                float wk[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const int k = 16 * kt + 2 * q + (e & 1) + (e >> 1) * 8;
+                    wk[e] = (k < NAA) ? 0.5f * (qbkg[k] + bd[k]) : 1.f;
+                }
+#pragma unroll
+                for (int mt = 0; mt < 2; mt++) {
+                    const float4* src = reinterpret_cast<const float4*>(
+                        a.qaa + ((((long long)s * 2 + mt) * 2 + kt) * 32 + lane) * 8);
+                    const float4 u0 = __ldg(src), u1 = __ldg(src + 1);
+                    const float v[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+                    unsigned h[8], l[8];
+#pragma unroll
+                    for (int e = 0; e < 8; e++) {
+                        // element e: register e / 2, k index 2q + (e & 1) + 8 (e >= 4)
+                        const float x = __fdividef(v[e], wk[(e & 1) + ((e >> 2) << 1)]);
+                        bf16_split(x, h[e], l[e]);
+                    }
+                    aas[((mt * 2 + kt) * 2 + 0) * 32 + lane] =
+                        make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16), h[6] | (h[7] << 16));
+                    aas[((mt * 2 + kt) * 2 + 1) * 32 + lane] =
+                        make_uint4(l[0] | (l[1] << 16), l[2] | (l[3] << 16), l[4] | (l[5] << 16), l[6] | (l[7] << 16));
+                }
+            }
+            // query row terms of this lane's fragment rows: 32 s + 16 mt + g + 8 h
+            float rq[2][2][3];
+#pragma unroll
+            for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+                for (int hh = 0; hh < 2; hh++) {
+                    const int rr = s * 32 + 16 * mt + g + 8 * hh;
+                    const float* qx = a.qrec + (long long)min(rr, Lq - 1) * QR_STRIDE;
+                    rq[mt][hh][0] = qx[QR_CN];
+                    rq[mt][hh][1] = qx[QR_PRIOR];
+                    rq[mt][hh][2] = qx[QR_HQ];
+                }
+            DPLane D;
+#pragma unroll
+            for (int i = 0; i < 7; i++) D.q7[i] = act ? qr[QR_TRN + i] : LOG0;
+            const bool z_left = (lane == 31);
+            const bool z_diag = (lane == 31 || lane == 0);
+            const St5 LB = z_left ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
+                                  : St5{0.f, qr[QR_C + 0], qr[QR_C + 1], qr[QR_C + 2], LOG0};
+            const St5 DB = z_diag ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
+                                  : St5{0.f, qr[QR_CP + 0], qr[QR_CP + 1], qr[QR_CP + 2], LOG0};
+            const int cA = (Lq <= r + edge) ? edge + r - Lq : -1;
+            const int cB = (r < edge) ? L - edge + r : 0x7fffffff;
+            D.mine = St5{0.f, 0.f, 0.f, 0.f, 0.f};
+            D.upp = D.mine;
+            D.best = 0.f;
+            D.kbest = 0;
+            float bc[5];
+#pragma unroll
+            for (int f = 0; f < 5; f++) {
+                bc[f] = 0.f;
+                D.bnxt[f] = 0.f;
+                if (s > 0) {
+                    if (lane < L) bc[f] = botr[f * Lmax + lane];
+                    if (32 + lane < L) D.bnxt[f] = botr[f * Lmax + 32 + lane];
+                }
+            }
+            const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
+            __syncwarp();
+            *reinterpret_cast<float4*>(bnd + lane * 8) = make_float4(bc[0], bc[1], bc[2], bc[3]);
+            bnd[lane * 8 + 4] = bc[4];
+            stage_cols(cring, cold, 0, L, lane);
+            stage_cols(cring, cold, 1, L, lane);
+            const int nch = (L + 31) >> 5;
+            const int kend = L + 31;
+            const unsigned* __restrict__ qa = a.qa + (long long)s * TC_QA_WORDS;
+            for (int m = 0; 32 * m < kend; m++) {
+                if (m < nch) {
+                    cp_async_wait_1();   // column records of chunk m have landed
+                    __syncwarp();
+                    stage_cols(cring, cold, m + 2, L, lane);
+                    // ---- score stage: 32 x 32 tile of chunk m on the tensor cores
+#pragma unroll 1
+                    for (int nt = 0; nt < 4; nt++) {
+                        const unsigned* tb = tb0 + (long long)(4 * m + nt) * TC_TILE_WORDS + lane * 2;
+                        uint2 B[3][2][2];
+#pragma unroll
+                        for (int d = 0; d < 3; d++)
+#pragma unroll
+                            for (int kt = 0; kt < 2; kt++)
+#pragma unroll
+                                for (int sp = 0; sp < 2; sp++)
+                                    B[d][kt][sp] = __ldg(reinterpret_cast<const uint2*>(tb + ((d * 2 + kt) * 2 + sp) * 64));
+                        const int c0 = 32 * m + 8 * nt + 2 * q;
+                        const float* cr0 = cring + (c0 & (P1T_CRING - 1)) * P1C_TRS;
+                        const float* cr1 = cring + ((c0 + 1) & (P1T_CRING - 1)) * P1C_TRS;
+                        const float cd[2] = {cr0[CO_CD], cr1[CO_CD]};
+                        const float pd[2] = {cr0[CO_PD], cr1[CO_PD]};
+                        const float hd[2] = {cr0[CO_HD], cr1[CO_HD]};
+#pragma unroll
+                        for (int mt = 0; mt < 2; mt++) {
+                            float acc[3][4];
+#pragma unroll
+                            for (int d = 0; d < 3; d++)
+#pragma unroll
+                                for (int i = 0; i < 4; i++) acc[d][i] = 0.f;
+#pragma unroll
+                            for (int kt = 0; kt < 2; kt++) {
+                                const uint4 ah = aas[((mt * 2 + kt) * 2 + 0) * 32 + lane];
+                                const uint4 al = aas[((mt * 2 + kt) * 2 + 1) * 32 + lane];
+                                const unsigned Ah[4] = {ah.x, ah.y, ah.z, ah.w};
+                                const unsigned Al[4] = {al.x, al.y, al.z, al.w};
+                                mma_bf16(acc[0], Al, B[0][kt][0].x, B[0][kt][0].y);
+                                mma_bf16(acc[0], Ah, B[0][kt][1].x, B[0][kt][1].y);
+                                mma_bf16(acc[0], Ah, B[0][kt][0].x, B[0][kt][0].y);
+                            }
+#pragma unroll
+                            for (int d = 1; d < 3; d++)
+#pragma unroll
+                                for (int kt = 0; kt < 2; kt++) {
+                                    const uint4* ap = reinterpret_cast<const uint4*>(
+                                        qa + ((((mt * 2 + (d - 1)) * 2 + kt) * 2) * 32 + lane) * 4);
+                                    const uint4 ah = __ldg(ap), al = __ldg(ap + 32);
+                                    const unsigned Ah[4] = {ah.x, ah.y, ah.z, ah.w};
+                                    const unsigned Al[4] = {al.x, al.y, al.z, al.w};
+                                    mma_bf16(acc[d], Al, B[d][kt][0].x, B[d][kt][0].y);
+                                    mma_bf16(acc[d], Ah, B[d][kt][1].x, B[d][kt][1].y);
+                                    mma_bf16(acc[d], Ah, B[d][kt][0].x, B[d][kt][0].y);
+                                }
+                            // epilogue: cell (row 16 mt + g + 8 hh, column c0 + e) is register 2 hh + e
+#pragma unroll
+                            for (int hh = 0; hh < 2; hh++)
+#pragma unroll
+                                for (int e = 0; e < 2; e++) {
+                                    const int i = 2 * hh + e;
+                                    const float S = tc_epilogue<P1C_CVREP>(acc[0][i], acc[1][i], acc[2][i],
+                                                                           rq[mt][hh][0], rq[mt][hh][1], rq[mt][hh][2],
+                                                                           cd[e], pd[e], hd[e], cvtab, sc, lane);
+                                    ring[((c0 + e) & (P1C_RING - 1)) * P1T_RLD + 16 * mt + g + 8 * hh] = S;
+                                }
+                        }
+                    }
+                }
+                __syncwarp();
+                // ---- DP stage: wavefront steps [32m, 32m + 32)
+                const int k0 = 32 * m, k1 = min(k0 + 32, kend);
+                if (m >= 1 && k0 + 31 < L && k1 == k0 + 32)
+                    p1c_steps<false, P1T_RLD, P1T_CRING - 1>(D, k0, k1, lane, L, act, cA, cB, ring, cring, bnd, LB,
+                                                             DB, wr_bot, botw, Lmax);
+                else
+                    p1c_steps<true, P1T_RLD, P1T_CRING - 1>(D, k0, k1, lane, L, act, cA, cB, ring, cring, bnd, LB,
+                                                            DB, wr_bot, botw, Lmax);
+                __syncwarp();
+                *reinterpret_cast<float4*>(bnd + lane * 8) = make_float4(D.bnxt[0], D.bnxt[1], D.bnxt[2], D.bnxt[3]);
+                bnd[lane * 8 + 4] = D.bnxt[4];
+#pragma unroll
+                for (int f = 0; f < 5; f++) {
+                    const int cc = k0 + 64 + lane;
+                    D.bnxt[f] = (s > 0 && cc < L) ? botr[f * Lmax + cc] : 0.f;
+                }
+                __syncwarp();
+            }
+            cp_async_wait_all();
+            {
+                float b = D.best;
+                int rr = (D.best > 0.f) ? r : 0x7fffffff;
+                int cc = (D.best > 0.f) ? D.kbest - lane : 0x7fffffff;
+                if (b > pbest || (b == pbest && (rr < prow || (rr == prow && cc < pcol)))) {
+                    pbest = b; prow = rr; pcol = cc;
+                }
+            }
+            float* t = botr; botr = botw; botw = t;
+            __syncwarp();
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            const float ob = __shfl_xor_sync(FULL, pbest, o);
+            const int orr = __shfl_xor_sync(FULL, prow, o);
+            const int oc = __shfl_xor_sync(FULL, pcol, o);
+            if (ob > pbest || (ob == pbest && (orr < prow || (orr == prow && oc < pcol)))) {
+                pbest = ob; prow = orr; pcol = oc;
+            }
+        }
+        if (lane == 0) {
+            const unsigned xy = (pbest > 0.f) ? (((unsigned)pcol << 16) | ((unsigned)prow & 0xffffu)) : 0u;
+            a.best[p] = pbest;
+            a.coords[p] = xy;
+        }
+        __syncwarp();
+    }
+}
+
 // Warp butterfly sum as the reference's FinalizeDPPro reduction
 // (src/libmycu/cudp/CuBatchDP_final.cu:254-260).
 __device__ __forceinline__ float warp_butterfly(float v)
@@ -830,10 +1217,18 @@ __global__ void __launch_bounds__(256) fin_kernel(FinArgs a)
     const signed char* bt = a.btck + a.cand_off[c];
     const float* sm = a.smat + a.cand_off[c];
     float* ch = cache[wid];
-    const float maxsc = a.best[p];
-    // the traceback sweep must reproduce the phase-1 maximum of this pair
-    if (lane == 0 && a.tbbest[c] != maxsc && a.status) atomicCAS(a.status, 0, 2);
-    const unsigned xx = a.coords[p];
+    // maximum and end cell from the traceback sweep (FP32 scores)
+    const unsigned long long key = a.tbkey[c];
+    const float maxsc = __uint_as_float((unsigned)(key >> 32));
+    const unsigned cell = 0xffffffffu - (unsigned)(key & 0xffffffffu);
+    const unsigned xx = (key != 0ull) ? (((cell & 0xffffu) << 16) | (cell >> 16)) : 0u;
+    // ... which must reproduce the phase-1 maximum of this pair (exactly when
+    // phase 1 used the same FP32 scores, within tol after BF16 scores)
+    if (lane == 0 && a.status) {
+        const float pb = a.best[p];
+        const bool ok = (a.tol == 0.f) ? (maxsc == pb && xx == a.coords[p]) : (fabsf(maxsc - pb) <= a.tol * fmaxf(1.f, pb));
+        if (!ok) atomicCAS(a.status, 0, 2);
+    }
     int x = (int)(xx >> 16), y = (int)(xx & 0xffff);
     int psts = 0;
     int b = BT_DIAG;
@@ -877,13 +1272,35 @@ __global__ void __launch_bounds__(256) fin_kernel(FinArgs a)
         a.psts[c] = psts;
         a.beg[c] = ((unsigned)(x + 1) << 16) | ((unsigned)(y + 1) & 0xffffu);
         a.endc[c] = xx;
-        a.passed[c] = (a.scorethld < sc) ? 1 : 0;
+        a.passed[c] = (a.scorethld < maxsc && a.scorethld < sc) ? 1 : 0;
         (void)L;
     }
 }
 
 // ---------------------------------------------------------------------------
 // launchers (host)
+size_t p1t_smem_bytes(int cvcard)
+{
+    return (size_t)(cvcard * P1C_CVREP + P1T_WARPS * P1T_WARP_FLOATS) * sizeof(float);
+}
+
+int p1t_blocks_per_sm(int cvcard)
+{
+    int n = 0;
+    const size_t sm = p1t_smem_bytes(cvcard);
+    cudaFuncSetAttribute(p1t_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, p1t_kernel, P1T_WARPS * 32, sm);
+    return n;
+}
+
+cudaError_t launch_tc_pack(const float* drec, const long long* poff, const int* plen, const long long* ttile,
+                           int nprof, unsigned* tcdb, float* cold, cudaStream_t st)
+{
+    if (nprof <= 0) return cudaSuccess;
+    tc_pack_kernel<<<nprof, 128, 0, st>>>(drec, poff, plen, ttile, tcdb, cold);
+    return cudaGetLastError();
+}
+
 size_t p1c_smem_bytes(int cvcard)
 {
     return (size_t)(cvcard * P1C_CVREP + P1C_WARPS * P1C_WARP_FLOATS) * sizeof(float);
@@ -905,6 +1322,12 @@ size_t p1_smem_bytes(int cvcard)
 
 cudaError_t launch_p1(const P1Args& a, const float* qbkg, int which, int grid, cudaStream_t st)
 {
+    if (which == P1K_TENSOR) {
+        const size_t sm = p1t_smem_bytes(a.sc.cvcard);
+        cudaFuncSetAttribute(p1t_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        p1t_kernel<<<grid, P1T_WARPS * 32, sm, st>>>(a, qbkg);
+        return cudaGetLastError();
+    }
     if (which == P1K_CHUNKED) {
         const size_t sm = p1c_smem_bytes(a.sc.cvcard);
         cudaFuncSetAttribute(p1c_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

@@ -26,8 +26,11 @@ EXPORTS = [
     "c2_create", "c2_destroy", "c2_last_error", "c2_upload_db", "c2_set_query", "c2_run_phase1",
     "c2_get_phase1", "c2_run_finalize", "c2_get_finalize", "c2_get_thresholds", "c2_set_stream", "c2_sync",
     "c2_launch_count", "c2_run_stats", "c2_run_map", "c2_get_hits", "c2_search", "c2_get_search_space",
-    "c2_run_phase1_static",
+    "c2_run_phase1_static", "c2_set_score_mode",
 ]
+
+SCORE_FP32 = 0
+SCORE_BF16_TC = 1
 
 _fp = C.POINTER(C.c_float)
 _i32p = C.POINTER(C.c_int32)
@@ -105,6 +108,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.c2_search.argtypes = [C.c_void_p, P(c2_profiles), P(C.c_int32)]
     lib.c2_get_search_space.argtypes = [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]
     lib.c2_run_phase1_static.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.c2_set_score_mode.argtypes = [C.c_void_p, C.c_int32]
     for n in EXPORTS:
         getattr(lib, n).restype = C.c_int
     _lib = lib
@@ -238,6 +242,10 @@ class Handle:
 
     def sync(self):
         self._ck(self.lib.c2_sync(self._h), "c2_sync")
+
+    def set_score_mode(self, mode: int):
+        """SCORE_FP32 (CUDA cores) or SCORE_BF16_TC (split-BF16 tensor-core contractions)."""
+        self._ck(self.lib.c2_set_score_mode(self._h, mode), "c2_set_score_mode")
 
     def phase1(self):
         out = (c2_p1_result * self.nprof)()

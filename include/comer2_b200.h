@@ -206,6 +206,19 @@ c2_status c2_sync(c2_handle* h);
 /* Number of kernel launches issued by the handle since creation. */
 c2_status c2_launch_count(const c2_handle* h, uint64_t* n);
 
+/* Score arithmetic of phase 1 (no counterpart in the reference, which has
+ * only FP32):
+ *   C2_SCORE_FP32     the three score contractions in FP32 on the CUDA cores;
+ *   C2_SCORE_BF16_TC  the contractions as split-BF16 (hi + lo) tensor-core
+ *                     products with FP32 accumulation; the DP stays FP32.
+ * In BF16 mode the phase-1 maxima (c2_get_phase1) carry the BF16 rounding;
+ * pairs within a 2e-3 relative margin of the score threshold are recomputed
+ * in FP32 (traceback sweep), so the finalised scores, hits, E-values and
+ * alignments are those of the FP32 mode.  Default: C2_SCORE_FP32. */
+#define C2_SCORE_FP32 0
+#define C2_SCORE_BF16_TC 1
+c2_status c2_set_score_mode(c2_handle* h, int32_t mode);
+
 /* Phase 1 (as c2_run_phase1) that allocates nothing.  No counterpart in the
  * reference.  Its scratch (work counter, strip-boundary rows) lives in one
  * static 16 MiB device array per device, so the grid is limited to the 8-warp

@@ -1,6 +1,9 @@
 """GPU parity of phase 1 (fused score + Viterbi DP) and the DP finalisation
 against the CPU oracle, called through the C ABI.
 
+Both score modes are checked: FP32 on the CUDA cores and the split-BF16
+tensor-core contractions (mode 1), against the same FP32 oracle.
+
 Tolerance: DP maxima within 1e-4 relative.  The context-vector term maps a
 continuous value through a step table (rint(2x) bins), so a rounding
 difference near a bin edge moves one cell's score by one table step
@@ -15,9 +18,14 @@ from comer2_b200 import synth as S
 pytestmark = pytest.mark.gpu
 
 
-def _handle(params):
+MODES = [0, 1]   # native.SCORE_FP32, native.SCORE_BF16_TC
+
+
+def _handle(params, mode=0):
     from comer2_b200.native import Handle
-    return Handle(params, 0)
+    h = Handle(params, 0)
+    h.set_score_mode(mode)
+    return h
 
 
 def _oracle_all(orc, q, db, ks):
@@ -40,9 +48,10 @@ def _check_phase1(best, coords, ref, ks):
     return rel_ok
 
 
-def test_phase1_small_db(params, orc32):
+@pytest.mark.parametrize("mode", MODES)
+def test_phase1_small_db(params, orc32, mode):
     w = S.config(1, seed=3, scale=0.002)  # 200 profiles, 4 planted homologs
-    h = _handle(params)
+    h = _handle(params, mode)
     h.upload_db(w.db)
     h.set_query(w.queries[0])
     h.run_phase1()
@@ -55,13 +64,14 @@ def test_phase1_small_db(params, orc32):
         assert best[k] > 100.0
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("lq", [1, 5, 31, 32, 33, 64, 65, 97])
-def test_phase1_edge_lengths(params, orc32, lq):
+def test_phase1_edge_lengths(params, orc32, lq, mode):
     rng = np.random.default_rng(100 + lq)
     q = S.random_profiles(rng, [lq])
     lens = [1, 2, 5, 31, 32, 33, 63, 64, 65, 96, 130, 257]
     db = S.random_profiles(rng, lens)
-    h = _handle(params)
+    h = _handle(params, mode)
     h.upload_db(db)
     h.set_query(q)
     h.run_phase1()
@@ -72,14 +82,15 @@ def test_phase1_edge_lengths(params, orc32, lq):
     assert ok >= len(ks) - 1
 
 
-def test_phase1_homolog_long_alignments(params, orc32):
+@pytest.mark.parametrize("mode", MODES)
+def test_phase1_homolog_long_alignments(params, orc32, mode):
     """Planted homologs give maxima in the hundreds; their paths cross many
     strips, so the strip hand-off and the column -1 boundary are exercised."""
     rng = np.random.default_rng(11)
     q = S.random_profiles(rng, [300])
     parts = [S.planted_homolog(rng, q, L) for L in (40, 77, 128, 200, 333, 600)]
     db = S.concat(parts)
-    h = _handle(params)
+    h = _handle(params, mode)
     h.upload_db(db)
     h.set_query(q)
     h.run_phase1()

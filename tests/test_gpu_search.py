@@ -37,9 +37,10 @@ def _oracle_search(orc, prm, w, searchspace, thld, logevthld):
     return out
 
 
-def _run(params, w):
+def _run(params, w, mode=0):
     from comer2_b200.native import Handle
     h = Handle(params, 0)
+    h.set_score_mode(mode)
     h.upload_db(w.db)
     hits = h.search(w.queries[0])
     thld, logevthld = h.thresholds()
@@ -47,10 +48,11 @@ def _run(params, w):
     return h, hits, thld, logevthld, ss
 
 
+@pytest.mark.parametrize("mode", [0, 1])   # FP32 scores; split-BF16 tensor-core scores
 @pytest.mark.parametrize("seed", [2, 9])
-def test_search_matches_oracle(params, orc32, seed):
+def test_search_matches_oracle(params, orc32, seed, mode):
     w = S.config(1, seed=seed, scale=0.003)   # 300 profiles, 6 planted homologs
-    h, hits, thld, logevthld, ss = _run(params, w)
+    h, hits, thld, logevthld, ss = _run(params, w, mode)
     ref = _oracle_search(orc32, params, w, ss, thld, logevthld)
     ref_hits = sorted(k for k, v in ref.items() if "map" in v)
     got = sorted(int(x["profile"]) for x in hits)
