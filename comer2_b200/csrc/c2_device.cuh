@@ -117,6 +117,7 @@ struct P1Args {
     float* bnd;                 // per candidate at 10 x (cand_off / Lq): two last-row buffers [5][L]
     int* prog;                  // [ncand][nstrips] finished columns per strip
     unsigned long long* tbkey;  // [ncand] maximum of the traceback sweep and its cell, packed
+    const int* worder;          // traceback sweep: rank -> candidate (longest first)
     // tensor-core operands (P1K_TENSOR)
     const unsigned* tcdb;       // db B fragments
     const long long* ttile;     // [nprof] first tile of each profile

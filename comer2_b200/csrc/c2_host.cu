@@ -101,7 +101,7 @@ struct c2_handle {
     int ncand = 0;
     std::vector<int> h_cand;
     std::vector<long long> h_cand_off;
-    DevBuf<int> d_cand_prof;
+    DevBuf<int> d_cand_prof, d_worder;
     DevBuf<long long> d_cand_off;
     DevBuf<signed char> d_btck;
     DevBuf<float> d_smat, d_mmat;
@@ -757,6 +757,16 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
         return fail(h, C2_ERR_NOMEM, "finalisation scratch for %d pairs (%lld cells) failed", nc, acc);
     CK(cudaMemcpyAsync(h->d_cand_prof.p, h->h_cand.data(), (size_t)nc * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_cand_off.p, h->h_cand_off.data(), (size_t)nc * 8, cudaMemcpyHostToDevice, h->stream));
+    // traceback sweep order: longest candidates first
+    {
+        std::vector<int> wo(nc);
+        std::iota(wo.begin(), wo.end(), 0);
+        std::stable_sort(wo.begin(), wo.end(),
+                         [&](int x, int y) { return h->h_plen[h->h_cand[x]] > h->h_plen[h->h_cand[y]]; });
+        if (h->d_worder.ensure(nc)) return fail(h, C2_ERR_NOMEM, "candidate order allocation failed");
+        CK(cudaMemcpyAsync(h->d_worder.p, wo.data(), (size_t)nc * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
     P1Args a;
     fill_p1(h, a);
     a.nwork = nc;
@@ -768,6 +778,7 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     a.bnd = h->d_bnd.p;
     a.prog = h->d_prog.p;
     a.tbkey = h->d_tbkey.p;
+    a.worder = h->d_worder.p;
     const long long nitems = (long long)nc * ((h->Lq + 31) / 32);
     CK(cudaMemsetAsync(h->d_counter.p, 0, sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_prog.p, 0, (size_t)nitems * sizeof(int), h->stream));
@@ -914,6 +925,18 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
             h->h_mapcand.push_back(h->h_p2[i]);
             h->h_mappass.push_back(i);
         }
+    {
+        // longest pairs first: their strip chains are the longest
+        std::vector<int> ix(h->h_mapcand.size());
+        std::iota(ix.begin(), ix.end(), 0);
+        std::stable_sort(ix.begin(), ix.end(), [&](int x, int y) {
+            return h->h_plen[h->h_cand[h->h_mapcand[x]]] > h->h_plen[h->h_cand[h->h_mapcand[y]]];
+        });
+        std::vector<int> mc(ix.size()), mp(ix.size());
+        for (size_t i = 0; i < ix.size(); i++) { mc[i] = h->h_mapcand[ix[i]]; mp[i] = h->h_mappass[ix[i]]; }
+        h->h_mapcand.swap(mc);
+        h->h_mappass.swap(mp);
+    }
     h->nmap = (int)h->h_mapcand.size();
     *nhits = h->nmap;
     if (h->nmap == 0) return C2_OK;

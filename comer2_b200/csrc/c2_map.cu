@@ -96,6 +96,37 @@ __device__ __forceinline__ void trn_bwd(const float* __restrict__ t0, int i, int
     for (int k = 0; k < 7; k++) t7[k] = __ldg(b + k);
 }
 
+// Column transitions of a sweep in a per-warp ring of 64 columns x 12 floats
+// (16-byte reads of 8 lanes at consecutive columns hit distinct banks).  Lane
+// t processes column k - t at step k, so the columns in use at step k are
+// [k - 31, k]; chunk m (columns [32m, 32m + 32)) is written at the end of
+// step 32m - 1, into the half of chunk m - 2, whose last use was step 32m - 2.
+constexpr int MTRS = 12;
+
+template <bool BWD>
+__device__ __forceinline__ void map_trn_col(const float* __restrict__ t0, int j, int L, float* t7)
+{
+    // forward: column j; backward: mirrored column j = actual column L - 1 - j
+    if (BWD) trn_bwd(t0, L - 1 - j, L, t7);
+    else trn_fwd(t0, j, L, t7);
+}
+
+__device__ __forceinline__ void map_trn_store(float* ring, int j, const float* t7)
+{
+    float* o = ring + (j & 63) * MTRS;
+    *reinterpret_cast<float4*>(o) = make_float4(t7[0], t7[1], t7[2], t7[3]);
+    *reinterpret_cast<float4*>(o + 4) = make_float4(t7[4], t7[5], t7[6], 0.f);
+}
+
+__device__ __forceinline__ void map_trn_load(const float* ring, int j, float* t7)
+{
+    const float* o = ring + (j & 63) * MTRS;
+    const float4 a = *reinterpret_cast<const float4*>(o);
+    const float4 b = *reinterpret_cast<const float4*>(o + 4);
+    t7[0] = a.x; t7[1] = a.y; t7[2] = a.z; t7[3] = a.w;
+    t7[4] = b.x; t7[5] = b.y; t7[6] = b.z;
+}
+
 struct MapPair {
     int c, p, L, pass;
     long long off, toff, base;
@@ -131,9 +162,11 @@ __global__ void __launch_bounds__(MAPW * 32) map_fwd_kernel(MapArgs a, const flo
                                                       const float* __restrict__ qcf)
 {
     __shared__ float rings[MAPW][2][32][33];
+    __shared__ __align__(16) float trings[MAPW][64 * MTRS];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float(*rin)[33] = rings[wid][0];
     float(*rout)[33] = rings[wid][1];
+    float* trs = trings[wid];
     const int Lq = a.Lq;
     const int nstrips = (Lq + 31) >> 5;
     const int nitems = a.nmap * nstrips;
@@ -149,6 +182,16 @@ __global__ void __launch_bounds__(MAPW * 32) map_fwd_kernel(MapArgs a, const flo
         const int L = P.L;
         const float* __restrict__ dt0 = dtrn + P.toff;
         float* fb = a.fb + P.base;
+        // column transitions: chunk 0 into the ring, chunk 1 into registers
+        float tnx[7];
+        {
+            float t[7];
+            __syncwarp();
+            map_trn_col<false>(dt0, lane, L, t);
+            map_trn_store(trs, lane, t);
+            map_trn_col<false>(dt0, 32 + lane, L, tnx);
+            __syncwarp();
+        }
         float* bnd = a.bnd + (P.base / Lq) * 10;
         const float* botr = bnd + ((s + 1) & 1) * 5 * L;   // last row of strip s-1
         float* botw = bnd + (s & 1) * 5 * L;
@@ -176,29 +219,14 @@ __global__ void __launch_bounds__(MAPW * 32) map_fwd_kernel(MapArgs a, const flo
                 bnxt[f] = (s > 0 && 32 + lane < L) ? __ldcg(botr + f * L + 32 + lane) : binit[f];
             }
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
-            // column k's score and transitions are loaded one step ahead
+            // column k's score is loaded one step ahead
             float nsc = act ? map_score(a, P, r) : MLOG0;
-            float ntc[7];
-            trn_fwd(dt0, 0, L, ntc);
             for (int k = 0; k < L + 31; k++) {
-                float tc[7];
                 if (k < L) {
                     rin[k & 31][lane] = nsc;
-#pragma unroll
-                    for (int i = 0; i < 7; i++) tc[i] = ntc[i];
-                    if (k + 1 < L) {
-                        nsc = act ? map_score(a, P, (long long)(k + 1) * Lq + r) : MLOG0;
-                        trn_fwd(dt0, k + 1, L, ntc);
-                    }
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 7; i++) tc[i] = MLOG0;
+                    if (k + 1 < L) nsc = act ? map_score(a, P, (long long)(k + 1) * Lq + r) : MLOG0;
                 }
-#pragma unroll
-                for (int i = 0; i < 7; i++) {
-                    const float x = __shfl_up_sync(FULL, t7[i], 1);
-                    t7[i] = (lane == 0) ? tc[i] : x;
-                }
+                map_trn_load(trs, k - lane, t7);
                 S5 up;
                 up.MM = __shfl_up_sync(FULL, mine.MM, 1);
                 up.MI = __shfl_up_sync(FULL, mine.MI, 1);
@@ -248,6 +276,12 @@ __global__ void __launch_bounds__(MAPW * 32) map_fwd_kernel(MapArgs a, const flo
                 upp = up;
                 const int cfl = k - 31;
                 if (cfl >= 0 && cfl < L && act) fb[(long long)cfl * Lq + r] = rout[cfl & 31][lane];
+                if ((k & 31) == 31) {
+                    // columns of chunk k / 32 + 1 into the ring, the next chunk into registers
+                    __syncwarp();
+                    map_trn_store(trs, k + 1 + lane, tnx);
+                    map_trn_col<false>(dt0, k + 33 + lane, L, tnx);
+                }
                 __syncwarp();
             }
         }
@@ -285,9 +319,11 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
                                                       const float* __restrict__ dtrn)
 {
     __shared__ float rings[MAPW][2][32][33];
+    __shared__ __align__(16) float trings[MAPW][64 * MTRS];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float(*rin)[33] = rings[wid][0];
     float(*rout)[33] = rings[wid][1];
+    float* trs = trings[wid];
     const int Lq = a.Lq;
     const int nstrips = (Lq + 31) >> 5;
     const int nitems = a.nmap * nstrips;
@@ -303,6 +339,16 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
         const int L = P.L;
         const float* __restrict__ dt0 = dtrn + P.toff;
         float* fb = a.fb + P.base;
+        // column transitions: chunk 0 into the ring, chunk 1 into registers
+        float tnx[7];
+        {
+            float t[7];
+            __syncwarp();
+            map_trn_col<true>(dt0, lane, L, t);
+            map_trn_store(trs, lane, t);
+            map_trn_col<true>(dt0, 32 + lane, L, tnx);
+            __syncwarp();
+        }
         float* bnd = a.bnd + (P.base / Lq) * 10;
         const float* botr = bnd + ((s + 1) & 1) * 5 * L;   // last row of mirrored strip s-1
         float* botw = bnd + (s & 1) * 5 * L;
@@ -330,34 +376,21 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
             // loads of mirrored column k (diagonal-successor score, transitions,
             // and the F value to add B to) are issued one step ahead
             float nsc = hasdn ? map_score(a, P, (long long)(L - 1) * Lq + r + 1) : MLOG0;
-            float ntc[7];
-            trn_bwd(dt0, L - 1, L, ntc);
             float nfb = act ? fb[(long long)(L - 1) * Lq + r] : 0.f;
             for (int k = 0; k < L + 31; k++) {
                 const int j = k - lane;         // mirrored column
                 // diagonal-successor score of column j, read before this step's
                 // write can reuse its ring slot (lane 31 reads slot (k+1)&31 = k&31)
                 const float sco = (j >= 1 && j < L) ? rin[(j - 1) & 31][lane] : MLOG0;
-                float tc[7];
                 if (k < L) {
                     // score of the diagonal successor of mirrored column k+1
                     rin[k & 31][lane] = nsc;
-#pragma unroll
-                    for (int i = 0; i < 7; i++) tc[i] = ntc[i];
                     if (k + 1 < L) {
                         const int ca1 = L - 2 - k;   // actual column of mirrored column k+1
                         nsc = hasdn ? map_score(a, P, (long long)ca1 * Lq + r + 1) : MLOG0;
-                        trn_bwd(dt0, ca1, L, ntc);
                     }
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 7; i++) tc[i] = MLOG0;
                 }
-#pragma unroll
-                for (int i = 0; i < 7; i++) {
-                    const float x = __shfl_up_sync(FULL, t7[i], 1);
-                    t7[i] = (lane == 0) ? tc[i] : x;
-                }
+                map_trn_load(trs, j, t7);
                 S5 dn;   // successor below (mirrored "up")
                 dn.MM = __shfl_up_sync(FULL, mine.MM, 1);
                 dn.MI = __shfl_up_sync(FULL, mine.MI, 1);
@@ -402,6 +435,12 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
                 if (cfl >= 0 && cfl < L && act) {
                     fb[(long long)(L - 1 - cfl) * Lq + r] = nfb + rout[cfl & 31][lane];
                     if (cfl + 1 < L) nfb = fb[(long long)(L - 2 - cfl) * Lq + r];
+                }
+                if ((k & 31) == 31) {
+                    // mirrored columns of chunk k / 32 + 1 into the ring, the next chunk into registers
+                    __syncwarp();
+                    map_trn_store(trs, k + 1 + lane, tnx);
+                    map_trn_col<true>(dt0, k + 33 + lane, L, tnx);
                 }
                 __syncwarp();
             }
