@@ -44,6 +44,15 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def _bf16_peak():
+    """Dense BF16 tensor throughput (TFLOP/s): measured burst figure, else the fallback."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            return float(json.load(fh).get("bf16_tflops", 1590.0))
+    return 1590.0
+
+
 def _traffic_per_position():
     """DRAM bytes per db position of the phase-1 kernel from the committed ncu summary."""
     p = os.path.join(ROOT, "profiles", "p1_kernel_traffic.json")
@@ -213,37 +222,53 @@ def main():
         e[2].synchronize()
         return e[0].elapsed_time(e[2]), e[0].elapsed_time(e[1]), nh
 
-    h.set_query(q)
-    for _ in range(args.warmup):
-        device_step()
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+    def measure(mode):
+        """Device-timed search (inputs resident) and end-to-end search through
+        the C ABI (query from host memory, hits and alignments back) in one
+        score mode."""
+        h.set_score_mode(mode)
+        h.set_query(q)
+        for _ in range(args.warmup):
+            device_step()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        l0 = h.launch_count()
+        tot, p1 = [], []
+        for _ in range(args.steps):
+            a, b, _ = device_step()
+            tot.append(a)
+            p1.append(b)
+        torch.cuda.synchronize()
+        launches = h.launch_count() - l0
+        if world > 1:
+            torch.distributed.barrier()
+        ms = _max_over_ranks(float(np.mean(tot)), world, backend)
+        p1ms = _max_over_ranks(float(np.mean(p1)), world, backend)
+        e2e = []
+        hits = []
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            hits = h.search(q)
+            torch.cuda.synchronize()
+            e2e.append((time.perf_counter() - t0) * 1e3)
+        e2e_ms = _max_over_ranks(float(np.mean(e2e)), world, backend)
+        return {"ms": ms, "p1ms": p1ms, "e2e_ms": e2e_ms, "launches": launches, "hits": hits}
+
+    from comer2_b200.native import SCORE_BF16_TC, SCORE_FP32
     clk = ClockSampler(local)
     clk.start()
-    l0 = h.launch_count()
-    tot, p1, nh = [], [], 0
-    for _ in range(args.steps):
-        a, b, nh = device_step()
-        tot.append(a)
-        p1.append(b)
-    torch.cuda.synchronize()
-    launches = h.launch_count() - l0
-    if world > 1:
-        torch.distributed.barrier()
-    ms = _max_over_ranks(float(np.mean(tot)), world, backend)
-    p1ms = _max_over_ranks(float(np.mean(p1)), world, backend)
-    # e2e: host buffers through the C ABI (query upload + search + hits back)
-    e2e = []
-    hits = []
-    for _ in range(args.steps):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        hits = h.search(q)
-        torch.cuda.synchronize()
-        e2e.append((time.perf_counter() - t0) * 1e3)
+    res = {"bf16": measure(SCORE_BF16_TC), "fp32": measure(SCORE_FP32)}
     clocks = clk.stop()
-    e2e_ms = _max_over_ranks(float(np.mean(e2e)), world, backend)
+    main_r = res[args.score_mode]
+    ms, p1ms, e2e_ms, launches, hits = (main_r["ms"], main_r["p1ms"], main_r["e2e_ms"], main_r["launches"],
+                                        main_r["hits"])
+
+    def hitset(hs):
+        return [(int(x["profile"]), round(float(x["logE"]), 3)) for x in hs]
+
+    same_hits = hitset(res["bf16"]["hits"]) == hitset(res["fp32"]["hits"])
     nprof = w.db.nprofiles
     h2d = Lq * (64 + 6) * 4 + (Lq + 1) * 7 * 4 + 2 * Lq + 20 * 4
     d2h = nprof * 4 + sum(5 * (x["alnlen"] + 1) for x in hits) + len(hits) * 80
@@ -252,10 +277,14 @@ def main():
     alg_bytes = 209.0 * npos                      # FP32 profile fields streamed per query pass
     achieved = alg_bytes / (p1ms * 1e-3) / 1e9
     tpp = _traffic_per_position()
+    gc = lambda t: world * cells / (t * 1e-3) / 1e9   # noqa: E731
+    bf, fp = res["bf16"], res["fp32"]
     line = {
-        "metric": METRIC, "value": world * cells / (ms * 1e-3) / 1e9, "unit": UNIT, "n_gpus": world,
+        "metric": METRIC, "value": gc(ms), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16" if args.score_mode == "bf16" else "f32",
+        "data": "synthetic",
         "config": {"workload": WORKLOAD, "cells_per_gpu": cells, "db_profiles": nprof, "db_positions": npos,
                    "scale": args.scale, "l2": "inputs larger than L2 (db records %.1f GB)" % (npos * 224 / 1e9),
                    "parallelism": "db replicas, one per GPU" if world > 1 else "single GPU"},
@@ -264,7 +293,22 @@ def main():
         "gpu_launches": launches,
         "hits": len(hits), "homologs_found": int(sum(1 for x in hits if x["profile"] in set(w.homologs.tolist()))),
         "stage_ms": {"phase1": p1ms, "finalize+stats+map": ms - p1ms},
-        "roofline": {"kernel": "p1_kernel (fused score + Viterbi DP)", "bound": "hbm",
+        "score_forms": {
+            "bf16": {"what": "score contractions as split-BF16 (hi+lo) tensor-core mma.sync, FP32 accumulate and DP",
+                     "value": gc(bf["ms"]), "e2e": gc(bf["e2e_ms"]), "phase1_ms": bf["p1ms"],
+                     "ms_per_step": bf["ms"]},
+            "fp32": {"what": "score contractions in FP32 on the CUDA cores, FP32 DP",
+                     "value": gc(fp["ms"]), "e2e": gc(fp["e2e_ms"]), "phase1_ms": fp["p1ms"],
+                     "ms_per_step": fp["ms"]},
+            "bf16_over_fp32_e2e": fp["e2e_ms"] / bf["e2e_ms"],
+            "same_hit_lists": same_hits},
+        "tensor_pipe": {"kernel": "p1t_kernel", "useful_flops_per_cell": 40,
+                        "achieved_tflops": 40.0 * cells / (bf["p1ms"] * 1e-3) / 1e12,
+                        "peak_tflops": _bf16_peak(), "frac": 40.0 * cells / (bf["p1ms"] * 1e-3) / 1e12 / _bf16_peak(),
+                        "note": "40 flops/cell = the amino-acid contraction (20 multiply-adds); executed tensor "
+                                "work is 3 split products x 3 contractions x K 32"},
+        "roofline": {"kernel": ("p1t_kernel" if args.score_mode == "bf16" else "p1c_kernel")
+                               + " (fused score + Viterbi DP)", "bound": "hbm",
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                      "peak_kind": peak_kind,
                      "traffic": (tpp * npos) if tpp else None,
