@@ -1081,18 +1081,46 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                     cp_async_wait_1();   // column records of chunk m have landed
                     __syncwarp();
                     stage_cols(cring, cold, m + 2, L, lane);
-                    // ---- score stage: 32 x 32 tile of chunk m on the tensor cores
-#pragma unroll 1
-                    for (int nt = 0; nt < 4; nt++) {
-                        const unsigned* tb = tb0 + (long long)(4 * m + nt) * TC_TILE_WORDS + lane * 2;
-                        uint2 B[3][2][2];
+                    // the next chunk's db operands (12 KB) towards L2 while this one is used
+                    if (m + 1 < nch) {
+                        const char* nx = reinterpret_cast<const char*>(tb0 + (long long)(4 * m + 4) * TC_TILE_WORDS);
+#pragma unroll
+                        for (int i = 0; i < 3; i++)
+                            asm volatile("prefetch.global.L2 [%0];" ::"l"(nx + (i * 32 + lane) * 128));
+                    }
+                    // ---- score stage: 32 x 32 tile of chunk m on the tensor cores;
+                    // the fragments of tile nt + 1 are loaded before the products of tile nt
+                    uint2 Bn[3][2][2];
+                    {
+                        const unsigned* tb = tb0 + (long long)(4 * m) * TC_TILE_WORDS + lane * 2;
 #pragma unroll
                         for (int d = 0; d < 3; d++)
 #pragma unroll
                             for (int kt = 0; kt < 2; kt++)
 #pragma unroll
                                 for (int sp = 0; sp < 2; sp++)
-                                    B[d][kt][sp] = __ldg(reinterpret_cast<const uint2*>(tb + ((d * 2 + kt) * 2 + sp) * 64));
+                                    Bn[d][kt][sp] = __ldg(reinterpret_cast<const uint2*>(tb + ((d * 2 + kt) * 2 + sp) * 64));
+                    }
+#pragma unroll 1
+                    for (int nt = 0; nt < 4; nt++) {
+                        uint2 B[3][2][2];
+#pragma unroll
+                        for (int d = 0; d < 3; d++)
+#pragma unroll
+                            for (int kt = 0; kt < 2; kt++)
+#pragma unroll
+                                for (int sp = 0; sp < 2; sp++) B[d][kt][sp] = Bn[d][kt][sp];
+                        if (nt < 3) {
+                            const unsigned* tb = tb0 + (long long)(4 * m + nt + 1) * TC_TILE_WORDS + lane * 2;
+#pragma unroll
+                            for (int d = 0; d < 3; d++)
+#pragma unroll
+                                for (int kt = 0; kt < 2; kt++)
+#pragma unroll
+                                    for (int sp = 0; sp < 2; sp++)
+                                        Bn[d][kt][sp] =
+                                            __ldg(reinterpret_cast<const uint2*>(tb + ((d * 2 + kt) * 2 + sp) * 64));
+                        }
                         const int c0 = 32 * m + 8 * nt + 2 * q;
                         const float* cr0 = cring + (c0 & (P1T_CRING - 1)) * P1C_TRS;
                         const float* cr1 = cring + ((c0 + 1) & (P1T_CRING - 1)) * P1C_TRS;
