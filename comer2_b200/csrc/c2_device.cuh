@@ -85,9 +85,11 @@ constexpr int P1C_WARP_FLOATS =
 // fragment-layout writes and the per-lane wavefront reads are both free of
 // bank conflicts), a column-record ring of 4 chunks, the row above the strip
 // and the pair-scaled amino-acid A fragments of the strip ([mt][kt][split][lane][4])
-constexpr int P1T_WARPS = 11;
+// and two slots for db operand tiles (bulk async copies, one mbarrier each)
+constexpr int P1T_WARPS = 9;
 constexpr int P1T_RLD = 36, P1T_CRING = 128;
-constexpr int P1T_WARP_FLOATS = P1C_RING * P1T_RLD + P1T_CRING * P1C_TRS + 32 * 8 + 2 * 2 * 2 * 32 * 4;
+constexpr int P1T_WARP_FLOATS =
+    P1C_RING * P1T_RLD + P1T_CRING * P1C_TRS + 32 * 8 + 2 * 2 * 2 * 32 * 4 + 2 * TC_TILE_WORDS + 4;
 
 struct P1Args {
     const float* qrec;      // [Lq][QR_STRIDE]

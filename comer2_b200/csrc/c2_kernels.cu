@@ -851,6 +851,41 @@ __device__ __forceinline__ void mma_bf16(float* d, const unsigned* a, unsigned b
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+// mbarrier and bulk (non-tensor, non-multicast) async copy helpers
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// one thread: expect `bytes` on the barrier and start the copy global -> shared
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Wait for phase `parity` of the barrier to complete; gives up after a bounded
+// number of polls (returns false; the caller records a device status).
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity)
+{
+    const unsigned a = smem_u32(bar);
+    for (int it = 0; it < (1 << 22); it++) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
 // Pack the db operands of one profile per CTA (4 warps over its 8-column
 // tiles) and its column records.
 __global__ void __launch_bounds__(128) tc_pack_kernel(const float* __restrict__ drec, const long long* __restrict__ poff,
@@ -968,8 +1003,16 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
     float* cring = ring + P1C_RING * P1T_RLD;                 // [P1T_CRING][P1C_TRS] column records
     float* bnd = cring + P1T_CRING * P1C_TRS;                 // [32][8] row above the strip
     uint4* aas = reinterpret_cast<uint4*>(bnd + 32 * 8);      // [mt][kt][split][lane] amino-acid A fragments
+    unsigned* btile = reinterpret_cast<unsigned*>(aas + 2 * 2 * 2 * 32);   // [2][TC_TILE_WORDS] db operand tiles
+    unsigned long long* tbar = reinterpret_cast<unsigned long long*>(btile + 2 * TC_TILE_WORDS);  // [2]
     for (int i = threadIdx.x; i < cvcard * P1C_CVREP; i += blockDim.x) cvtab[i] = a.cvvals[i / P1C_CVREP];
+    if (lane == 0) {
+        mbar_init(tbar, 1);
+        mbar_init(tbar + 1, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     __syncthreads();
+    unsigned tph0 = 0, tph1 = 0;   // phase parity of the two tile slots
 
     const long long slotw = (long long)blockIdx.x * P1T_WARPS + wid;
     const int Lmax = (int)(a.botstride / 10);
@@ -1076,6 +1119,12 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
             const int nch = (L + 31) >> 5;
             const int kend = L + 31;
             const unsigned* __restrict__ qa = a.qa + (long long)s * TC_QA_WORDS;
+            // db operand tiles T = 4m + nt stream through the two slots, two tiles ahead
+            const int ntile = 4 * nch;
+            if (lane == 0) {
+                bulk_load(btile, tb0, TC_TILE_WORDS * 4, tbar);
+                bulk_load(btile + TC_TILE_WORDS, tb0 + TC_TILE_WORDS, TC_TILE_WORDS * 4, tbar + 1);
+            }
             for (int m = 0; 32 * m < kend; m++) {
                 if (m < nch) {
                     cp_async_wait_1();   // column records of chunk m have landed
@@ -1088,39 +1137,27 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                         for (int i = 0; i < 3; i++)
                             asm volatile("prefetch.global.L2 [%0];" ::"l"(nx + (i * 32 + lane) * 128));
                     }
-                    // ---- score stage: 32 x 32 tile of chunk m on the tensor cores;
-                    // the fragments of tile nt + 1 are loaded before the products of tile nt
-                    uint2 Bn[3][2][2];
-                    {
-                        const unsigned* tb = tb0 + (long long)(4 * m) * TC_TILE_WORDS + lane * 2;
-#pragma unroll
-                        for (int d = 0; d < 3; d++)
-#pragma unroll
-                            for (int kt = 0; kt < 2; kt++)
-#pragma unroll
-                                for (int sp = 0; sp < 2; sp++)
-                                    Bn[d][kt][sp] = __ldg(reinterpret_cast<const uint2*>(tb + ((d * 2 + kt) * 2 + sp) * 64));
-                    }
+                    // ---- score stage: 32 x 32 tile of chunk m on the tensor cores
 #pragma unroll 1
                     for (int nt = 0; nt < 4; nt++) {
+                        const int T = 4 * m + nt, sl = T & 1;
+                        const bool got = mbar_wait(tbar + sl, sl ? tph1 : tph0);
+                        if (sl) tph1 ^= 1u; else tph0 ^= 1u;
+                        if (!got && lane == 0 && a.status) atomicCAS(a.status, 0, PIPE_ERR_TIMEOUT);
+                        const unsigned* bt = btile + sl * TC_TILE_WORDS + lane * 2;
                         uint2 B[3][2][2];
 #pragma unroll
                         for (int d = 0; d < 3; d++)
 #pragma unroll
                             for (int kt = 0; kt < 2; kt++)
 #pragma unroll
-                                for (int sp = 0; sp < 2; sp++) B[d][kt][sp] = Bn[d][kt][sp];
-                        if (nt < 3) {
-                            const unsigned* tb = tb0 + (long long)(4 * m + nt + 1) * TC_TILE_WORDS + lane * 2;
-#pragma unroll
-                            for (int d = 0; d < 3; d++)
-#pragma unroll
-                                for (int kt = 0; kt < 2; kt++)
-#pragma unroll
-                                    for (int sp = 0; sp < 2; sp++)
-                                        Bn[d][kt][sp] =
-                                            __ldg(reinterpret_cast<const uint2*>(tb + ((d * 2 + kt) * 2 + sp) * 64));
-                        }
+                                for (int sp = 0; sp < 2; sp++)
+                                    B[d][kt][sp] = *reinterpret_cast<const uint2*>(bt + ((d * 2 + kt) * 2 + sp) * 64);
+                        // slot free once every lane holds its fragments: tile T + 2 into it
+                        __syncwarp();
+                        if (lane == 0 && T + 2 < ntile)
+                            bulk_load(btile + sl * TC_TILE_WORDS, tb0 + (long long)(T + 2) * TC_TILE_WORDS,
+                                      TC_TILE_WORDS * 4, tbar + sl);
                         const int c0 = 32 * m + 8 * nt + 2 * q;
                         const float* cr0 = cring + (c0 & (P1T_CRING - 1)) * P1C_TRS;
                         const float* cr1 = cring + ((c0 + 1) & (P1T_CRING - 1)) * P1C_TRS;
