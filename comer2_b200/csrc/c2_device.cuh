@@ -120,6 +120,7 @@ struct P1Args {
     int* prog;                  // [ncand][nstrips] finished columns per strip
     unsigned long long* tbkey;  // [ncand] maximum of the traceback sweep and its cell, packed
     const int* worder;          // traceback sweep: rank -> candidate (longest first)
+    const int* items;           // traceback sweep: work item -> rank * nstrips + strip
     // tensor-core operands (P1K_TENSOR)
     const unsigned* tcdb;       // db B fragments
     const long long* ttile;     // [nprof] first tile of each profile
@@ -155,8 +156,10 @@ struct FinArgs {
 // ---------------------------------------------------------------------------
 // Phase-2 sweeps (traceback DP, MAP forward/backward/MAP DP) run one strip of
 // one pair per warp: a work item is (pair m, strip s), items are handed out
-// in order from a global counter, so the item a warp waits on was taken
-// earlier by a warp that is running.  Strip s writes its last row (5 states
+// in the order of a host-built table from a global counter.  The table puts
+// (m, s) after (m, s - 1) (ordered by m + K s, K = pairs started per strip
+// lag), so the item a warp waits on was taken earlier by a warp that is
+// running, and strips are handed out about when their predecessor is ready.  Strip s writes its last row (5 states
 // per column) to bnd[m][s & 1][5][L] and publishes the number of finished
 // columns in prog[m * nstrips + s]; strip s+1 waits for the columns it
 // prefetches.  A long pair is thus swept by up to nstrips warps at once

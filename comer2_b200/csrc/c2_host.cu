@@ -101,7 +101,7 @@ struct c2_handle {
     int ncand = 0;
     std::vector<int> h_cand;
     std::vector<long long> h_cand_off;
-    DevBuf<int> d_cand_prof, d_worder;
+    DevBuf<int> d_cand_prof, d_worder, d_tbitems, d_mapitems;
     DevBuf<long long> d_cand_off;
     DevBuf<signed char> d_btck;
     DevBuf<float> d_smat, d_mmat;
@@ -360,6 +360,28 @@ static inline void trn_of(const c2_profiles* d, int k, int i, float* t7)
     const float* b = a + 7;
     t7[TMM] = a[0]; t7[TMI] = b[1]; t7[TMD] = a[2];
     t7[TIM] = a[3]; t7[TII] = b[4]; t7[TDM] = a[5]; t7[TDD] = a[6];
+}
+
+// Work-item table of a strip-pipelined sweep over np pairs (in processing
+// order, lengths lens): item (p, s) at key p + K s, K = pairs started per
+// strip lag when nwarps warps are busy, so that strip s of a pair is handed
+// out about when strip s - 1 is far enough ahead (a strip needs 64 columns
+// of its predecessor, which lags ~96 wavefront steps).  Ties keep s order, so
+// (p, s - 1) always precedes (p, s).
+static void strip_items(const std::vector<int>& lens, int nstrips, int nwarps, std::vector<int>& items)
+{
+    const int np = (int)lens.size();
+    double lm = 31.0;
+    for (int L : lens) lm += (double)L / std::max(1, np);
+    const double K = 96.0 * nwarps / (nstrips * lm);
+    std::vector<std::pair<double, int>> key((size_t)np * nstrips);
+    for (int p = 0; p < np; p++)
+        for (int s = 0; s < nstrips; s++) key[(size_t)p * nstrips + s] = {p + K * s, p * nstrips + s};
+    std::stable_sort(key.begin(), key.end(), [&](const std::pair<double, int>& x, const std::pair<double, int>& y) {
+        return x.first < y.first;
+    });
+    items.resize(key.size());
+    for (size_t i = 0; i < key.size(); i++) items[i] = key[i].second;
 }
 
 // candidate margin and traceback tolerance of the BF16 score mode (relative)
@@ -763,8 +785,13 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
         std::iota(wo.begin(), wo.end(), 0);
         std::stable_sort(wo.begin(), wo.end(),
                          [&](int x, int y) { return h->h_plen[h->h_cand[x]] > h->h_plen[h->h_cand[y]]; });
-        if (h->d_worder.ensure(nc)) return fail(h, C2_ERR_NOMEM, "candidate order allocation failed");
+        std::vector<int> lens(nc), items;
+        for (int i = 0; i < nc; i++) lens[i] = h->h_plen[h->h_cand[wo[i]]];
+        strip_items(lens, (h->Lq + 31) / 32, h->grid * P1_WARPS, items);
+        if (h->d_worder.ensure(nc) || h->d_tbitems.ensure(items.size()))
+            return fail(h, C2_ERR_NOMEM, "candidate order allocation failed");
         CK(cudaMemcpyAsync(h->d_worder.p, wo.data(), (size_t)nc * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->d_tbitems.p, items.data(), items.size() * 4, cudaMemcpyHostToDevice, h->stream));
         CK(cudaStreamSynchronize(h->stream));
     }
     P1Args a;
@@ -779,6 +806,7 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     a.prog = h->d_prog.p;
     a.tbkey = h->d_tbkey.p;
     a.worder = h->d_worder.p;
+    a.items = h->d_tbitems.p;
     const long long nitems = (long long)nc * ((h->Lq + 31) / 32);
     CK(cudaMemsetAsync(h->d_counter.p, 0, sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_prog.p, 0, (size_t)nitems * sizeof(int), h->stream));
@@ -950,6 +978,14 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
         h->d_pairc.ensure(nm) || h->d_alninfo.ensure((size_t)nm * 8) || h->d_aln.ensure((size_t)nm * 5 * h->alnstride) ||
         h->d_pairk.ensure(nm))
         return fail(h, C2_ERR_NOMEM, "MAP buffers for %d pairs failed", nm);
+    {
+        std::vector<int> lens(nm), items;
+        for (int i = 0; i < nm; i++) lens[i] = h->h_plen[h->h_cand[h->h_mapcand[i]]];
+        strip_items(lens, (h->Lq + 31) / 32, h->grid * P1_WARPS, items);
+        if (h->d_mapitems.ensure(items.size())) return fail(h, C2_ERR_NOMEM, "MAP work table allocation failed");
+        CK(cudaMemcpyAsync(h->d_mapitems.p, items.data(), items.size() * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
     CK(cudaMemcpyAsync(h->d_mapcand.p, h->h_mapcand.data(), (size_t)nm * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_mappass.p, h->h_mappass.data(), (size_t)nm * 4, cudaMemcpyHostToDevice, h->stream));
     MapArgs a;
@@ -972,6 +1008,7 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
     a.bnd = h->d_bnd.p;
     a.prog = h->d_prog.p;
     a.pairk = h->d_pairk.p;
+    a.items = h->d_mapitems.p;
     a.status = h->d_status.p;
     a.counter = h->d_counter.p;
     a.minpp = h->prm.minpp;

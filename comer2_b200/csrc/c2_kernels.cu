@@ -378,7 +378,8 @@ p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
         if (lane == 0) item = atomicAdd(a.counter, 1);
         item = __shfl_sync(FULL, item, 0);
         if (item >= nitems) break;
-        const int rank = item / nstrips, s = item - rank * nstrips;
+        const int iv = a.items[item];
+        const int rank = iv / nstrips, s = iv - rank * nstrips;
         const int cand = a.worder[rank];
         const int p = a.order[cand];
         const int L = a.plen[p];

@@ -177,7 +177,8 @@ __global__ void __launch_bounds__(MAPW * 32) map_fwd_kernel(MapArgs a, const flo
         if (lane == 0) item = atomicAdd(a.counter, 1);
         item = __shfl_sync(FULL, item, 0);
         if (item >= nitems) break;
-        const int m = item / nstrips, s = item - m * nstrips;
+        const int iv = a.items[item];
+        const int m = iv / nstrips, s = iv - m * nstrips;
         const MapPair P = map_pair(a, qtrn, m);
         const int L = P.L;
         const float* __restrict__ dt0 = dtrn + P.toff;
@@ -334,7 +335,8 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
         if (lane == 0) item = atomicAdd(a.counter, 1);
         item = __shfl_sync(FULL, item, 0);
         if (item >= nitems) break;
-        const int m = item / nstrips, s = item - m * nstrips;
+        const int iv = a.items[item];
+        const int m = iv / nstrips, s = iv - m * nstrips;
         const MapPair P = map_pair(a, qtrn, m);
         const int L = P.L;
         const float* __restrict__ dt0 = dtrn + P.toff;
@@ -476,7 +478,8 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
         if (lane == 0) item = atomicAdd(a.counter, 1);
         item = __shfl_sync(FULL, item, 0);
         if (item >= nitems) break;
-        const int m = item / nstrips, s = item - m * nstrips;
+        const int iv = a.items[item];
+        const int m = iv / nstrips, s = iv - m * nstrips;
         const int c = a.map_cand[m];
         const int p = a.cand_prof[c];
         const int L = a.plen[p];

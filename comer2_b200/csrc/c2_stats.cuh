@@ -54,6 +54,7 @@ struct MapArgs {
     unsigned* pairc;            // [nmap]: MAP end coordinates
     float* bnd;                 // per candidate at 10 x (cand_off / Lq): two last-row buffers [5][L]
     int* prog;                  // [ncand][nstrips] finished columns per strip
+    const int* items;           // work item -> m * nstrips + strip (ready-time order)
     unsigned long long* pairk;  // [nmap] MAP DP maximum and end cell, packed for atomicMax
     int* status;
     int* counter;
