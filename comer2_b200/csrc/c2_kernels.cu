@@ -998,15 +998,15 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
     extern __shared__ float smem[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int cvcard = a.sc.cvcard;
-    float* cvtab = smem;                                      // [cvcard][P1C_CVREP]
-    float* wb = smem + cvcard * P1C_CVREP + wid * P1T_WARP_FLOATS;
+    float* cvtab = smem;                                      // [cvcard][P1T_CVREP]
+    float* wb = smem + cvcard * P1T_CVREP + wid * P1T_WARP_FLOATS;
     float* ring = wb;                                         // [P1C_RING][P1T_RLD] scores
     float* cring = ring + P1C_RING * P1T_RLD;                 // [P1T_CRING][P1C_TRS] column records
     float* bnd = cring + P1T_CRING * P1C_TRS;                 // [32][8] row above the strip
     uint4* aas = reinterpret_cast<uint4*>(bnd + 32 * 8);      // [mt][kt][split][lane] amino-acid A fragments
     unsigned* btile = reinterpret_cast<unsigned*>(aas + 2 * 2 * 2 * 32);   // [2][TC_TILE_WORDS] db operand tiles
     unsigned long long* tbar = reinterpret_cast<unsigned long long*>(btile + 2 * TC_TILE_WORDS);  // [2]
-    for (int i = threadIdx.x; i < cvcard * P1C_CVREP; i += blockDim.x) cvtab[i] = a.cvvals[i / P1C_CVREP];
+    for (int i = threadIdx.x; i < cvcard * P1T_CVREP; i += blockDim.x) cvtab[i] = a.cvvals[i / P1T_CVREP];
     if (lane == 0) {
         mbar_init(tbar, 1);
         mbar_init(tbar + 1, 1);
@@ -1201,7 +1201,7 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
 #pragma unroll
                                 for (int e = 0; e < 2; e++) {
                                     const int i = 2 * hh + e;
-                                    const float S = tc_epilogue<P1C_CVREP>(acc[0][i], acc[1][i], acc[2][i],
+                                    const float S = tc_epilogue<P1T_CVREP>(acc[0][i], acc[1][i], acc[2][i],
                                                                            rq[mt][hh][0], rq[mt][hh][1], rq[mt][hh][2],
                                                                            cd[e], pd[e], hd[e], cvtab, sc, lane);
                                     ring[((c0 + e) & (P1C_RING - 1)) * P1T_RLD + 16 * mt + g + 8 * hh] = S;
@@ -1348,7 +1348,7 @@ __global__ void __launch_bounds__(256) fin_kernel(FinArgs a)
 // launchers (host)
 size_t p1t_smem_bytes(int cvcard)
 {
-    return (size_t)(cvcard * P1C_CVREP + P1T_WARPS * P1T_WARP_FLOATS) * sizeof(float);
+    return (size_t)(cvcard * P1T_CVREP + P1T_WARPS * P1T_WARP_FLOATS) * sizeof(float);
 }
 
 int p1t_blocks_per_sm(int cvcard)
