@@ -19,6 +19,7 @@
 #include "../../include/comer2_b200.h"
 #include "c2_device.cuh"
 #include "c2_stats.cuh"
+#include "c2_adj.cuh"
 
 namespace c2 {
 cudaError_t launch_stats(const StatsArgs& a, cudaStream_t st);
@@ -28,7 +29,7 @@ size_t p1_smem_bytes(int cvcard);
 cudaError_t launch_p1(const P1Args& a, const float* qbkg, int which, int grid, cudaStream_t st);
 int p1_blocks_per_sm(int cvcard);
 int p1c_blocks_per_sm(int cvcard);
-int p1t_blocks_per_sm(int cvcard);
+int p1t_blocks_per_sm(int cvcard, cudaError_t* err);
 cudaError_t launch_tc_pack(const float* drec, const long long* poff, const int* plen, const long long* ttile,
                            int nprof, unsigned* tcdb, float* cold, cudaStream_t st);
 cudaError_t launch_fin(const FinArgs& a, cudaStream_t st);
@@ -87,7 +88,17 @@ struct c2_handle {
     int Lq = 0;
     float qeno = 0.f;
     std::vector<float> h_qrec;
-    DevBuf<float> d_qrec, d_qbkg, d_qtrn, d_qcf;
+    DevBuf<float> d_qrec, d_qbkg, d_qtrn, d_qcf, d_qcfx;
+    // differentiable alignment (c2_logz_fwd / c2_logz_bwd)
+    std::vector<int> adj_prof;
+    std::vector<long long> adj_off;
+    long long adj_cells = 0;
+    bool adj_fwd_done = false;
+    float adj_theta[7] = {0, 0, 0, 0, 0, 0, 0};
+    float adj_wss = 0.f, adj_wcv = 0.f;
+    DevBuf<int> d_adjprof;
+    DevBuf<long long> d_adjoff;
+    DevBuf<float> d_adjbuf, d_adjlogz, d_adjgrad;
     DevBuf<unsigned char> d_qaa, d_qss;
     float scorethld = 0.f, logevthld = 0.f;
     unsigned long long searchspace = 0, deltalen = 0;
@@ -596,6 +607,31 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
             h->d_qss.ensure(Lq))
             return fail(h, C2_ERR_NOMEM, "query side arrays allocation failed");
         CK(cudaMemcpyAsync(h->d_qcf.p, qcf.data(), qcf.size() * 4, cudaMemcpyHostToDevice, h->stream));
+        // the same column -1 states with exact exp/log, for the log-partition model
+        std::vector<float> qx((size_t)Lq * 6, 0.f);
+        {
+            auto xl2 = [](double a, double b) { const double m = std::max(a, b); return std::log(std::exp(a - m) + std::exp(b - m)) + m; };
+            double pMI = 0, pIM = 0, pDN = 0;
+            for (int r = 0; r < Lq; r++) {
+                float t[7];
+                trn_of(q, 0, r, t);
+                const double L0 = -99.0;
+                double uMI = L0, uDN = L0;
+                if (r % 32 != 0) { uMI = pMI; uDN = pDN; }
+                const double mi = xl2((0.0 + t[TMM]) + L0, (uMI + t[TMM]) + L0);
+                const double im = (r % 32 == 0) ? xl2((0.0 + t[TMI]) + L0, (L0 + t[TII]) + L0)
+                                                : xl2((0.0 + t[TMI]) + L0, ((((0.0 + t[TMI]) + L0) + t[TII]) + L0));
+                const double dn = xl2(0.0 + t[TMD], uDN + t[TDD]);
+                float* c = qx.data() + (size_t)r * 6;
+                c[0] = (float)mi; c[1] = (float)im; c[2] = (float)dn;
+                c[3] = (float)pMI; c[4] = (float)pIM; c[5] = (float)pDN;
+                pMI = mi; pIM = im; pDN = dn;
+            }
+        }
+        if (h->d_qcfx.ensure(qx.size())) return fail(h, C2_ERR_NOMEM, "query side arrays allocation failed");
+        CK(cudaMemcpyAsync(h->d_qcfx.p, qx.data(), qx.size() * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        h->adj_fwd_done = false;
         CK(cudaMemcpyAsync(h->d_qtrn.p, q->trn, (size_t)(Lq + 1) * 7 * 4, cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(h->d_qaa.p, q->aa, (size_t)Lq, cudaMemcpyHostToDevice, h->stream));
         if (q->ssstate) CK(cudaMemcpyAsync(h->d_qss.p, q->ssstate, (size_t)Lq, cudaMemcpyHostToDevice, h->stream));
@@ -699,8 +735,11 @@ extern "C" c2_status c2_run_phase1(c2_handle* h)
         a.cold = h->d_cold.p;
         a.qa = h->d_qa.p;
         a.qaa = h->d_qaaf.p;
-        int gt = h->nsm * p1t_blocks_per_sm(h->sc.cvcard);
-        if (gt < 1) return fail(h, C2_ERR_CUDA, "tensor-core phase-1 kernel does not fit on an SM");
+        cudaError_t oe = cudaSuccess;
+        int gt = h->nsm * p1t_blocks_per_sm(h->sc.cvcard, &oe);
+        if (gt < 1)
+            return fail(h, C2_ERR_CUDA, "tensor-core phase-1 kernel does not fit on an SM (%s)",
+                        cudaGetErrorString(oe));
         gt = std::min(gt, h->grid * P1_WARPS / P1T_WARPS);
         CK(launch_p1(a, h->d_qbkg.p, P1K_TENSOR, gt, h->stream));
         h->launches++;
@@ -1171,5 +1210,113 @@ extern "C" c2_status c2_run_phase1_static(c2_handle* h, float* d_best, uint32_t*
     CK(cudaMemsetAsync(base, 0, sizeof(int), h->stream));
     CK(launch_p1(a, h->d_qbkg.p, P1K_STRIP, grid, h->stream));
     h->launches++;
+    return C2_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Differentiable alignment (no counterpart in the reference): log-partition
+// of the MAP forward model and its gradients (model in c2_adj.cu).
+
+static void fill_adj(c2_handle* h, AdjArgs& a)
+{
+    memset(&a, 0, sizeof a);
+    const long long NC = h->adj_cells;
+    a.Lq = h->Lq;
+    a.npairs = (int)h->adj_prof.size();
+    a.prof = h->d_adjprof.p;
+    a.off = h->d_adjoff.p;
+    a.plen = h->d_plen.p;
+    a.poff = h->d_poff.p;
+    a.qrec = h->d_qrec.p;
+    a.drec = h->d_drec.p;
+    a.pbkg = h->d_pbkg.p;
+    a.qbkg = h->d_qbkg.p;
+    a.ssss = h->d_ssss.p;
+    a.cvvals = h->d_cvvals.p;
+    a.sc = h->sc;
+    a.qtrn = h->d_qtrn.p;
+    a.dtrn = h->d_dtrn.p;
+    a.qcfx = h->d_qcfx.p;
+    for (int k = 0; k < 7; k++) a.theta[k] = h->adj_theta[k];
+    a.wss = h->adj_wss;
+    a.wcv = h->adj_wcv;
+    a.ncells = NC;
+    float* b = h->d_adjbuf.p;
+    a.p0 = b;
+    a.pss = b + NC;
+    a.pcv = b + 2 * NC;
+    a.F = b + 3 * NC;
+    a.B = b + 8 * NC;
+    a.gS = b + 13 * NC;
+    a.post = b + 14 * NC;
+    a.logz = h->d_adjlogz.p;
+    a.grad = h->d_adjgrad.p;
+}
+
+extern "C" c2_status c2_logz_fwd(c2_handle* h, const int32_t* profiles, int32_t npairs, const float* theta, float wss,
+                                 float wcv, float* logz)
+{
+    if (!h || !profiles || npairs <= 0 || !logz) return C2_ERR_ARG;
+    if (h->nprof <= 0 || h->Lq <= 0) return fail(h, C2_ERR_STATE, "logz_fwd needs a database and a query");
+    CK(cudaSetDevice(h->device));
+    h->adj_prof.assign(profiles, profiles + npairs);
+    h->adj_off.resize(npairs);
+    long long acc = 0;
+    for (int k = 0; k < npairs; k++) {
+        if (profiles[k] < 0 || profiles[k] >= h->nprof)
+            return fail(h, C2_ERR_ARG, "logz_fwd: profile %d out of range", profiles[k]);
+        h->adj_off[k] = acc;
+        acc += (long long)h->Lq * h->h_plen[profiles[k]];
+    }
+    h->adj_cells = acc;
+    for (int k = 0; k < 7; k++) h->adj_theta[k] = theta ? theta[k] : 0.f;
+    h->adj_wss = wss;
+    h->adj_wcv = wcv;
+    if (h->d_adjprof.ensure(npairs) || h->d_adjoff.ensure(npairs) || h->d_adjbuf.ensure((size_t)acc * 15) ||
+        h->d_adjlogz.ensure(npairs) || h->d_adjgrad.ensure((size_t)npairs * 9))
+        return fail(h, C2_ERR_NOMEM, "logz_fwd: scratch for %d pairs (%lld cells) failed", npairs, acc);
+    CK(cudaMemcpyAsync(h->d_adjprof.p, profiles, (size_t)npairs * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_adjoff.p, h->adj_off.data(), (size_t)npairs * 8, cudaMemcpyHostToDevice, h->stream));
+    AdjArgs a;
+    fill_adj(h, a);
+    CK(launch_adj_fwd(a, h->stream));
+    h->launches += 2;
+    CK(cudaMemcpyAsync(logz, h->d_adjlogz.p, (size_t)npairs * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->adj_fwd_done = true;
+    return C2_OK;
+}
+
+extern "C" c2_status c2_logz_bwd(c2_handle* h, float* grad)
+{
+    if (!h || !grad) return C2_ERR_ARG;
+    if (!h->adj_fwd_done) return fail(h, C2_ERR_STATE, "logz_bwd needs a preceding logz_fwd for the current query");
+    CK(cudaSetDevice(h->device));
+    AdjArgs a;
+    fill_adj(h, a);
+    CK(launch_adj_bwd(a, h->stream));
+    h->launches += 2;
+    CK(cudaMemcpyAsync(grad, h->d_adjgrad.p, (size_t)a.npairs * 9 * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return C2_OK;
+}
+
+extern "C" c2_status c2_logz_cells(c2_handle* h, int32_t pair, float* dlogz_ds, float* post)
+{
+    if (!h || (!dlogz_ds && !post)) return C2_ERR_ARG;
+    if (!h->adj_fwd_done || pair < 0 || pair >= (int)h->adj_prof.size())
+        return fail(h, C2_ERR_STATE, "logz_cells: no such pair after logz_fwd/logz_bwd");
+    CK(cudaSetDevice(h->device));
+    const int Lq = h->Lq, L = h->h_plen[h->adj_prof[pair]];
+    const size_t n = (size_t)Lq * L;
+    std::vector<float> t(n);
+    const long long NC = h->adj_cells;
+    for (int w = 0; w < 2; w++) {
+        float* dst = w ? post : dlogz_ds;
+        if (!dst) continue;
+        CK(cudaMemcpy(t.data(), h->d_adjbuf.p + (13 + w) * NC + h->adj_off[pair], n * 4, cudaMemcpyDeviceToHost));
+        for (int j = 0; j < L; j++)
+            for (int i = 0; i < Lq; i++) dst[(size_t)i * L + j] = t[(size_t)j * Lq + i];   // row-major [Lq][L]
+    }
     return C2_OK;
 }

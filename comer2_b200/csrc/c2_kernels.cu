@@ -1351,12 +1351,13 @@ size_t p1t_smem_bytes(int cvcard)
     return (size_t)(cvcard * P1T_CVREP + P1T_WARPS * P1T_WARP_FLOATS) * sizeof(float);
 }
 
-int p1t_blocks_per_sm(int cvcard)
+int p1t_blocks_per_sm(int cvcard, cudaError_t* err)
 {
     int n = 0;
     const size_t sm = p1t_smem_bytes(cvcard);
-    cudaFuncSetAttribute(p1t_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, p1t_kernel, P1T_WARPS * 32, sm);
+    cudaError_t e = cudaFuncSetAttribute(p1t_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, p1t_kernel, P1T_WARPS * 32, sm);
+    if (err) *err = e;
     return n;
 }
 

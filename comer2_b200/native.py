@@ -26,7 +26,7 @@ EXPORTS = [
     "c2_create", "c2_destroy", "c2_last_error", "c2_upload_db", "c2_set_query", "c2_run_phase1",
     "c2_get_phase1", "c2_run_finalize", "c2_get_finalize", "c2_get_thresholds", "c2_set_stream", "c2_sync",
     "c2_launch_count", "c2_run_stats", "c2_run_map", "c2_get_hits", "c2_search", "c2_get_search_space",
-    "c2_run_phase1_static", "c2_set_score_mode",
+    "c2_run_phase1_static", "c2_set_score_mode", "c2_logz_fwd", "c2_logz_bwd", "c2_logz_cells",
 ]
 
 SCORE_FP32 = 0
@@ -109,6 +109,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.c2_get_search_space.argtypes = [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]
     lib.c2_run_phase1_static.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     lib.c2_set_score_mode.argtypes = [C.c_void_p, C.c_int32]
+    lib.c2_logz_fwd.argtypes = [C.c_void_p, _i32p, C.c_int32, _fp, C.c_float, C.c_float, _fp]
+    lib.c2_logz_bwd.argtypes = [C.c_void_p, _fp]
+    lib.c2_logz_cells.argtypes = [C.c_void_p, C.c_int32, _fp, _fp]
     for n in EXPORTS:
         getattr(lib, n).restype = C.c_int
     _lib = lib
@@ -227,6 +230,7 @@ class Handle:
         k = _Keep()
         s = make_profiles(q, k)
         self._ck(self.lib.c2_set_query(self._h, C.byref(s)), "c2_set_query")
+        self.Lq = int(q.lengths[0])
 
     def thresholds(self):
         a, b = C.c_float(), C.c_float()
@@ -242,6 +246,29 @@ class Handle:
 
     def sync(self):
         self._ck(self.lib.c2_sync(self._h), "c2_sync")
+
+    def logz_fwd(self, profiles, theta=None, wss: float = 0.0, wcv: float = 0.0) -> np.ndarray:
+        """Log-partition of the MAP forward model for the current query vs db profiles (c2_logz_fwd)."""
+        pr = np.ascontiguousarray(profiles, np.int32)
+        th = np.zeros(7, np.float32) if theta is None else np.ascontiguousarray(theta, np.float32)
+        out = np.zeros(pr.shape[0], np.float32)
+        self._ck(self.lib.c2_logz_fwd(self._h, _ptr(pr, C.c_int32), int(pr.shape[0]), _ptr(th, C.c_float),
+                                      float(wss), float(wcv), _ptr(out, C.c_float)), "c2_logz_fwd")
+        self._adj_n = int(pr.shape[0])
+        return out
+
+    def logz_bwd(self) -> np.ndarray:
+        """[npairs, 9]: dlogZ/dtheta (7), dlogZ/dwss, dlogZ/dwcv of the last logz_fwd."""
+        g = np.zeros((self._adj_n, 9), np.float32)
+        self._ck(self.lib.c2_logz_bwd(self._h, _ptr(g, C.c_float)), "c2_logz_bwd")
+        return g
+
+    def logz_cells(self, k: int, L: int):
+        """(dlogZ/dS, MM posterior) of pair k, each [Lq][L] (L: the pair's db profile length)."""
+        ds = np.zeros((self.Lq, L), np.float32)
+        po = np.zeros((self.Lq, L), np.float32)
+        self._ck(self.lib.c2_logz_cells(self._h, int(k), _ptr(ds, C.c_float), _ptr(po, C.c_float)), "c2_logz_cells")
+        return ds, po
 
     def set_score_mode(self, mode: int):
         """SCORE_FP32 (CUDA cores) or SCORE_BF16_TC (split-BF16 tensor-core contractions)."""

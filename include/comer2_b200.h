@@ -219,6 +219,28 @@ c2_status c2_launch_count(const c2_handle* h, uint64_t* n);
 #define C2_SCORE_BF16_TC 1
 c2_status c2_set_score_mode(c2_handle* h, int32_t mode);
 
+/* Differentiable alignment (no counterpart in the reference, whose
+ * forward-backward only feeds its MAP alignment).  Log-partition of the MAP
+ * forward model -- the recursion of src/libmycu/cumapdp/CuBatchMAPDP_fwd.cu
+ * with exact exp/log -- for the current query against db profiles
+ * `profiles[0..npairs)`, over the score matrix S = s0 + wss*ss + wcv*cv
+ * (amino-acid score; SS and context-vector terms before their weights) and
+ * with theta[7] (MM MI MD IM II DM DD, may be NULL = 0) added to the query's
+ * transition log-probabilities in every cell update.  logz[k] receives
+ * log sum over cells exp(F.MM) of pair k.  Keeps the forward states for
+ * c2_logz_bwd; a new query or c2_logz_fwd call replaces them. */
+c2_status c2_logz_fwd(c2_handle* h, const int32_t* profiles, int32_t npairs, const float* theta, float wss,
+                      float wcv, float* logz);
+
+/* Gradients of the last c2_logz_fwd: grad[9 * k + t] = dlogZ_k/dtheta_t
+ * (t < 7), grad[9 * k + 7] = dlogZ_k/dwss, grad[9 * k + 8] = dlogZ_k/dwcv. */
+c2_status c2_logz_bwd(c2_handle* h, float* grad);
+
+/* Per-cell results of pair k after c2_logz_bwd, row-major [Lq][L]:
+ * dlogz_ds = dlogZ/dS (expected MM emissions), post = MM state posterior
+ * exp(F.MM + B.MM - logZ).  Either pointer may be NULL. */
+c2_status c2_logz_cells(c2_handle* h, int32_t pair, float* dlogz_ds, float* post);
+
 /* Phase 1 (as c2_run_phase1) that allocates nothing.  No counterpart in the
  * reference.  Its scratch (work counter, strip-boundary rows) lives in one
  * static 16 MiB device array per device, so the grid is limited to the 8-warp

@@ -1,0 +1,115 @@
+"""Differentiable alignment on the GPU (c2_logz_fwd / c2_logz_bwd) against
+the FP64 oracle: log-partition values, gradients against central finite
+differences of the oracle's log-partition (step 1e-4), per-cell gradients,
+the MM state posteriors against the oracle's MAP posteriors (exact exp/log,
+no log-E-value score adjustment), and the torch.autograd wrapper.
+
+Tolerances: logZ 2e-4 relative; gradients 2e-3 relative to max(1, |g|)
+(FP32 sweeps against FP64 differences); posteriors 2e-4 absolute.
+"""
+import numpy as np
+import pytest
+
+from comer2_b200 import synth as S
+
+pytestmark = pytest.mark.gpu
+
+THETA = np.array([0.05, -0.1, 0.02, 0.0, 0.1, -0.05, 0.03])
+
+
+def _setup(params, seed=7, lq=70, lens=(33, 64, 90, 41)):
+    from comer2_b200.native import Handle
+    rng = np.random.default_rng(seed)
+    q = S.random_profiles(rng, [lq])
+    parts = [S.planted_homolog(rng, q, L, seg_lo=20, seg_hi=40) for L in lens]
+    db = S.concat(parts)
+    h = Handle(params, 0)
+    h.upload_db(db)
+    h.set_query(q)
+    return h, q, db
+
+
+def _corners(lq, ld):
+    """Cells of the two far corner triangles (the DP and MAP stages' corner masking)."""
+    e = min(60, int(np.rint(0.34 * max(lq, ld))))
+    y, x = np.mgrid[0:lq, 0:ld]
+    return ((lq <= y + e) & (x <= e + y - lq)) | ((ld - e + y <= x) & (y < e))
+
+
+def _oracle_S(orc, qo, do, wss, wcv):
+    s0, ss, cv = orc.score_parts(qo, do)
+    return s0 + wss * ss + wcv * cv, ss, cv
+
+
+def test_logz_and_gradients(params, orc64):
+    h, q, db = _setup(params)
+    ks = list(range(db.nprofiles))
+    wss, wcv = params.ssswgt, params.cvswgt
+    z = h.logz_fwd(ks, THETA, wss, wcv)
+    g = h.logz_bwd()
+    qo = orc64.profile(q)
+    hstep = 1e-4
+    for k in ks:
+        do = orc64.profile(db, k)
+        Sk, ss, cv = _oracle_S(orc64, qo, do, wss, wcv)
+        zr = orc64.logz(qo, do, Sk, THETA)
+        assert z[k] == pytest.approx(zr, rel=2e-4), k
+        for t in range(7):
+            tp = THETA.copy(); tp[t] += hstep
+            tm = THETA.copy(); tm[t] -= hstep
+            fd = (orc64.logz(qo, do, Sk, tp) - orc64.logz(qo, do, Sk, tm)) / (2 * hstep)
+            assert abs(g[k, t] - fd) <= 2e-3 * max(1.0, abs(fd)), (k, t, g[k, t], fd)
+        fss = (orc64.logz(qo, do, Sk + hstep * ss, THETA) - orc64.logz(qo, do, Sk - hstep * ss, THETA)) / (2 * hstep)
+        fcv = (orc64.logz(qo, do, Sk + hstep * cv, THETA) - orc64.logz(qo, do, Sk - hstep * cv, THETA)) / (2 * hstep)
+        assert abs(g[k, 7] - fss) <= 2e-3 * max(1.0, abs(fss)), (k, g[k, 7], fss)
+        assert abs(g[k, 8] - fcv) <= 2e-3 * max(1.0, abs(fcv)), (k, g[k, 8], fcv)
+    h.close()
+
+
+def test_cell_gradients_and_posteriors(params, orc64):
+    h, q, db = _setup(params, seed=8, lq=45, lens=(38, 52))
+    wss, wcv = params.ssswgt, params.cvswgt
+    h.logz_fwd([0, 1], None, wss, wcv)
+    h.logz_bwd()
+    qo = orc64.profile(q)
+    rng = np.random.default_rng(3)
+    for k in (0, 1):
+        L = int(db.lengths[k])
+        ds, post = h.logz_cells(k, L)
+        do = orc64.profile(db, k)
+        Sk, _, _ = _oracle_S(orc64, qo, do, wss, wcv)
+        # dlogZ/dS at sampled cells by central differences
+        hstep = 1e-4
+        for _ in range(12):
+            i, j = int(rng.integers(0, q.lengths[0])), int(rng.integers(0, L))
+            Sp = Sk.copy(); Sp[i, j] += hstep
+            Sm = Sk.copy(); Sm[i, j] -= hstep
+            fd = (orc64.logz(qo, do, Sp) - orc64.logz(qo, do, Sm)) / (2 * hstep)
+            assert abs(ds[i, j] - fd) <= 2e-4 + 2e-3 * abs(fd), (k, i, j, ds[i, j], fd)
+        # the MM posterior is the MAP stage's posterior of the same model
+        m = orc64.map(qo, do, Sk, np.zeros_like(Sk), -500.0, exact=True, with_post=True)
+        keep = ~_corners(int(q.lengths[0]), L)   # the MAP stage masks the two far corners
+        assert np.abs(post - m["post"])[keep].max() <= 2e-4
+        # expected emissions never exceed the posterior mass of the cell
+        assert (ds <= post + 1e-5).all() and (ds >= -1e-6).all()
+    h.close()
+
+
+def test_torch_autograd_wrapper(params):
+    import torch
+    from comer2_b200.adjoint import logz
+    h, q, db = _setup(params, seed=9)
+    ks = list(range(db.nprofiles))
+    theta = torch.tensor(THETA, dtype=torch.float32, requires_grad=True)
+    wss = torch.tensor(float(params.ssswgt), requires_grad=True)
+    wcv = torch.tensor(float(params.cvswgt), requires_grad=True)
+    z = logz(h, ks, theta, wss, wcv)
+    weights = torch.arange(1, len(ks) + 1, dtype=torch.float32)
+    (weights * z).sum().backward()
+    h.logz_fwd(ks, THETA, float(params.ssswgt), float(params.cvswgt))
+    g = h.logz_bwd()
+    want = (weights.numpy()[:, None] * g).sum(0)
+    assert np.allclose(theta.grad.numpy(), want[:7], rtol=1e-5, atol=1e-5)
+    assert wss.grad.item() == pytest.approx(want[7], rel=1e-5, abs=1e-5)
+    assert wcv.grad.item() == pytest.approx(want[8], rel=1e-5, abs=1e-5)
+    h.close()

@@ -147,3 +147,18 @@ def test_length_adjustment(orc32, params):
     ss, dl = orc32.length_adjustment(params.gapped_lambda, params.gapped_K, params.gapped_alpha,
                                      params.gapped_beta, 400, 22_000_000, 100_000)
     assert (ss, dl) == (400 * 22_000_000, 0)
+
+
+def test_logz_model_is_the_map_forward(params, orc64):
+    """The log-partition of the differentiable-alignment model at theta = 0 is
+    the MAP stage's total probability (exact exp/log, unadjusted scores)."""
+    rng = np.random.default_rng(21)
+    q = S.random_profiles(rng, [45])
+    d = S.random_profiles(rng, [38])
+    qo, do = orc64.profile(q), orc64.profile(d)
+    s0, ss, cv = orc64.score_parts(qo, do)
+    Sk = s0 + params.ssswgt * ss + params.cvswgt * cv
+    full, _ = orc64.score_matrix(qo, do)
+    assert np.allclose(Sk, full, atol=1e-6)
+    m = orc64.map(qo, do, Sk, np.zeros_like(Sk), -500.0, exact=True)
+    assert orc64.logz(qo, do, Sk) == pytest.approx(m["logZ"], rel=1e-12)
