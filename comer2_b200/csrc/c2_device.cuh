@@ -84,12 +84,10 @@ constexpr int P1C_WARP_FLOATS =
 // tensor-core kernel: score ring of 64 columns with 36 floats per column (the
 // fragment-layout writes and the per-lane wavefront reads are both free of
 // bank conflicts), a column-record ring of 4 chunks, the row above the strip
-// and the pair-scaled amino-acid A fragments of the strip ([mt][kt][split][lane][4])
 // and two slots for db operand tiles (bulk async copies, one mbarrier each)
-constexpr int P1T_WARPS = 8;
+constexpr int P1T_WARPS = 10;
 constexpr int P1T_RLD = 36, P1T_CRING = 128, P1T_CVREP = 8;
-constexpr int P1T_WARP_FLOATS =
-    P1C_RING * P1T_RLD + P1T_CRING * P1C_TRS + 32 * 8 + 2 * 2 * 2 * 32 * 4 + 2 * TC_TILE_WORDS + 4;
+constexpr int P1T_WARP_FLOATS = P1C_RING * P1T_RLD + P1T_CRING * P1C_TRS + 32 * 8 + 2 * TC_TILE_WORDS + 4;
 
 struct P1Args {
     const float* qrec;      // [Lq][QR_STRIDE]

@@ -1003,8 +1003,7 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
     float* ring = wb;                                         // [P1C_RING][P1T_RLD] scores
     float* cring = ring + P1C_RING * P1T_RLD;                 // [P1T_CRING][P1C_TRS] column records
     float* bnd = cring + P1T_CRING * P1C_TRS;                 // [32][8] row above the strip
-    uint4* aas = reinterpret_cast<uint4*>(bnd + 32 * 8);      // [mt][kt][split][lane] amino-acid A fragments
-    unsigned* btile = reinterpret_cast<unsigned*>(aas + 2 * 2 * 2 * 32);   // [2][TC_TILE_WORDS] db operand tiles
+    unsigned* btile = reinterpret_cast<unsigned*>(bnd + 32 * 8);   // [2][TC_TILE_WORDS] db operand tiles
     unsigned long long* tbar = reinterpret_cast<unsigned long long*>(btile + 2 * TC_TILE_WORDS);  // [2]
     for (int i = threadIdx.x; i < cvcard * P1T_CVREP; i += blockDim.x) cvtab[i] = a.cvvals[i / P1T_CVREP];
     if (lane == 0) {
@@ -1045,8 +1044,8 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
             const bool act = r < Lq;
             const float* __restrict__ qr = a.qrec + (long long)(act ? r : Lq - 1) * QR_STRIDE;
             // amino-acid A fragments of this strip, scaled for the pair and split
-            // into shared memory (q(a) / (0.5 (bq(a) + bd(a))), as cell_score's Qt)
-            __syncwarp();
+            // (q(a) / (0.5 (bq(a) + bd(a))), as cell_score's Qt), kept in registers
+            unsigned Aaa[2][2][2][4];   // [mtile][ktile][split][reg]
 #pragma unroll
             for (int kt = 0; kt < 2; kt++) {
                 float wk[4];
@@ -1068,10 +1067,11 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                         const float x = __fdividef(v[e], wk[(e & 1) + ((e >> 2) << 1)]);
                         bf16_split(x, h[e], l[e]);
                     }
-                    aas[((mt * 2 + kt) * 2 + 0) * 32 + lane] =
-                        make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16), h[6] | (h[7] << 16));
-                    aas[((mt * 2 + kt) * 2 + 1) * 32 + lane] =
-                        make_uint4(l[0] | (l[1] << 16), l[2] | (l[3] << 16), l[4] | (l[5] << 16), l[6] | (l[7] << 16));
+#pragma unroll
+                    for (int w = 0; w < 4; w++) {
+                        Aaa[mt][kt][0][w] = h[2 * w] | (h[2 * w + 1] << 16);
+                        Aaa[mt][kt][1][w] = l[2 * w] | (l[2 * w + 1] << 16);
+                    }
                 }
             }
             // query row terms of this lane's fragment rows: 32 s + 16 mt + g + 8 h
@@ -1174,13 +1174,9 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                                 for (int i = 0; i < 4; i++) acc[d][i] = 0.f;
 #pragma unroll
                             for (int kt = 0; kt < 2; kt++) {
-                                const uint4 ah = aas[((mt * 2 + kt) * 2 + 0) * 32 + lane];
-                                const uint4 al = aas[((mt * 2 + kt) * 2 + 1) * 32 + lane];
-                                const unsigned Ah[4] = {ah.x, ah.y, ah.z, ah.w};
-                                const unsigned Al[4] = {al.x, al.y, al.z, al.w};
-                                mma_bf16(acc[0], Al, B[0][kt][0].x, B[0][kt][0].y);
-                                mma_bf16(acc[0], Ah, B[0][kt][1].x, B[0][kt][1].y);
-                                mma_bf16(acc[0], Ah, B[0][kt][0].x, B[0][kt][0].y);
+                                mma_bf16(acc[0], Aaa[mt][kt][1], B[0][kt][0].x, B[0][kt][0].y);
+                                mma_bf16(acc[0], Aaa[mt][kt][0], B[0][kt][1].x, B[0][kt][1].y);
+                                mma_bf16(acc[0], Aaa[mt][kt][0], B[0][kt][0].x, B[0][kt][0].y);
                             }
 #pragma unroll
                             for (int d = 1; d < 3; d++)

@@ -252,22 +252,22 @@ class Handle:
         pr = np.ascontiguousarray(profiles, np.int32)
         th = np.zeros(7, np.float32) if theta is None else np.ascontiguousarray(theta, np.float32)
         out = np.zeros(pr.shape[0], np.float32)
-        self._ck(self.lib.c2_logz_fwd(self._h, _ptr(pr, C.c_int32), int(pr.shape[0]), _ptr(th, C.c_float),
-                                      float(wss), float(wcv), _ptr(out, C.c_float)), "c2_logz_fwd")
+        self._ck(self.lib.c2_logz_fwd(self._h, _ptr(pr, _i32p), int(pr.shape[0]), _ptr(th, _fp),
+                                      float(wss), float(wcv), _ptr(out, _fp)), "c2_logz_fwd")
         self._adj_n = int(pr.shape[0])
         return out
 
     def logz_bwd(self) -> np.ndarray:
         """[npairs, 9]: dlogZ/dtheta (7), dlogZ/dwss, dlogZ/dwcv of the last logz_fwd."""
         g = np.zeros((self._adj_n, 9), np.float32)
-        self._ck(self.lib.c2_logz_bwd(self._h, _ptr(g, C.c_float)), "c2_logz_bwd")
+        self._ck(self.lib.c2_logz_bwd(self._h, _ptr(g, _fp)), "c2_logz_bwd")
         return g
 
     def logz_cells(self, k: int, L: int):
         """(dlogZ/dS, MM posterior) of pair k, each [Lq][L] (L: the pair's db profile length)."""
         ds = np.zeros((self.Lq, L), np.float32)
         po = np.zeros((self.Lq, L), np.float32)
-        self._ck(self.lib.c2_logz_cells(self._h, int(k), _ptr(ds, C.c_float), _ptr(po, C.c_float)), "c2_logz_cells")
+        self._ck(self.lib.c2_logz_cells(self._h, int(k), _ptr(ds, _fp), _ptr(po, _fp)), "c2_logz_cells")
         return ds, po
 
     def set_score_mode(self, mode: int):
