@@ -87,6 +87,27 @@ def test_search_matches_oracle(params, orc32, seed, mode):
     h.close()
 
 
+@pytest.mark.parametrize("mode", [0, 1])
+def test_long_query_matches_oracle(params, orc32, mode):
+    """A 3,000-position query of six domains (94 strips) against 30 profiles
+    with planted single-domain homologs: the same hits, E-values and
+    alignments as the oracle."""
+    w = S.config(4, seed=5, scale=0.0006)
+    h, hits, thld, logevthld, ss = _run(params, w, mode)
+    ref = _oracle_search(orc32, params, w, ss, thld, logevthld)
+    ref_hits = sorted(k for k, v in ref.items() if "map" in v)
+    assert sorted(int(x["profile"]) for x in hits) == ref_hits
+    for x in hits:
+        r = ref[int(x["profile"])]
+        if abs(x["score"] - r["score"]) > 1e-4 * max(1.0, abs(r["score"])):
+            continue
+        assert x["logE"] == pytest.approx(r["stats"]["logE"], abs=1e-3)
+        assert x["strings"][:3] == r["map"]["strings"][:3]
+    for k in w.homologs:
+        assert k in [int(x["profile"]) for x in hits]
+    h.close()
+
+
 def test_search_space_matches_oracle(params, orc32):
     w = S.config(0, seed=4, scale=0.05)
     from comer2_b200.native import Handle
