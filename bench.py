@@ -312,8 +312,9 @@ def main():
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                      "peak_kind": peak_kind,
                      "traffic": (tpp * npos) if tpp else None,
-                     "note": "algorithmic bytes = 209 B x db positions per query pass; the FP32 kernel is "
-                             "issue/latency bound, not HBM bound"},
+                     "note": "algorithmic bytes = 209 B x db positions per query pass; traffic = DRAM bytes per "
+                             "position from the 20k-profile ncu capture (profiles/p1t_kernel_20k.md) x positions; "
+                             "the kernel is issue/latency bound, not HBM bound"},
         "clocks": clocks,
         "db_upload_s": upload_s,
     }
