@@ -1,0 +1,169 @@
+// c2_dbio.cpp -- reader of the reference's binary profile database (the
+// `db2bin` output, format v2.2) into the c2_profiles field set.
+//
+// File layout (written by Db::WriteBinaryHeader, src/libpro/srcpro/Db.cpp:733-741,
+// CalculateAndWriteAddressTable_v2_2 and BinaryWriteProfile_v2_2,
+// src/libpro/srcpro/PMProfileModel.cpp:1468-1930):
+//   "COMER profile bin database v" "2.2"        (no terminator)
+//   size_t nprofiles, uint64 npositions
+//   size_t address[79]                          (file offset of every section)
+//   int lengths[P]; float eno[P]; float bkg[20][P]
+//   float trn[7][P + N]   (MM MI MD IM II DM DD; per profile the beginning
+//                          state, then one value per position; natural logs,
+//                          x 0.4 for IM II DM DD, -32768 for probability 0)
+//   float trg[20][N]; float cv[19][N]; float cvprior[N]; float cvnorm2[N]
+//   float ss[3][N]; float hdp1prob[N]; int hdp1index[N]
+//   char aa[N]; char ssstate[N] (lower case, ' ' without SS; read as upper case)
+//   size_t desc_end[P]; descriptions (NUL terminated)
+// The sections are field-major; c2_profiles is position-major.
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/comer2_b200.h"
+
+namespace {
+
+constexpr const char* kSig = "COMER profile bin database v";
+constexpr const char* kVer = "2.2";
+constexpr int kNAA = 20, kNCV = 19, kNSS = 3, kNTRN = 7;
+constexpr int kNSECTIONS = 1 + 1 + kNAA + kNTRN + kNAA + kNCV + 1 + 1 + kNSS + 1 + 1 + 1 + 1 + 1 + 1;
+
+struct File {
+    FILE* f = nullptr;
+    ~File() { if (f) fclose(f); }
+};
+
+void set_err(char* err, size_t n, const std::string& m)
+{
+    if (err && n) {
+        std::strncpy(err, m.c_str(), n - 1);
+        err[n - 1] = 0;
+    }
+}
+
+bool read_at(FILE* f, uint64_t off, void* dst, size_t bytes)
+{
+    if (fseeko(f, (off_t)off, SEEK_SET) != 0) return false;
+    return fread(dst, 1, bytes, f) == bytes;
+}
+
+struct Header {
+    uint64_t nprof = 0, npos = 0;
+    uint64_t addr[kNSECTIONS] = {};
+};
+
+c2_status read_header(FILE* f, Header& h, char* err, size_t errlen)
+{
+    const size_t ls = std::strlen(kSig), lv = std::strlen(kVer);
+    std::vector<char> sig(ls + lv);
+    if (fread(sig.data(), 1, sig.size(), f) != sig.size() || std::memcmp(sig.data(), kSig, ls) != 0) {
+        set_err(err, errlen, "not a COMER binary profile database");
+        return C2_ERR_ARG;
+    }
+    if (std::memcmp(sig.data() + ls, kVer, lv) != 0) {
+        set_err(err, errlen, "unsupported binary database version (2.2 expected)");
+        return C2_ERR_ARG;
+    }
+    uint64_t np = 0, nn = 0;
+    if (fread(&np, sizeof np, 1, f) != 1 || fread(&nn, sizeof nn, 1, f) != 1 ||
+        fread(h.addr, sizeof(uint64_t), kNSECTIONS, f) != (size_t)kNSECTIONS) {
+        set_err(err, errlen, "truncated binary database header");
+        return C2_ERR_ARG;
+    }
+    if (np == 0 || np > 0x7fffffffULL) {
+        set_err(err, errlen, "invalid number of profiles in the binary database");
+        return C2_ERR_ARG;
+    }
+    h.nprof = np;
+    h.npos = nn;
+    return C2_OK;
+}
+
+}  // namespace
+
+extern "C" c2_status c2_db2bin_info(const char* path, int32_t* nprofiles, int64_t* npositions, char* err,
+                                    size_t errlen)
+{
+    if (!path || !nprofiles || !npositions) return C2_ERR_ARG;
+    File F;
+    F.f = fopen(path, "rb");
+    if (!F.f) {
+        set_err(err, errlen, std::string("cannot open ") + path);
+        return C2_ERR_ARG;
+    }
+    Header h;
+    c2_status st = read_header(F.f, h, err, errlen);
+    if (st != C2_OK) return st;
+    *nprofiles = (int32_t)h.nprof;
+    *npositions = (int64_t)h.npos;
+    return C2_OK;
+}
+
+extern "C" c2_status c2_db2bin_read(const char* path, int32_t* lengths, int64_t* offsets, float* bkg, float* eno,
+                                    float* trn, float* trg, float* cv, float* cvprior, float* cvnorm2, float* ss,
+                                    uint8_t* ssstate, uint8_t* aa, char* err, size_t errlen)
+{
+    if (!path || !lengths || !offsets || !bkg || !eno || !trn || !trg || !cv || !cvprior || !cvnorm2 || !ss ||
+        !ssstate || !aa)
+        return C2_ERR_ARG;
+    File F;
+    F.f = fopen(path, "rb");
+    if (!F.f) {
+        set_err(err, errlen, std::string("cannot open ") + path);
+        return C2_ERR_ARG;
+    }
+    Header h;
+    c2_status st = read_header(F.f, h, err, errlen);
+    if (st != C2_OK) return st;
+    const uint64_t P = h.nprof, N = h.npos;
+    FILE* f = F.f;
+    int a = 0;
+    auto fail = [&](const char* what) {
+        set_err(err, errlen, std::string("truncated or inconsistent binary database: ") + what);
+        return C2_ERR_ARG;
+    };
+    // lengths, ENOs, backgrounds
+    if (!read_at(f, h.addr[a++], lengths, P * sizeof(int32_t))) return fail("lengths");
+    uint64_t acc = 0;
+    for (uint64_t k = 0; k < P; k++) {
+        if (lengths[k] < 1) return fail("profile length");
+        offsets[k] = (int64_t)acc;
+        acc += (uint64_t)lengths[k];
+    }
+    if (acc != N) return fail("sum of profile lengths");
+    if (!read_at(f, h.addr[a++], eno, P * sizeof(float))) return fail("ENOs");
+    std::vector<float> col(std::max<uint64_t>(N + P, P));
+    for (int r = 0; r < kNAA; r++) {
+        if (!read_at(f, h.addr[a++], col.data(), P * sizeof(float))) return fail("backgrounds");
+        for (uint64_t k = 0; k < P; k++) bkg[k * kNAA + r] = col[k];
+    }
+    for (int t = 0; t < kNTRN; t++) {
+        if (!read_at(f, h.addr[a++], col.data(), (N + P) * sizeof(float))) return fail("transitions");
+        for (uint64_t i = 0; i < N + P; i++) trn[i * kNTRN + t] = col[i];
+    }
+    for (int r = 0; r < kNAA; r++) {
+        if (!read_at(f, h.addr[a++], col.data(), N * sizeof(float))) return fail("target probabilities");
+        for (uint64_t i = 0; i < N; i++) trg[i * kNAA + r] = col[i];
+    }
+    for (int r = 0; r < kNCV; r++) {
+        if (!read_at(f, h.addr[a++], col.data(), N * sizeof(float))) return fail("context vectors");
+        for (uint64_t i = 0; i < N; i++) cv[i * kNCV + r] = col[i];
+    }
+    if (!read_at(f, h.addr[a++], cvprior, N * sizeof(float))) return fail("context vector priors");
+    if (!read_at(f, h.addr[a++], cvnorm2, N * sizeof(float))) return fail("context vector norms");
+    for (int r = 0; r < kNSS; r++) {
+        if (!read_at(f, h.addr[a++], col.data(), N * sizeof(float))) return fail("SS probabilities");
+        for (uint64_t i = 0; i < N; i++) ss[i * kNSS + r] = col[i];
+    }
+    a += 2;   // HDP1 cluster probabilities and indices: not used by this search path
+    if (!read_at(f, h.addr[a++], aa, N)) return fail("residues");
+    if (!read_at(f, h.addr[a++], ssstate, N)) return fail("SS states");
+    for (uint64_t i = 0; i < N; i++) {
+        const uint8_t c = ssstate[i];
+        ssstate[i] = (c >= 'a' && c <= 'z') ? (uint8_t)(c - 'a' + 'A') : c;   // ' ': no SS prediction
+    }
+    return C2_OK;
+}

@@ -27,6 +27,7 @@ EXPORTS = [
     "c2_get_phase1", "c2_run_finalize", "c2_get_finalize", "c2_get_thresholds", "c2_set_stream", "c2_sync",
     "c2_launch_count", "c2_run_stats", "c2_run_map", "c2_get_hits", "c2_search", "c2_get_search_space",
     "c2_run_phase1_static", "c2_set_score_mode", "c2_logz_fwd", "c2_logz_bwd", "c2_logz_cells",
+    "c2_db2bin_info", "c2_db2bin_read",
 ]
 
 SCORE_FP32 = 0
@@ -112,6 +113,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.c2_logz_fwd.argtypes = [C.c_void_p, _i32p, C.c_int32, _fp, C.c_float, C.c_float, _fp]
     lib.c2_logz_bwd.argtypes = [C.c_void_p, _fp]
     lib.c2_logz_cells.argtypes = [C.c_void_p, C.c_int32, _fp, _fp]
+    lib.c2_db2bin_info.argtypes = [C.c_char_p, _i32p, _i64p, C.c_char_p, C.c_size_t]
+    lib.c2_db2bin_read.argtypes = [C.c_char_p, _i32p, _i64p, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _u8p, _u8p,
+                                   C.c_char_p, C.c_size_t]
     for n in EXPORTS:
         getattr(lib, n).restype = C.c_int
     _lib = lib
@@ -337,3 +341,35 @@ class Handle:
         n = C.c_uint64()
         self._ck(self.lib.c2_launch_count(self._h, C.byref(n)), "c2_launch_count")
         return n.value
+
+
+def read_db2bin(path: str):
+    """Read a database written by the reference's db2bin (format v2.2) into a
+    synth.ProfileSet (c2_db2bin_info / c2_db2bin_read; no GPU needed)."""
+    from .synth import ProfileSet
+    lib = load()
+    P, N = C.c_int32(), C.c_int64()
+    err = C.create_string_buffer(512)
+    st = lib.c2_db2bin_info(path.encode(), C.byref(P), C.byref(N), err, 512)
+    if st != C2_OK:
+        raise C2Error("c2_db2bin_info: %s" % err.value.decode())
+    P, N = P.value, N.value
+    lengths = np.zeros(P, np.int32)
+    offsets = np.zeros(P, np.int64)
+    bkg = np.zeros((P, 20), np.float32)
+    eno = np.zeros(P, np.float32)
+    trn = np.zeros((N + P, 7), np.float32)
+    trg = np.zeros((N, 20), np.float32)
+    cv = np.zeros((N, 19), np.float32)
+    cvp = np.zeros(N, np.float32)
+    cvn = np.zeros(N, np.float32)
+    ss = np.zeros((N, 3), np.float32)
+    sss = np.zeros(N, np.uint8)
+    aa = np.zeros(N, np.uint8)
+    st = lib.c2_db2bin_read(path.encode(), _ptr(lengths, _i32p), _ptr(offsets, _i64p), _ptr(bkg, _fp), _ptr(eno, _fp),
+                            _ptr(trn, _fp), _ptr(trg, _fp), _ptr(cv, _fp), _ptr(cvp, _fp), _ptr(cvn, _fp),
+                            _ptr(ss, _fp), _ptr(sss, _u8p), _ptr(aa, _u8p), err, 512)
+    if st != C2_OK:
+        raise C2Error("c2_db2bin_read: %s" % err.value.decode())
+    return ProfileSet(lengths, offsets, bkg, eno, trn, trg, cv, cvp, cvn, ss, sss, aa,
+                      np.zeros((N + P, 7), np.int32), np.zeros((N, 20), np.int32))

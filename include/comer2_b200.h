@@ -219,6 +219,18 @@ c2_status c2_launch_count(const c2_handle* h, uint64_t* n);
 #define C2_SCORE_BF16_TC 1
 c2_status c2_set_score_mode(c2_handle* h, int32_t mode);
 
+/* Reader of the reference's binary profile database (`db2bin` output,
+ * format v2.2: Db::WriteBinaryHeader, src/libpro/srcpro/Db.cpp:733-741;
+ * BinaryWriteProfile_v2_2, src/libpro/srcpro/PMProfileModel.cpp:1468-1930),
+ * the input the reference's reader threads stream (TdDataReader,
+ * CuDbReader).  c2_db2bin_info gives the sizes; c2_db2bin_read fills
+ * caller-owned arrays with the c2_profiles field set (position-major; SS
+ * states upper case).  err (may be NULL) receives a message on failure. */
+c2_status c2_db2bin_info(const char* path, int32_t* nprofiles, int64_t* npositions, char* err, size_t errlen);
+c2_status c2_db2bin_read(const char* path, int32_t* lengths, int64_t* offsets, float* bkg, float* eno, float* trn,
+                         float* trg, float* cv, float* cvprior, float* cvnorm2, float* ss, uint8_t* ssstate,
+                         uint8_t* aa, char* err, size_t errlen);
+
 /* Differentiable alignment (no counterpart in the reference, whose
  * forward-backward only feeds its MAP alignment).  Log-partition of the MAP
  * forward model -- the recursion of src/libmycu/cumapdp/CuBatchMAPDP_fwd.cu

@@ -1,0 +1,80 @@
+"""Reader of the reference's binary profile database (c2_db2bin_read).
+
+Profiles are written in the COMER text format, turned into a binary
+database by the reference's own makedb and db2bin (built from its sources by
+oracle/build_ref.sh), and read back by this library.  The values must be
+those of the text profiles as the reference's text reader converts them
+(comer2_b200.textfmt.read_profiles): exact for target probabilities, context
+vectors and their priors and norms, backgrounds and ENOs; transitions within
+1e-7 (log computed in float or double); SS probabilities within 1.5e-4 (one
+text quantum: makedb's reader and the query-side reader round them
+differently).  Skipped where the reference tools are not built.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from comer2_b200 import synth as S
+from comer2_b200 import textfmt
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.path.join(ROOT, "oracle", "_ref")
+
+needs_ref = pytest.mark.skipif(not (os.path.exists(os.path.join(REF, "makedb")) and
+                                    os.path.exists(os.path.join(REF, "db2bin"))),
+                               reason="reference tools not built (oracle/build_ref.sh)")
+
+
+def _make_db(tmp, ps):
+    pro = tmp / "pro"
+    pro.mkdir()
+    texts = []
+    for k in range(ps.nprofiles):
+        f = pro / ("p%04d.pro" % k)
+        with open(f, "w") as fh:
+            textfmt.write_profile(fh, ps, k, "p%04d" % k, "p%04d" % k)
+        texts.append(f.read_text())
+    opts = os.path.join(REF, "var", "options.txt")
+    subprocess.run([os.path.join(REF, "makedb"), "-o", str(tmp / "db"), "-p", opts, "-d", str(pro)], check=True,
+                   capture_output=True)
+    subprocess.run([os.path.join(REF, "db2bin"), "-d", str(tmp / "db"), "-p", opts], check=True,
+                   capture_output=True)
+    return str(tmp / "db.bin"), textfmt.read_profiles("".join(texts))
+
+
+@needs_ref
+def test_db2bin_matches_text_profiles(tmp_path):
+    from comer2_b200.native import read_db2bin
+    rng = np.random.default_rng(5)
+    q = S.random_profiles(rng, [80])
+    ps = S.concat([S.random_profiles(rng, [31, 1, 140]), S.planted_homolog(rng, q, 90, 30, 60),
+                   S.random_profiles(rng, [64, 7])])
+    path, T = _make_db(tmp_path, ps)
+    P = read_db2bin(path)
+    assert P.nprofiles == T.nprofiles
+    assert int(P.lengths.sum()) == int(T.lengths.sum())
+    used = set()
+    for k in range(P.nprofiles):
+        L, o = int(P.lengths[k]), int(P.offsets[k])
+        m = [t for t in range(T.nprofiles) if t not in used and T.lengths[t] == L and
+             (T.aa[T.offsets[t]:T.offsets[t] + L] == P.aa[o:o + L]).all()][0]
+        used.add(m)
+        to = int(T.offsets[m])
+        for f in ("trg", "cv", "cvprior", "cvnorm2"):
+            assert np.array_equal(getattr(P, f)[o:o + L], getattr(T, f)[to:to + L]), f
+        assert np.array_equal(P.bkg[k], T.bkg[m])
+        assert P.eno[k] == pytest.approx(T.eno[m], abs=1e-6)
+        assert np.allclose(P.trn[o + k:o + k + L + 1], T.trn[to + m:to + m + L + 1], rtol=1e-6, atol=1e-7)
+        assert np.abs(P.ss[o:o + L] - T.ss[to:to + L]).max() <= 1.5e-4
+        sp = P.ssstate[o:o + L]
+        assert (np.where(sp == ord(" "), ord("C"), sp) == T.ssstate[to:to + L]).all()
+
+
+def test_db2bin_rejects_other_files(tmp_path):
+    from comer2_b200.native import C2Error, read_db2bin
+    f = tmp_path / "x.bin"
+    f.write_bytes(b"not a database" * 10)
+    with pytest.raises(C2Error, match="not a COMER binary profile database"):
+        read_db2bin(str(f))
