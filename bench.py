@@ -250,7 +250,7 @@ def main():
         for _ in range(args.steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            hits = h.search(q)
+            hits = h.search(q, arrays=True)
             torch.cuda.synchronize()
             e2e.append((time.perf_counter() - t0) * 1e3)
         e2e_ms = _max_over_ranks(float(np.mean(e2e)), world, backend)
@@ -266,12 +266,14 @@ def main():
                                         main_r["hits"])
 
     def hitset(hs):
-        return [(int(x["profile"]), round(float(x["logE"]), 3)) for x in hs]
+        rec, _ = hs
+        return [(int(p), round(float(e), 3)) for p, e in zip(rec["profile"], rec["logE"])]
 
     same_hits = hitset(res["bf16"]["hits"]) == hitset(res["fp32"]["hits"])
     nprof = w.db.nprofiles
     h2d = Lq * (64 + 6) * 4 + (Lq + 1) * 7 * 4 + 2 * Lq + 20 * 4
-    d2h = nprof * 4 + sum(5 * (x["alnlen"] + 1) for x in hits) + len(hits) * 80
+    hrec, hbuf = hits
+    d2h = nprof * 4 + int(hbuf.nbytes) + hrec.nbytes
     hbm_peak, peak_kind = _peaks()
     npos = int(w.db.lengths.sum())
     alg_bytes = 209.0 * npos                      # FP32 profile fields streamed per query pass
@@ -291,7 +293,7 @@ def main():
         "e2e": {"value": world * cells / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
-        "hits": len(hits), "homologs_found": int(sum(1 for x in hits if x["profile"] in set(w.homologs.tolist()))),
+        "hits": int(hrec.shape[0]), "homologs_found": int(np.isin(hrec["profile"], w.homologs).sum()),
         "stage_ms": {"phase1": p1ms, "finalize+stats+map": ms - p1ms},
         "score_forms": {
             "bf16": {"what": "score contractions as split-BF16 (hi+lo) tensor-core mma.sync, FP32 accumulate and DP",

@@ -78,6 +78,10 @@ class c2_hit(C.Structure):
                 ("beg", C.c_uint32), ("end", C.c_uint32), ("aln_offset", C.c_int64)]
 
 
+HIT_DTYPE = np.dtype([(k, {C.c_int32: np.int32, C.c_float: np.float32, C.c_uint32: np.uint32,
+                           C.c_int64: np.int64}[t]) for k, t in c2_hit._fields_], align=True)
+assert HIT_DTYPE.itemsize == C.sizeof(c2_hit)
+
 _lib: Optional[C.CDLL] = None
 
 
@@ -329,13 +333,26 @@ class Handle:
             out.append(d)
         return out
 
-    def search(self, q: ProfileSet):
-        """Complete search of query q over the uploaded database; returns the hits."""
+    def hits_arrays(self, n: int):
+        """The current hits as (records, alignments): a numpy structured array with
+        the c2_hit fields (sorted by log E-value) and the bytes holding each hit's
+        five NUL-terminated alignment strings from its aln_offset."""
+        sz = C.c_size_t(0)
+        self._ck(self.lib.c2_get_hits(self._h, None, 0, None, C.byref(sz)), "c2_get_hits(size)")
+        rec = np.zeros(max(n, 1), dtype=HIT_DTYPE)
+        buf = np.zeros(max(sz.value, 1), np.uint8)
+        self._ck(self.lib.c2_get_hits(self._h, rec.ctypes.data_as(C.POINTER(c2_hit)), n,
+                                      buf.ctypes.data_as(C.c_char_p), C.byref(sz)), "c2_get_hits")
+        return rec[:n], buf
+
+    def search(self, q: ProfileSet, arrays: bool = False):
+        """Complete search of query q over the uploaded database; returns the hits
+        as a list of dicts, or with arrays=True as hits_arrays() does."""
         k = _Keep()
         s = make_profiles(q, k)
         n = C.c_int32()
         self._ck(self.lib.c2_search(self._h, C.byref(s), C.byref(n)), "c2_search")
-        return self.hits(n.value)
+        return self.hits_arrays(n.value) if arrays else self.hits(n.value)
 
     def launch_count(self) -> int:
         n = C.c_uint64()

@@ -136,3 +136,20 @@ def test_no_hits_db(params):
     hits = h.search(q)
     assert len(hits) == 0
     h.close()
+
+
+def test_hits_arrays_match_dicts(params):
+    """search(arrays=True) returns the same records and alignment strings as the dict form."""
+    from comer2_b200.native import Handle
+    w = S.config(1, seed=2, scale=0.002)
+    h = Handle(params, 0)
+    h.upload_db(w.db)
+    hits = h.search(w.queries[0])
+    rec, buf = h.search(w.queries[0], arrays=True)
+    assert rec.shape[0] == len(hits) > 0
+    raw = buf.tobytes()
+    for x, r in zip(hits, rec):
+        assert int(r["profile"]) == x["profile"] and float(r["logE"]) == x["logE"]
+        o, L = int(r["aln_offset"]), int(r["alnlen"])
+        assert [raw[o + k * (L + 1):o + k * (L + 1) + L].decode() for k in range(5)] == x["strings"]
+    h.close()
