@@ -1213,3 +1213,96 @@ void orc_batch_phase1(const orc_params* P, const orc_profile* q, const orc_profi
     free(th);
     pthread_mutex_destroy(&J.mu);
 }
+
+/* ====================================================================== */
+/* Log-partition of the MAP forward model with exact exp/log, for the     */
+/* adjoint (differentiable alignment) checks.                             */
+/* ====================================================================== */
+static real xlse(const real* v, int n)
+{
+    real mx = v[0];
+    for (int k = 1; k < n; k++) mx = MAXR(mx, v[k]);
+    real s = 0;
+    for (int k = 0; k < n; k++) s += EXP(v[k] - mx);
+    return LOG(s) + mx;
+}
+
+/*
+ * logZ of the forward recursion of orc_map (same states, transitions, column
+ * -1 states and local start term; src/libmycu/cumapdp/CuBatchMAPDP_fwd.cu:72-478)
+ * over the score matrix S [lq*ld] (used as is: no log-E-value adjustment),
+ * with exact exp/log and theta[7] (MM MI MD IM II DM DD) added to the query
+ * row transitions of every cell update (the column -1 states use theta = 0).
+ * logZ = log of the sum over cells of exp(F.MM).
+ */
+real orc_logz(const orc_profile* q, const orc_profile* d, const real* S, const real* theta)
+{
+    const int lq = q->len, ld = d->len;
+    const size_t N = (size_t)lq * ld;
+    st5* F = (st5*)malloc(sizeof(st5) * N);
+    st5* CF = (st5*)malloc(sizeof(st5) * (size_t)lq);
+    for (int r = 0; r < lq; r++) {
+        trn7 t = map_trn(q, r);
+        st5 U = (r % 32 == 0) ? INIT5 : CF[r - 1];
+        st5 c;
+        real v[2];
+        c.MM = 0;
+        v[0] = (U.MM + t.MM) + MLOG0; v[1] = (U.MI + t.MM) + MLOG0; c.MI = xlse(v, 2);
+        if (r % 32 == 0) { v[0] = (INIT5.MM + t.MI) + MLOG0; v[1] = (INIT5.IM + t.II) + MLOG0; }
+        else { v[0] = ((real)0 + t.MI) + MLOG0; v[1] = ((((real)0 + t.MI) + MLOG0) + t.II) + MLOG0; }
+        c.IM = xlse(v, 2);
+        v[0] = U.MM + t.MD; v[1] = U.DN + t.DD; c.DN = xlse(v, 2);
+        c.ND = MLOG0;
+        CF[r] = c;
+    }
+    real acc = 0, mxF = -1e30;
+    for (int i = 0; i < lq; i++) {
+        trn7 qt = map_trn(q, i);
+        if (i < lq) {
+            qt.MM += theta[0]; qt.MI += theta[1]; qt.MD += theta[2]; qt.IM += theta[3];
+            qt.II += theta[4]; qt.DM += theta[5]; qt.DD += theta[6];
+        }
+        for (int j = 0; j < ld; j++) {
+            const trn7 t = map_trn(d, j);
+            st5 up = (i == 0) ? INIT5 : F[(size_t)(i - 1) * ld + j];
+            st5 left, diag;
+            if (j == 0) {
+                left = (i % 32 == 31) ? INIT5 : CF[i];
+                diag = (i % 32 == 31 || i % 32 == 0) ? INIT5 : CF[i - 1];
+            } else {
+                left = F[(size_t)i * ld + j - 1];
+                diag = (i == 0) ? INIT5 : F[(size_t)(i - 1) * ld + j - 1];
+            }
+            const real s = S[(size_t)i * ld + j];
+            st5 c;
+            real v[6];
+            v[0] = ((diag.MI + qt.MM) + t.IM) + s; v[1] = ((diag.IM + qt.IM) + t.MM) + s;
+            v[2] = ((diag.DN + qt.DM) + t.MM) + s; v[3] = ((diag.ND + qt.MM) + t.DM) + s;
+            v[4] = ((diag.MM + qt.MM) + t.MM) + s; v[5] = 0;
+            c.MM = xlse(v, 6);
+            v[0] = (up.MM + qt.MM) + t.MI; v[1] = (up.MI + qt.MM) + t.II; c.MI = xlse(v, 2);
+            v[0] = (left.MM + qt.MI) + t.MM; v[1] = (left.IM + qt.II) + t.MM; c.IM = xlse(v, 2);
+            v[0] = up.MM + qt.MD; v[1] = up.DN + qt.DD; c.DN = xlse(v, 2);
+            v[0] = left.MM + t.MD; v[1] = left.ND + t.DD; c.ND = xlse(v, 2);
+            F[(size_t)i * ld + j] = c;
+            mxF = MAXR(mxF, c.MM);
+        }
+    }
+    for (size_t k = 0; k < N; k++) acc += EXP(F[k].MM - mxF);
+    free(F); free(CF);
+    return LOG(acc) + mxF;
+}
+
+/* The three parts of the cell score (amino acids; SS and CV terms before
+ * their weights), so that S = s0 + wss * ss + wcv * cv. */
+void orc_score_parts(const orc_params* P, const orc_profile* q, const orc_profile* d, real* S0, real* SSr, real* CVr)
+{
+    orc_params U = *P;
+    U.ssswgt = 1.0f;
+    U.cvswgt = 1.0f;
+    for (int i = 0; i < q->len; i++)
+        for (int j = 0; j < d->len; j++) {
+            const size_t k = (size_t)i * d->len + j;
+            orc_score_cell(&U, q, d, i, j, NULL, NULL, S0 + k, SSr + k, CVr + k);
+        }
+}

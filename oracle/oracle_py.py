@@ -86,6 +86,10 @@ class Oracle:
         L.orc_length_adjustment.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, C.c_size_t,
                                             C.c_ulonglong, C.c_size_t, C.POINTER(C.c_ulonglong),
                                             C.POINTER(C.c_ulonglong)]
+        L.orc_logz.argtypes = [C.POINTER(orc_profile), C.POINTER(orc_profile), rp, rp]
+        L.orc_logz.restype = self.crt
+        L.orc_score_parts.argtypes = [C.POINTER(orc_params), C.POINTER(orc_profile), C.POINTER(orc_profile),
+                                      rp, rp, rp]
         self.StatsOut = _stats_out(self.crt)
         self.MapOut = _map_out(self.crt)
         L.orc_stats.argtypes = [C.POINTER(orc_stats_in), rp, _u8p, _u8p, C.c_int, C.POINTER(self.StatsOut)]
@@ -155,6 +159,22 @@ class Oracle:
         self.lib.orc_score_matrix(C.byref(self.P), C.byref(q), C.byref(d), S.ctypes.data_as(rp),
                                   M.ctypes.data_as(rp))
         return S, M
+
+    def score_parts(self, q, d):
+        """Amino-acid score and the SS and CV terms before their weights, [Lq][Ld] each."""
+        sh = (q.len, d.len)
+        S0, SS, CV = (np.zeros(sh, self.rt) for _ in range(3))
+        rp = C.POINTER(self.crt)
+        self.lib.orc_score_parts(C.byref(self.P), C.byref(q), C.byref(d), S0.ctypes.data_as(rp),
+                                 SS.ctypes.data_as(rp), CV.ctypes.data_as(rp))
+        return S0, SS, CV
+
+    def logz(self, q, d, S, theta=None):
+        """Exact log-partition of the MAP forward model over S (theta: 7 query transition offsets)."""
+        S = np.ascontiguousarray(S, self.rt)
+        th = np.zeros(7, self.rt) if theta is None else np.ascontiguousarray(theta, self.rt)
+        rp = C.POINTER(self.crt)
+        return float(self.lib.orc_logz(C.byref(q), C.byref(d), S.ctypes.data_as(rp), th.ctypes.data_as(rp)))
 
     def dp(self, q, d, S, with_btck: bool = False):
         S = np.ascontiguousarray(S, self.rt)
