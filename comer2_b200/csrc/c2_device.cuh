@@ -64,12 +64,28 @@ constexpr int MAX_CVCARD = 256;
 // m16 x k16) per query: qa[strip][mtile 2][dot 2: cv, ss][ktile 2][split 2]
 // [lane 32][4 words] and the unscaled amino-acid rows qaa[strip][mtile 2]
 // [ktile 2][lane 32][8 floats] (scaled per pair by 1 / (0.5 (bq + bd))).
+// The constant parts of the CV and SS terms ride in the spare K columns:
+// CV k = 19 carries 1 (query) x 1/kappa0 (db), so the CV accumulator is the
+// shifted dot product; the SS operand is weighted by the SS weight on the db
+// side and k = 30, 31 carry P(H)q + 0.1 x w (P(H)d + 0.1) / 9 and 1 x -0.05 w,
+// so the SS accumulator is the complete weighted SS term (the reference's
+// "-99 < ss" guard always holds for tables above SS_FOLD_MIN, which the
+// tensor-core form requires, with card <= 30).
 // Per db position the DP and the score epilogue also read a column record
-// cold[pos][P1C_TRS]: transitions 0..6, pad, cvnorm, CV prior, P(H) + 0.1, pad.
+// cold[pos][P1C_TRS]: the DP transitions in the pair order below (slots
+// 0..8), cvnorm, 2 x CV log prior, pad.
 constexpr int TC_TILE_WORDS = 3 * 2 * 2 * 32 * 2;
 constexpr int TC_QA_WORDS = 2 * 2 * 2 * 2 * 32 * 4;   // per strip
 constexpr int TC_QAA_FLOATS = 2 * 2 * 32 * 8;         // per strip
-enum : int { CO_CD = 8, CO_PD = 9, CO_HD = 10 };
+constexpr float SS_FOLD_MIN = -49.f;
+constexpr int TC_SS_KMAX = 30;
+enum : int { CO_CD = 9, CO_PD2 = 10 };
+// DP transition record of a db column, ordered for the packed-pair Viterbi
+// step: (MM, MM), (IM, MM), (MD, DD), MI, II, DM.  DPT_SRC packs, per record
+// slot i, the transition index (TMM..TDD) in bits [4i, 4i + 4).
+constexpr int DPT_N = 9;
+constexpr unsigned long long DPT_SRC = 0x541620300ull;
+__host__ __device__ constexpr int dpt_src(int i) { return (int)((DPT_SRC >> (4 * i)) & 0xf); }
 // chunked phase-1 kernel: 11 warps per CTA, one CTA per SM; per warp a score
 // ring of 64 columns x 32 rows, a transition ring of 64 columns (stride 12
 // floats: the two 16-byte reads of 8 lanes at consecutive columns cover 32
@@ -81,13 +97,25 @@ enum : int { P1K_STRIP = 0, P1K_CHUNKED = 1, P1K_TRACEBACK = 2, P1K_TENSOR = 3 }
 constexpr int P1C_RING = 64, P1C_TRS = 12, P1C_CVREP = 16;
 constexpr int P1C_WARP_FLOATS =
     P1C_RING * 32 + P1C_RING * P1C_TRS + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE + 32 * 8;
-// tensor-core kernel: score ring of 64 columns with 36 floats per column (the
+// tensor-core kernel: score ring of 64 anti-diagonals with 36 floats each (the
 // fragment-layout writes and the per-lane wavefront reads are both free of
-// bank conflicts), a column-record ring of 4 chunks, the row above the strip
-// and two slots for db operand tiles (bulk async copies, one mbarrier each)
+// bank conflicts), a column-record ring of 3 chunks plus a mirror of its first
+// chunk (slots 96..127), so that the 32 records a lane reads in one DP stage
+// never wrap, the row above the strip and two slots for db operand tiles
+// (bulk async copies, one mbarrier each)
 constexpr int P1T_WARPS = 10;
-constexpr int P1T_RLD = 36, P1T_CRING = 128, P1T_CVREP = 8;
+constexpr int P1T_RLD = 36, P1T_CRING = 128, P1T_CMOD = 96, P1T_CVREP = 8;
+constexpr unsigned P1T_TMEM_COLS = 512;   // TMEM columns of a CTA (3 warps x 128 per lane quarter)
 constexpr int P1T_WARP_FLOATS = P1C_RING * P1T_RLD + P1T_CRING * P1C_TRS + 32 * 8 + 2 * TC_TILE_WORDS + 4;
+
+// Epilogue constants of the tensor-core form: x = 2 x (CV score argument)
+// = (2 pownu0 ln2) log2(det) + 2 cterm - 2 prior_q - 2 prior_d, compared
+// with twice the table keys; table values pre-multiplied by the CV weight.
+// uniform: the table index clamp alone reproduces the key range tests.
+struct TcConsts {
+    float shift, p2l, c2, kf2, kl2, vfw, vlw;
+    int ilo, ihi, uniform;
+};
 
 struct P1Args {
     const float* qrec;      // [Lq][QR_STRIDE]
@@ -125,6 +153,7 @@ struct P1Args {
     const float* cold;          // [npos][P1C_TRS] column records
     const unsigned* qa;         // query A fragments (cv, ss)
     const float* qaa;           // query amino-acid rows in fragment order
+    TcConsts tc;
 };
 
 struct FinArgs {

@@ -31,7 +31,7 @@ int p1_blocks_per_sm(int cvcard);
 int p1c_blocks_per_sm(int cvcard);
 int p1t_blocks_per_sm(int cvcard, cudaError_t* err);
 cudaError_t launch_tc_pack(const float* drec, const long long* poff, const int* plen, const long long* ttile,
-                           int nprof, unsigned* tcdb, float* cold, cudaStream_t st);
+                           int nprof, unsigned* tcdb, float* cold, float lok, float wss, cudaStream_t st);
 cudaError_t launch_fin(const FinArgs& a, cudaStream_t st);
 }  // namespace c2
 
@@ -530,8 +530,9 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
     if (h->d_qrec.ensure(h->h_qrec.size()) || h->d_qbkg.ensure(NAA))
         return fail(h, C2_ERR_NOMEM, "query allocation failed");
     // tensor-core query operands (layouts in c2_device.cuh): context vectors
-    // and SS row tables U[r][c] = sum_s p_q(s) T[idx_q(s)][c] as split BF16 A
-    // fragments, amino-acid rows unscaled in fragment order
+    // (k = 19: 1, the 1/kappa0 column) and SS row tables
+    // U[r][c] = sum_s p_q(s) T[idx_q(s)][c] (k = 30: P(H) + 0.1, k = 31: 1) as
+    // split BF16 A fragments, amino-acid rows unscaled in fragment order
     {
         const int ns = (Lq + 31) / 32;
         const int card = h->sc.ssss_card;
@@ -545,7 +546,9 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
         }
         auto aval = [&](int d, int r, int k) -> float {
             if (r >= Lq) return 0.f;
-            if (d == 0) return k < NCV ? q->cv[(size_t)r * NCV + k] : 0.f;
+            if (d == 0) return k < NCV ? q->cv[(size_t)r * NCV + k] : (k == NCV ? 1.f : 0.f);
+            if (k == TC_SS_KMAX) return h->h_qrec[(size_t)r * QR_STRIDE + QR_HQ];
+            if (k == TC_SS_KMAX + 1) return 1.f;
             return k < card ? U[(size_t)r * 32 + k] : 0.f;
         };
         std::vector<uint32_t> qa((size_t)ns * TC_QA_WORDS, 0u);
@@ -667,6 +670,25 @@ extern "C" c2_status c2_get_thresholds(const c2_handle* h, float* s, float* le)
     return C2_OK;
 }
 
+// Epilogue constants of the tensor-core form (TcConsts in c2_device.cuh)
+static TcConsts tc_consts(const ScoreConsts& sc)
+{
+    TcConsts t;
+    t.shift = sc.shift;
+    t.p2l = 2.f * sc.pownu0 * 0.693147180559945309f;
+    t.c2 = 2.f * sc.cterm;
+    t.kf2 = 2.f * sc.cvkey_first;
+    t.kl2 = 2.f * sc.cvkey_last;
+    t.vfw = sc.cvval_first * sc.cvswgt;
+    t.vlw = sc.cvval_last * sc.cvswgt;
+    t.ilo = -sc.cvshift;
+    t.ihi = sc.cvcard - 1 - sc.cvshift;
+    // x <= 2 key_first gives index <= 0 and x >= 2 key_last index >= card - 1
+    // when the keys sit at the table's ends: the clamp alone is exact then
+    t.uniform = (sc.cvshift + (int)rintf(t.kf2) <= 0 && sc.cvshift + (int)rintf(t.kl2) >= sc.cvcard - 1) ? 1 : 0;
+    return t;
+}
+
 // Pack the db operands of the tensor-core path (once per database).
 static c2_status tc_prepare_db(c2_handle* h)
 {
@@ -682,7 +704,7 @@ static c2_status tc_prepare_db(c2_handle* h)
         return fail(h, C2_ERR_NOMEM, "tensor-core db operands (%lld tiles) allocation failed", ntiles);
     CK(cudaMemcpyAsync(h->d_ttile.p, tt.data(), (size_t)h->nprof * 8, cudaMemcpyHostToDevice, h->stream));
     CK(launch_tc_pack(h->d_drec.p, h->d_poff.p, h->d_plen.p, h->d_ttile.p, h->nprof, h->d_tcdb.p, h->d_cold.p,
-                      h->stream));
+                      h->sc.lokappa0, h->sc.ssswgt, h->stream));
     h->launches++;
     CK(cudaStreamSynchronize(h->stream));
     h->tc_ready = true;
@@ -693,6 +715,15 @@ extern "C" c2_status c2_set_score_mode(c2_handle* h, int32_t mode)
 {
     if (!h) return C2_ERR_ARG;
     if (mode != C2_SCORE_FP32 && mode != C2_SCORE_BF16_TC) return fail(h, C2_ERR_ARG, "unknown score mode %d", mode);
+    if (mode == C2_SCORE_BF16_TC) {
+        // the SS constants ride in K columns 30 and 31, and dropping the
+        // reference's "-99 < ss" guard needs table entries well above -99
+        if (h->sc.ssss_card > TC_SS_KMAX)
+            return fail(h, C2_ERR_ARG, "tensor-core score form needs an SS table of at most %d states", TC_SS_KMAX);
+        for (float v : h->ssss)
+            if (!(v >= SS_FOLD_MIN))
+                return fail(h, C2_ERR_ARG, "tensor-core score form needs SS table entries >= %g", (double)SS_FOLD_MIN);
+    }
     h->score_mode = mode;
     return C2_OK;
 }
@@ -735,6 +766,7 @@ extern "C" c2_status c2_run_phase1(c2_handle* h)
         a.cold = h->d_cold.p;
         a.qa = h->d_qa.p;
         a.qaa = h->d_qaaf.p;
+        a.tc = tc_consts(h->sc);
         cudaError_t oe = cudaSuccess;
         int gt = h->nsm * p1t_blocks_per_sm(h->sc.cvcard, &oe);
         if (gt < 1)

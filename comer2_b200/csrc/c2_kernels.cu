@@ -587,76 +587,151 @@ p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
 // rings; then the warp advances the anti-diagonal wavefront by 32 steps.
 // Wavefront steps whose 32 cells all lie inside the matrix (every chunk but
 // the first and the last ones of a strip) run without bounds checks.
-struct DPLane {
-    St5 mine, upp;           // own state at the previous step, up-state of the previous step
-    float q7[7];             // row transitions
-    float bnxt[5];           // row above the strip: columns [32m+32, 32m+64) (lane i: column 32m+32+i)
+//
+// Score rings are indexed by anti-diagonal: the score of cell (row i of the
+// strip, column j) sits in slot (i + j) & 63, so at step k every lane reads
+// slot k & 63 and a DP stage reads 32 consecutive slots from one base.
+
+// Packed FP32 pair add (sm_100 add.f32x2): two IEEE round-to-nearest adds,
+// bit-identical to the scalar ones.
+__device__ __forceinline__ float2 add2(float2 a, float2 b)
+{
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
+// Maximum of three (sm_100 three-input max.f32; exact, like two fmaxf)
+__device__ __forceinline__ float max3f(float a, float b, float c)
+{
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+// One lane of the wavefront DP.  Every Viterbi candidate of the reference's
+// recurrence is (state + query transition) + db transition, evaluated in that
+// order (bit-identical to the scalar form) and issued as packed pairs where
+// two candidates share the operation:
+//   X = (up.MM, up.DN) + (qMM, qDM)   W = (up.MM, up.DN) + (qMD, qDD)
+//   Y = (up.MI, up.IM) + (qMM, qIM)   z = up.ND + qMM
+// X, Y and z are the up-sums of this step and the diagonal sums of the next
+// (the diagonal predecessor of a cell is the up-neighbour of its left one).
+struct WfLane {
+    float MM, MI, IM, DN, ND;     // own state at the previous step (left)
+    float2 X, Y;                  // up-sums of the previous step
+    float z;
+    float2 qX, qW, qY;            // (qMM, qDM), (qMD, qDD), (qMM, qIM)
+    float qMM, qMI, qII;
+    float2 XB, YB;                // diagonal sums of the column -1 boundary state
+    float zB, lbMM, lbIM, lbND;   // and the column -1 left state
+    float bnxt[5];                // row above the strip: columns [32m+32, 32m+64) (lane i: column 32m+32+i)
     float best;
     int kbest;
 };
 
-// RLD: floats per column of the score ring; TMASK: slot mask of the
-// transition ring (stride P1C_TRS floats per column)
-template <bool CHECK, int RLD = 32, int TMASK = P1C_RING - 1>
-__device__ __forceinline__ void p1c_steps(DPLane& D, int k0, int k1, int lane, int L, bool act, int cA, int cB,
-                                          const float* __restrict__ ring, const float* __restrict__ trn,
-                                          const float* __restrict__ bnd, const St5& LB, const St5& DB, bool wr_bot,
-                                          float* __restrict__ botw, int Lmax)
+__device__ __forceinline__ void wf_init(WfLane& D, const float* q7, const St5& LB, const St5& DB)
 {
-#pragma unroll 4
-    for (int k = k0; k < k1; k++) {
-        const int j = k - lane;
-        const int slot = j & (P1C_RING - 1);
-        float S = ring[slot * RLD + lane];
-        if (j <= cA || j >= cB) S = -9.f;   // corner cells (CellYXinCorners)
-        float t7[7];
-        {
-            const int ts = (j & TMASK) * P1C_TRS;
-            const float4 ta = *reinterpret_cast<const float4*>(trn + ts);
-            const float4 tb = *reinterpret_cast<const float4*>(trn + ts + 4);
-            t7[0] = ta.x; t7[1] = ta.y; t7[2] = ta.z; t7[3] = ta.w;
-            t7[4] = tb.x; t7[5] = tb.y; t7[6] = tb.z;
-        }
-        St5 up;
-        up.MM = __shfl_up_sync(FULL, D.mine.MM, 1);
-        up.MI = __shfl_up_sync(FULL, D.mine.MI, 1);
-        up.IM = __shfl_up_sync(FULL, D.mine.IM, 1);
-        up.DN = __shfl_up_sync(FULL, D.mine.DN, 1);
-        up.ND = __shfl_up_sync(FULL, D.mine.ND, 1);
+    D.qX = make_float2(q7[TMM], q7[TDM]);
+    D.qW = make_float2(q7[TMD], q7[TDD]);
+    D.qY = make_float2(q7[TMM], q7[TIM]);
+    D.qMM = q7[TMM];
+    D.qMI = q7[TMI];
+    D.qII = q7[TII];
+    D.XB = add2(make_float2(DB.MM, DB.DN), D.qX);
+    D.YB = add2(make_float2(DB.MI, DB.IM), D.qY);
+    D.zB = DB.ND + q7[TMM];
+    D.lbMM = LB.MM;
+    D.lbIM = LB.IM;
+    D.lbND = LB.ND;
+    D.MM = D.MI = D.IM = D.DN = D.ND = 0.f;
+    D.X = D.Y = make_float2(0.f, 0.f);
+    D.z = 0.f;
+    D.best = 0.f;
+    D.kbest = 0;
+}
+
+// Wavefront steps [k0, k0 + nst) of a strip (k0 a multiple of 32, nst <= 32;
+// 32 when !CHECK).  ring: diagonal-indexed scores, RLD floats per slot.
+// Column records (DPT_N transitions, P1C_TRS floats apart): with TMIRROR,
+// tcol points at this lane's record for step k0 and the next 31 follow
+// without wrapping; otherwise tcol is a ring of TMASK + 1 records indexed by
+// column & TMASK.  bnd: row above the strip for columns [k0, k0 + 32).
+template <bool CHECK, int RLD, bool TMIRROR, int TMASK>
+__device__ __forceinline__ void wf_steps(WfLane& D, int k0, int nst, int lane, int L, bool act,
+                                         const float* __restrict__ ring, const float* __restrict__ tcol,
+                                         const float* __restrict__ bnd, bool wr_bot, float* __restrict__ botw,
+                                         int Lmax)
+{
+    const float* __restrict__ rb = ring + (k0 & (P1C_RING - 1)) * RLD + lane;
+    if (!CHECK) nst = 32;
+    int ub = -1;
+#pragma unroll 8
+    for (int u = 0; u < nst; u++) {
+        const float S = rb[u * RLD];
+        const float* __restrict__ tp =
+            TMIRROR ? tcol + u * P1C_TRS : tcol + ((k0 + u - lane) & TMASK) * P1C_TRS;
+        const float4 ta = *reinterpret_cast<const float4*>(tp);       // MM MM IM MM
+        const float4 tb = *reinterpret_cast<const float4*>(tp + 4);   // MD DD MI II
+        const float tDM = tp[8];
+        float uMM = __shfl_up_sync(FULL, D.MM, 1);
+        float uMI = __shfl_up_sync(FULL, D.MI, 1);
+        float uIM = __shfl_up_sync(FULL, D.IM, 1);
+        float uDN = __shfl_up_sync(FULL, D.DN, 1);
+        float uND = __shfl_up_sync(FULL, D.ND, 1);
         {
             // row above the strip at column k (lane 0's column), broadcast reads
-            const float4 ba = *reinterpret_cast<const float4*>(bnd + (k & 31) * 8);
-            const float b4 = bnd[(k & 31) * 8 + 4];
-            if (lane == 0) up = St5{ba.x, ba.y, ba.z, ba.w, b4};
+            const float4 ba = *reinterpret_cast<const float4*>(bnd + u * 8);
+            const float b4 = bnd[u * 8 + 4];
+            if (lane == 0) { uMM = ba.x; uMI = ba.y; uIM = ba.z; uDN = ba.w; uND = b4; }
         }
-        St5 left = D.mine, diag = D.upp;
-        if (CHECK && j == 0) { left = LB; diag = DB; }
-        const float* q7 = D.q7;
-        St5 nw;
-        {
-            float v = fmaxf((diag.MI + q7[TMM]) + t7[TIM], (diag.IM + q7[TIM]) + t7[TMM]);
-            v = fmaxf(v, (diag.DN + q7[TDM]) + t7[TMM]);
-            v = fmaxf(v, (diag.ND + q7[TMM]) + t7[TDM]);
-            v = fmaxf(v, (diag.MM + q7[TMM]) + t7[TMM]);
-            nw.MM = fmaxf(v + S, 0.f);
-            nw.MI = fmaxf((up.MM + q7[TMM]) + t7[TMI], (up.MI + q7[TMM]) + t7[TII]);
-            nw.IM = fmaxf((left.MM + q7[TMI]) + t7[TMM], (left.IM + q7[TII]) + t7[TMM]);
-            nw.DN = fmaxf(up.MM + q7[TMD], up.DN + q7[TDD]);
-            nw.ND = fmaxf(left.MM + t7[TMD], left.ND + t7[TDD]);
+        const int j = k0 + u - lane;
+        float2 Xd = D.X, Yd = D.Y;
+        float zd = D.z, lMM = D.MM, lIM = D.IM, lND = D.ND;
+        if (CHECK && j == 0) {
+            Xd = D.XB; Yd = D.YB; zd = D.zB;
+            lMM = D.lbMM; lIM = D.lbIM; lND = D.lbND;
         }
+        const float2 T0 = make_float2(ta.x, ta.y), T1 = make_float2(ta.z, ta.w), T2 = make_float2(tb.x, tb.y);
+        const float2 X = add2(make_float2(uMM, uDN), D.qX);
+        const float2 W = add2(make_float2(uMM, uDN), D.qW);
+        const float2 Y = add2(make_float2(uMI, uIM), D.qY);
+        const float z = uND + D.qMM;
+        const float2 c53 = add2(Xd, T0);   // diag MM + MM + MM, diag DN + DM + MM
+        const float2 c12 = add2(Yd, T1);   // diag MI + MM + IM, diag IM + IM + MM
+        const float v = max3f(max3f(c12.x, c12.y, c53.y), zd + tDM, c53.x);
+        const float nMM = fmaxf(v + S, 0.f);
+        const float nMI = fmaxf(X.x + tb.z, Y.x + tb.w);
+        const float2 c89 = add2(make_float2(lMM + D.qMI, lIM + D.qII), T0);
+        const float2 cND = add2(make_float2(lMM, lND), T2);
+        const float nIM = fmaxf(c89.x, c89.y);
+        const float nDN = fmaxf(W.x, W.y);
+        const float nND = fmaxf(cND.x, cND.y);
+        // inactive lanes (rows past the query) carry LOG0 query transitions:
+        // their MM stays 0 and never beats a maximum
         const bool inm = !CHECK || (j >= 0 && j < L);
-        if (act && inm && nw.MM > D.best) { D.best = nw.MM; D.kbest = k; }
+        if ((!CHECK || act) && inm && nMM > D.best) { D.best = nMM; ub = u; }
         if (wr_bot && inm) {
-            botw[0 * Lmax + j] = nw.MM;
-            botw[1 * Lmax + j] = nw.MI;
-            botw[2 * Lmax + j] = nw.IM;
-            botw[3 * Lmax + j] = nw.DN;
-            botw[4 * Lmax + j] = nw.ND;
+            float* bw = botw + (k0 - 31 + u);
+            bw[0 * Lmax] = nMM;
+            bw[1 * Lmax] = nMI;
+            bw[2 * Lmax] = nIM;
+            bw[3 * Lmax] = nDN;
+            bw[4 * Lmax] = nND;
         }
-        D.mine = nw;
-        D.upp = up;
+        D.MM = nMM; D.MI = nMI; D.IM = nIM; D.DN = nDN; D.ND = nND;
+        D.X = X; D.Y = Y; D.z = z;
     }
+    if (ub >= 0) D.kbest = k0 + ub;
 }
+
+// Corner cells (CellYXinCorners): row r keeps S = -9 at columns j <= cA(r)
+// and j >= cB(r).
+__device__ __forceinline__ int corner_a(int r, int Lq, int edge) { return (Lq <= r + edge) ? edge + r - Lq : -1; }
+__device__ __forceinline__ int corner_b(int r, int L, int edge) { return (r < edge) ? L - edge + r : 0x7fffffff; }
 
 __global__ void __launch_bounds__(P1C_WARPS * 32, 1)
 p1c_kernel(P1Args a, const float* __restrict__ qbkg)
@@ -718,9 +793,10 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
                     U[c * 32 + lane] = q0 * __ldg(a.ssss + i0 * card + c) + q1 * __ldg(a.ssss + i1 * card + c) +
                                        q2 * __ldg(a.ssss + i2 * card + c);
             }
-            DPLane D;
+            WfLane D;
+            float q7[7];
 #pragma unroll
-            for (int i = 0; i < 7; i++) D.q7[i] = act ? qr[QR_TRN + i] : LOG0;
+            for (int i = 0; i < 7; i++) q7[i] = act ? qr[QR_TRN + i] : LOG0;
             // column -1 boundary states of this row and of the row above
             const bool z_left = (lane == 31);
             const bool z_diag = (lane == 31 || lane == 0);
@@ -729,12 +805,9 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
             const St5 DB = z_diag ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
                                   : St5{0.f, qr[QR_CP + 0], qr[QR_CP + 1], qr[QR_CP + 2], LOG0};
             // corner cells of this row: j <= cA or j >= cB
-            const int cA = (Lq <= r + edge) ? edge + r - Lq : -1;
-            const int cB = (r < edge) ? L - edge + r : 0x7fffffff;
-            D.mine = St5{0.f, 0.f, 0.f, 0.f, 0.f};
-            D.upp = D.mine;
-            D.best = 0.f;
-            D.kbest = 0;
+            const int cA = corner_a(r, Lq, edge);
+            const int cB = corner_b(r, L, edge);
+            wf_init(D, q7, LB, DB);
             float bc[5];
 #pragma unroll
             for (int f = 0; f < 5; f++) {
@@ -758,6 +831,8 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
                 // ---- score stage: columns [32m, min(32m + 32, L))
                 if (m < nch) {
                     const int c0 = 32 * m, c1 = min(c0 + 32, L);
+                    // does any row of the strip have corner cells in this chunk?
+                    const bool hasc = __any_sync(FULL, cA >= c0 || cB < c1);
                     for (int c = c0; c < c1; c++) {
                         if ((c & (REC_CHUNK - 1)) == 0) {
                             cp_async_wait_1();
@@ -767,9 +842,9 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
                         float mod;
                         float Sc = cell_score<P1C_CVREP>(R, reinterpret_cast<const float4*>(rc), U, cvtab, sc, lane, mod);
                         (void)mod;
-                        const int slot = c & (P1C_RING - 1);
-                        ring[slot * 32 + lane] = Sc;
-                        if (lane < 7) trn[slot * P1C_TRS + lane] = rc[DR_TRN + lane];
+                        if (hasc && (c <= cA || c >= cB)) Sc = -9.f;
+                        ring[((c + lane) & (P1C_RING - 1)) * 32 + lane] = Sc;
+                        if (lane < DPT_N) trn[(c & (P1C_RING - 1)) * P1C_TRS + lane] = rc[DR_TRN + dpt_src(lane)];
                         if ((c & (REC_CHUNK - 1)) == REC_CHUNK - 1) {
                             // group fully read by every lane: refill its slots two groups ahead
                             __syncwarp();
@@ -781,9 +856,11 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
                 // ---- DP stage: wavefront steps [32m, 32m + 32)
                 const int k0 = 32 * m, k1 = min(k0 + 32, kend);
                 if (m >= 1 && k0 + 31 < L && k1 == k0 + 32)
-                    p1c_steps<false>(D, k0, k1, lane, L, act, cA, cB, ring, trn, bnd, LB, DB, wr_bot, botw, Lmax);
+                    wf_steps<false, 32, false, P1C_RING - 1>(D, k0, 32, lane, L, act, ring, trn, bnd, wr_bot, botw,
+                                                             Lmax);
                 else
-                    p1c_steps<true>(D, k0, k1, lane, L, act, cA, cB, ring, trn, bnd, LB, DB, wr_bot, botw, Lmax);
+                    wf_steps<true, 32, false, P1C_RING - 1>(D, k0, k1 - k0, lane, L, act, ring, trn, bnd, wr_bot,
+                                                            botw, Lmax);
                 __syncwarp();
                 // next 32 columns of the row above the strip
                 *reinterpret_cast<float4*>(bnd + lane * 8) = make_float4(D.bnxt[0], D.bnxt[1], D.bnxt[2], D.bnxt[3]);
@@ -855,6 +932,55 @@ __device__ __forceinline__ void mma_bf16(float* d, const unsigned* a, unsigned b
 // mbarrier and bulk (non-tensor, non-multicast) async copy helpers
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
+// Tensor memory (TMEM) as a per-lane store of loop-invariant fragments: the
+// allocating warp takes ncols columns for the CTA; warp w reads and writes
+// lanes [32 (w % 4), 32 (w % 4) + 32) only (32x32b shape: thread i <-> lane
+// 32 (w % 4) + i, consecutive 32-bit columns).
+__device__ __forceinline__ void tmem_alloc(unsigned* dst_smem, unsigned ncols)
+{
+    const unsigned a = (unsigned)__cvta_generic_to_shared(dst_smem);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(a), "r"(ncols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_st16(unsigned taddr, const unsigned* v)
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};" ::"r"(taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+        "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+// 32 columns into v; the wait takes v as operands so no use of v can be
+// scheduled before the load has completed
+__device__ __forceinline__ void tmem_ld32(unsigned taddr, unsigned* v)
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+          "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+          "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+          "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
+                   "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]),
+                   "+r"(v[15]), "+r"(v[16]), "+r"(v[17]), "+r"(v[18]), "+r"(v[19]), "+r"(v[20]), "+r"(v[21]),
+                   "+r"(v[22]), "+r"(v[23]), "+r"(v[24]), "+r"(v[25]), "+r"(v[26]), "+r"(v[27]), "+r"(v[28]),
+                   "+r"(v[29]), "+r"(v[30]), "+r"(v[31])
+                 :
+                 : "memory");
+}
+
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count)
 {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
@@ -888,10 +1014,12 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 }
 
 // Pack the db operands of one profile per CTA (4 warps over its 8-column
-// tiles) and its column records.
+// tiles) and its column records.  lok: 1/kappa0 (CV column k = 19); wss: SS
+// weight (SS operand and its folded columns k = 30, 31).
 __global__ void __launch_bounds__(128) tc_pack_kernel(const float* __restrict__ drec, const long long* __restrict__ poff,
                                                       const int* __restrict__ plen, const long long* __restrict__ ttile,
-                                                      unsigned* __restrict__ tcdb, float* __restrict__ cold)
+                                                      unsigned* __restrict__ tcdb, float* __restrict__ cold, float lok,
+                                                      float wss)
 {
     const int p = blockIdx.x;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -917,8 +1045,12 @@ __global__ void __launch_bounds__(128) tc_pack_kernel(const float* __restrict__ 
                     float x = 0.f;
                     if (valid) {
                         if (d == 0) x = (k < NAA) ? rc[DR_TRG + k] : 0.f;
-                        else if (d == 1) x = (k < NCV) ? rc[DR_CV + k] : 0.f;
-                        else x = (k == i0) ? rc[DR_SS] : (k == i1) ? rc[DR_SS + 1] : (k == i2) ? rc[DR_SS + 2] : 0.f;
+                        else if (d == 1) x = (k < NCV) ? rc[DR_CV + k] : (k == NCV) ? lok : 0.f;
+                        else if (k == i0) x = wss * rc[DR_SS];
+                        else if (k == i1) x = wss * rc[DR_SS + 1];
+                        else if (k == i2) x = wss * rc[DR_SS + 2];
+                        else if (k == TC_SS_KMAX) x = wss * (rc[DR_HD] * 0.1111111f);
+                        else if (k == TC_SS_KMAX + 1) x = -0.05f * wss;
                     }
                     v[e] = x;
                 }
@@ -937,52 +1069,52 @@ __global__ void __launch_bounds__(128) tc_pack_kernel(const float* __restrict__ 
         const float* rc = drec + (off + c) * DR_STRIDE;
         float* o = cold + (off + c) * P1C_TRS;
 #pragma unroll
-        for (int i = 0; i < 7; i++) o[i] = rc[DR_TRN + i];
-        o[7] = 0.f;
+        for (int i = 0; i < DPT_N; i++) o[i] = rc[DR_TRN + dpt_src(i)];
         o[CO_CD] = rc[DR_CN];
-        o[CO_PD] = rc[DR_PRIOR];
-        o[CO_HD] = rc[DR_HD];
+        o[CO_PD2] = 2.f * rc[DR_PRIOR];
         o[11] = 0.f;
     }
 }
 
-// Score epilogue of one cell from its three contractions (same arithmetic as
-// cell_score after the dot products)
-template <int CVREP>
-__device__ __forceinline__ float tc_epilogue(float daa, float dcv, float dss, float cq, float pq, float hq, float cd,
-                                             float pd, float hd, const float* __restrict__ cvtab,
-                                             const ScoreConsts& sc, int lane)
+// Score epilogue of one cell of the tensor-core form from its three
+// contractions (the CV one with 1/kappa0 folded in, the SS one the complete
+// weighted SS term):
+//   s0  = ln(aa) - shift
+//   x   = 2 (cterm + pownu0 ln(cq cd - dot^2) - prior_q - prior_d)
+//   cvm = w_cv T[shift + rint(x)] (T clamped; the key range tests when the
+//         table is not uniform), S = s0 + (ss + cvm)
+// (cell_score is the FP32 form; src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cu)
+constexpr float C2_LN2 = 0.693147180559945309f;
+__device__ __forceinline__ float tc_cell(float daa, float dot, float ss, float cq, float pq2, float cd, float pd2,
+                                         const float* __restrict__ cvl, const TcConsts& tc)
 {
-    const float s0 = __logf(daa) - sc.shift;
-    const float dot = dcv + sc.lokappa0;
-    const float det = cq * cd - dot * dot;
-    const float cvs = sc.cterm + sc.pownu0 * __logf(det) - pq - pd;
-    float cvm;
-    if (cvs <= sc.cvkey_first) cvm = sc.cvval_first;
-    else if (sc.cvkey_last <= cvs) cvm = sc.cvval_last;
-    else {
-        const int ix = min(max(sc.cvshift + (int)rintf(2.f * cvs), 0), sc.cvcard - 1);
-        cvm = cvtab[ix * CVREP + (lane & (CVREP - 1))];
-    }
-    cvm *= sc.cvswgt;
-    float ss = dss;
-    if (-99.f < ss) {
-        ss += hq * hd * 0.1111111f;
-        ss -= 0.05f;
-        ss *= sc.ssswgt;
+    const float s0 = fmaf(__log2f(daa), C2_LN2, -tc.shift);
+    const float det = fmaf(-dot, dot, cq * cd);
+    const float x = (fmaf(tc.p2l, __log2f(det), tc.c2) - pq2) - pd2;
+    const int ix = min(max(__float2int_rn(x), tc.ilo), tc.ihi);
+    float cvm = cvl[ix * P1T_CVREP];
+    if (!tc.uniform) {
+        cvm = (tc.kl2 <= x) ? tc.vlw : cvm;
+        cvm = (x <= tc.kf2) ? tc.vfw : cvm;
     }
     return s0 + (ss + cvm);
 }
 
 // Stage the column records of chunk m (32 columns) into the column ring
+// (3 chunks; chunks at slot 0 also into the mirror slots 96..127)
 __device__ __forceinline__ void stage_cols(float* cring, const float* __restrict__ cold, int m, int L, int lane)
 {
     const int c0 = 32 * m;
     const int nc = min(32, L - c0);
     if (nc > 0) {
-        float* dst = cring + (c0 & (P1T_CRING - 1)) * P1C_TRS;
+        const int base = c0 % P1T_CMOD;
+        float* dst = cring + base * P1C_TRS;
         const float* src = cold + (long long)c0 * P1C_TRS;
         for (int i = lane; i < nc * (P1C_TRS / 4); i += 32) cp_async16(dst + 4 * i, src + 4 * i);
+        if (base == 0) {
+            float* mir = cring + P1T_CMOD * P1C_TRS;
+            for (int i = lane; i < nc * (P1C_TRS / 4); i += 32) cp_async16(mir + 4 * i, src + 4 * i);
+        }
     }
     cp_async_commit();
 }
@@ -998,20 +1130,28 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
     extern __shared__ float smem[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int cvcard = a.sc.cvcard;
-    float* cvtab = smem;                                      // [cvcard][P1T_CVREP]
+    float* cvtab = smem;                                      // [cvcard][P1T_CVREP], x CV weight
     float* wb = smem + cvcard * P1T_CVREP + wid * P1T_WARP_FLOATS;
-    float* ring = wb;                                         // [P1C_RING][P1T_RLD] scores
+    float* ring = wb;                                         // [64 anti-diagonals][P1T_RLD] scores
     float* cring = ring + P1C_RING * P1T_RLD;                 // [P1T_CRING][P1C_TRS] column records
     float* bnd = cring + P1T_CRING * P1C_TRS;                 // [32][8] row above the strip
     unsigned* btile = reinterpret_cast<unsigned*>(bnd + 32 * 8);   // [2][TC_TILE_WORDS] db operand tiles
     unsigned long long* tbar = reinterpret_cast<unsigned long long*>(btile + 2 * TC_TILE_WORDS);  // [2]
-    for (int i = threadIdx.x; i < cvcard * P1T_CVREP; i += blockDim.x) cvtab[i] = a.cvvals[i / P1T_CVREP];
+    for (int i = threadIdx.x; i < cvcard * P1T_CVREP; i += blockDim.x)
+        cvtab[i] = a.cvvals[i / P1T_CVREP] * a.sc.cvswgt;
+    __shared__ unsigned tmem_base;
     if (lane == 0) {
         mbar_init(tbar, 1);
         mbar_init(tbar + 1, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    // query CV / SS A fragments of the current strip live in TMEM (64 columns
+    // per warp; warps w, w + 4, w + 8 share lanes and take 128-column blocks)
+    if (wid == 0) tmem_alloc(&tmem_base, P1T_TMEM_COLS);
+    tmem_fence_before();
     __syncthreads();
+    tmem_fence_after();
+    const unsigned tq = tmem_base + ((unsigned)(32 * (wid & 3)) << 16) + (unsigned)((wid >> 2) * 128);
     unsigned tph0 = 0, tph1 = 0;   // phase parity of the two tile slots
 
     const long long slotw = (long long)blockIdx.x * P1T_WARPS + wid;
@@ -1019,8 +1159,10 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
     float* bot0 = a.bot + slotw * a.botstride;
     const int Lq = a.Lq;
     const int nstrips = (Lq + 31) >> 5;
-    const ScoreConsts sc = a.sc;
+    const TcConsts tc = a.tc;
     const int g = lane >> 2, q = lane & 3;
+    // this lane's CV table replica, offset so that index 0 is the table's key 0
+    const float* __restrict__ cvl = cvtab + a.sc.cvshift * P1T_CVREP + (lane & (P1T_CVREP - 1));
 
     for (;;) {
         int item = 0;
@@ -1074,8 +1216,25 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                     }
                 }
             }
-            // query row terms of this lane's fragment rows: 32 s + 16 mt + g + 8 h
-            float rq[2][2][3];
+            // this strip's query CV / SS fragments into TMEM: column 4 idx + w holds
+            // word w of fragment idx = ((mt * 2 + dot) * 2 + ktile) * 2 + split
+            {
+                const uint4* src = reinterpret_cast<const uint4*>(a.qa + (long long)s * TC_QA_WORDS) + lane;
+#pragma unroll
+                for (int blk = 0; blk < 4; blk++) {
+                    unsigned v[16];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const uint4 x = __ldg(src + (4 * blk + i) * 32);
+                        v[4 * i + 0] = x.x; v[4 * i + 1] = x.y; v[4 * i + 2] = x.z; v[4 * i + 3] = x.w;
+                    }
+                    tmem_st16(tq + 16 * blk, v);
+                }
+                tmem_wait_st();
+            }
+            // query row terms of this lane's fragment rows 32 s + 16 mt + g + 8 hh:
+            // cvnorm and twice the CV log prior
+            float rq[2][2][2];
 #pragma unroll
             for (int mt = 0; mt < 2; mt++)
 #pragma unroll
@@ -1083,24 +1242,23 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                     const int rr = s * 32 + 16 * mt + g + 8 * hh;
                     const float* qx = a.qrec + (long long)min(rr, Lq - 1) * QR_STRIDE;
                     rq[mt][hh][0] = qx[QR_CN];
-                    rq[mt][hh][1] = qx[QR_PRIOR];
-                    rq[mt][hh][2] = qx[QR_HQ];
+                    rq[mt][hh][1] = 2.f * qx[QR_PRIOR];
                 }
-            DPLane D;
+            WfLane D;
+            {
+                float q7[7];
 #pragma unroll
-            for (int i = 0; i < 7; i++) D.q7[i] = act ? qr[QR_TRN + i] : LOG0;
-            const bool z_left = (lane == 31);
-            const bool z_diag = (lane == 31 || lane == 0);
-            const St5 LB = z_left ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
-                                  : St5{0.f, qr[QR_C + 0], qr[QR_C + 1], qr[QR_C + 2], LOG0};
-            const St5 DB = z_diag ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
-                                  : St5{0.f, qr[QR_CP + 0], qr[QR_CP + 1], qr[QR_CP + 2], LOG0};
-            const int cA = (Lq <= r + edge) ? edge + r - Lq : -1;
-            const int cB = (r < edge) ? L - edge + r : 0x7fffffff;
-            D.mine = St5{0.f, 0.f, 0.f, 0.f, 0.f};
-            D.upp = D.mine;
-            D.best = 0.f;
-            D.kbest = 0;
+                for (int i = 0; i < 7; i++) q7[i] = act ? qr[QR_TRN + i] : LOG0;
+                const bool z_left = (lane == 31);
+                const bool z_diag = (lane == 31 || lane == 0);
+                const St5 LB = z_left ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
+                                      : St5{0.f, qr[QR_C + 0], qr[QR_C + 1], qr[QR_C + 2], LOG0};
+                const St5 DB = z_diag ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
+                                      : St5{0.f, qr[QR_CP + 0], qr[QR_CP + 1], qr[QR_CP + 2], LOG0};
+                wf_init(D, q7, LB, DB);
+            }
+            const int cA = corner_a(r, Lq, edge);
+            const int cB = corner_b(r, L, edge);
             float bc[5];
 #pragma unroll
             for (int f = 0; f < 5; f++) {
@@ -1119,7 +1277,6 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
             stage_cols(cring, cold, 1, L, lane);
             const int nch = (L + 31) >> 5;
             const int kend = L + 31;
-            const unsigned* __restrict__ qa = a.qa + (long long)s * TC_QA_WORDS;
             // db operand tiles T = 4m + nt stream through the two slots, two tiles ahead
             const int ntile = 4 * nch;
             if (lane == 0) {
@@ -1130,7 +1287,6 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                 if (m < nch) {
                     cp_async_wait_1();   // column records of chunk m have landed
                     __syncwarp();
-                    stage_cols(cring, cold, m + 2, L, lane);
                     // the next chunk's db operands (12 KB) towards L2 while this one is used
                     if (m + 1 < nch) {
                         const char* nx = reinterpret_cast<const char*>(tb0 + (long long)(4 * m + 4) * TC_TILE_WORDS);
@@ -1138,6 +1294,9 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                         for (int i = 0; i < 3; i++)
                             asm volatile("prefetch.global.L2 [%0];" ::"l"(nx + (i * 32 + lane) * 128));
                     }
+                    // does any row of the strip have corner cells in this chunk?
+                    const bool hasc = __any_sync(FULL, cA >= 32 * m || cB < 32 * m + 32);
+                    const float* cbase = cring + ((32 * m) % P1T_CMOD) * P1C_TRS;
                     // ---- score stage: 32 x 32 tile of chunk m on the tensor cores
 #pragma unroll 1
                     for (int nt = 0; nt < 4; nt++) {
@@ -1159,12 +1318,10 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                         if (lane == 0 && T + 2 < ntile)
                             bulk_load(btile + sl * TC_TILE_WORDS, tb0 + (long long)(T + 2) * TC_TILE_WORDS,
                                       TC_TILE_WORDS * 4, tbar + sl);
-                        const int c0 = 32 * m + 8 * nt + 2 * q;
-                        const float* cr0 = cring + (c0 & (P1T_CRING - 1)) * P1C_TRS;
-                        const float* cr1 = cring + ((c0 + 1) & (P1T_CRING - 1)) * P1C_TRS;
-                        const float cd[2] = {cr0[CO_CD], cr1[CO_CD]};
-                        const float pd[2] = {cr0[CO_PD], cr1[CO_PD]};
-                        const float hd[2] = {cr0[CO_HD], cr1[CO_HD]};
+                        const int cl = 8 * nt + 2 * q;   // column within the chunk
+                        const float* cr0 = cbase + cl * P1C_TRS;
+                        const float cd[2] = {cr0[CO_CD], cr0[P1C_TRS + CO_CD]};
+                        const float pd[2] = {cr0[CO_PD2], cr0[P1C_TRS + CO_PD2]};
 #pragma unroll
                         for (int mt = 0; mt < 2; mt++) {
                             float acc[3][4];
@@ -1178,29 +1335,33 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                                 mma_bf16(acc[0], Aaa[mt][kt][0], B[0][kt][1].x, B[0][kt][1].y);
                                 mma_bf16(acc[0], Aaa[mt][kt][0], B[0][kt][0].x, B[0][kt][0].y);
                             }
+                            unsigned Q[32];   // (dot, ktile, split) fragments of this m-tile
+                            tmem_ld32(tq + 32 * mt, Q);
 #pragma unroll
                             for (int d = 1; d < 3; d++)
 #pragma unroll
                                 for (int kt = 0; kt < 2; kt++) {
-                                    const uint4* ap = reinterpret_cast<const uint4*>(
-                                        qa + ((((mt * 2 + (d - 1)) * 2 + kt) * 2) * 32 + lane) * 4);
-                                    const uint4 ah = __ldg(ap), al = __ldg(ap + 32);
-                                    const unsigned Ah[4] = {ah.x, ah.y, ah.z, ah.w};
-                                    const unsigned Al[4] = {al.x, al.y, al.z, al.w};
+                                    const unsigned* Ah = Q + (((d - 1) * 2 + kt) * 2 + 0) * 4;
+                                    const unsigned* Al = Q + (((d - 1) * 2 + kt) * 2 + 1) * 4;
                                     mma_bf16(acc[d], Al, B[d][kt][0].x, B[d][kt][0].y);
                                     mma_bf16(acc[d], Ah, B[d][kt][1].x, B[d][kt][1].y);
                                     mma_bf16(acc[d], Ah, B[d][kt][0].x, B[d][kt][0].y);
                                 }
-                            // epilogue: cell (row 16 mt + g + 8 hh, column c0 + e) is register 2 hh + e
+                            // epilogue: cell (row 16 mt + g + 8 hh, column 32 m + cl + e) is
+                            // register 2 hh + e; its score goes to anti-diagonal row + column
 #pragma unroll
                             for (int hh = 0; hh < 2; hh++)
 #pragma unroll
                                 for (int e = 0; e < 2; e++) {
                                     const int i = 2 * hh + e;
-                                    const float S = tc_epilogue<P1T_CVREP>(acc[0][i], acc[1][i], acc[2][i],
-                                                                           rq[mt][hh][0], rq[mt][hh][1], rq[mt][hh][2],
-                                                                           cd[e], pd[e], hd[e], cvtab, sc, lane);
-                                    ring[((c0 + e) & (P1C_RING - 1)) * P1T_RLD + 16 * mt + g + 8 * hh] = S;
+                                    const int row = 16 * mt + g + 8 * hh;
+                                    float S = tc_cell(acc[0][i], acc[1][i], acc[2][i], rq[mt][hh][0], rq[mt][hh][1],
+                                                      cd[e], pd[e], cvl, tc);
+                                    if (hasc) {
+                                        const int rr = 32 * s + row, cc = 32 * m + cl + e;
+                                        if (cc <= corner_a(rr, Lq, edge) || cc >= corner_b(rr, L, edge)) S = -9.f;
+                                    }
+                                    ring[((cl + e + row) ^ ((m & 1) << 5)) * P1T_RLD + row] = S;   // (32 m + cl + e + row) & 63
                                 }
                         }
                     }
@@ -1208,12 +1369,12 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                 __syncwarp();
                 // ---- DP stage: wavefront steps [32m, 32m + 32)
                 const int k0 = 32 * m, k1 = min(k0 + 32, kend);
+                const float* tcol = cring + ((k0 - lane + P1T_CMOD) % P1T_CMOD) * P1C_TRS;
                 if (m >= 1 && k0 + 31 < L && k1 == k0 + 32)
-                    p1c_steps<false, P1T_RLD, P1T_CRING - 1>(D, k0, k1, lane, L, act, cA, cB, ring, cring, bnd, LB,
-                                                             DB, wr_bot, botw, Lmax);
+                    wf_steps<false, P1T_RLD, true, 0>(D, k0, 32, lane, L, act, ring, tcol, bnd, wr_bot, botw, Lmax);
                 else
-                    p1c_steps<true, P1T_RLD, P1T_CRING - 1>(D, k0, k1, lane, L, act, cA, cB, ring, cring, bnd, LB,
-                                                            DB, wr_bot, botw, Lmax);
+                    wf_steps<true, P1T_RLD, true, 0>(D, k0, k1 - k0, lane, L, act, ring, tcol, bnd, wr_bot, botw,
+                                                     Lmax);
                 __syncwarp();
                 *reinterpret_cast<float4*>(bnd + lane * 8) = make_float4(D.bnxt[0], D.bnxt[1], D.bnxt[2], D.bnxt[3]);
                 bnd[lane * 8 + 4] = D.bnxt[4];
@@ -1222,6 +1383,8 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                     const int cc = k0 + 64 + lane;
                     D.bnxt[f] = (s > 0 && cc < L) ? botr[f * Lmax + cc] : 0.f;
                 }
+                // chunk m - 1's records are no longer read: chunk m + 2 into its slots
+                stage_cols(cring, cold, m + 2, L, lane);
                 __syncwarp();
             }
             cp_async_wait_all();
@@ -1251,6 +1414,13 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
             a.coords[p] = xy;
         }
         __syncwarp();
+    }
+    // every warp is past its last TMEM access: the allocating warp frees it
+    tmem_fence_before();
+    __syncthreads();
+    if (wid == 0) {
+        tmem_fence_after();
+        tmem_dealloc(tmem_base, P1T_TMEM_COLS);
     }
 }
 
@@ -1358,10 +1528,10 @@ int p1t_blocks_per_sm(int cvcard, cudaError_t* err)
 }
 
 cudaError_t launch_tc_pack(const float* drec, const long long* poff, const int* plen, const long long* ttile,
-                           int nprof, unsigned* tcdb, float* cold, cudaStream_t st)
+                           int nprof, unsigned* tcdb, float* cold, float lok, float wss, cudaStream_t st)
 {
     if (nprof <= 0) return cudaSuccess;
-    tc_pack_kernel<<<nprof, 128, 0, st>>>(drec, poff, plen, ttile, tcdb, cold);
+    tc_pack_kernel<<<nprof, 128, 0, st>>>(drec, poff, plen, ttile, tcdb, cold, lok, wss);
     return cudaGetLastError();
 }
 
