@@ -124,6 +124,7 @@ struct c2_handle {
     DevBuf<long long> d_ttile;
     DevBuf<float> d_cold, d_qaaf;
     DevBuf<int> d_prog;
+    size_t bnd_half = 0, prog_half = 0;   // floats / words of one sweep's strip-pipeline scratch
     DevBuf<float> d_fscore;
     DevBuf<int> d_fpsts, d_fpassed;
     DevBuf<unsigned> d_fbeg, d_fend;
@@ -139,7 +140,7 @@ struct c2_handle {
     int nmap = 0;
     std::vector<int> h_mapcand, h_mappass;
     DevBuf<int> d_mapcand, d_mappass, d_alninfo;
-    DevBuf<float> d_fb, d_pairf;
+    DevBuf<float> d_fb, d_bb, d_pairf;
     DevBuf<unsigned> d_pairc;
     DevBuf<unsigned long long> d_pairk;
     DevBuf<char> d_aln;
@@ -842,11 +843,13 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     *ncand = h->ncand;
     if (h->ncand == 0) return C2_OK;
     const int nc = h->ncand;
+    // strip-pipeline scratch: two halves, the second for the MAP backward sweep
+    h->bnd_half = (size_t)(acc / h->Lq) * 10;
+    h->prog_half = (size_t)nc * ((h->Lq + 31) / 32);
     if (h->d_cand_prof.ensure(nc) || h->d_cand_off.ensure(nc) || h->d_btck.ensure((size_t)acc) ||
         h->d_smat.ensure((size_t)acc) || h->d_mmat.ensure((size_t)acc) || h->d_fscore.ensure(nc) || h->d_fpsts.ensure(nc) ||
         h->d_fpassed.ensure(nc) || h->d_fbeg.ensure(nc) || h->d_fend.ensure(nc) ||
-        h->d_bnd.ensure((size_t)(acc / h->Lq) * 10) || h->d_tbkey.ensure(nc) ||
-        h->d_prog.ensure((size_t)nc * ((h->Lq + 31) / 32)))
+        h->d_bnd.ensure(2 * h->bnd_half) || h->d_tbkey.ensure(nc) || h->d_prog.ensure(2 * h->prog_half))
         return fail(h, C2_ERR_NOMEM, "finalisation scratch for %d pairs (%lld cells) failed", nc, acc);
     CK(cudaMemcpyAsync(h->d_cand_prof.p, h->h_cand.data(), (size_t)nc * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_cand_off.p, h->h_cand_off.data(), (size_t)nc * 8, cudaMemcpyHostToDevice, h->stream));
@@ -1045,7 +1048,8 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
     (void)cells;
     h->alnstride = h->Lq + h->Lmax + 1;
     size_t fbn = h->d_smat.n;   // same layout as the candidates' score matrices
-    if (h->d_mapcand.ensure(nm) || h->d_mappass.ensure(nm) || h->d_fb.ensure(fbn) || h->d_pairf.ensure((size_t)nm * 4) ||
+    if (h->d_mapcand.ensure(nm) || h->d_mappass.ensure(nm) || h->d_fb.ensure(fbn) || h->d_bb.ensure(fbn) ||
+        h->d_pairf.ensure((size_t)nm * 4) ||
         h->d_pairc.ensure(nm) || h->d_alninfo.ensure((size_t)nm * 8) || h->d_aln.ensure((size_t)nm * 5 * h->alnstride) ||
         h->d_pairk.ensure(nm))
         return fail(h, C2_ERR_NOMEM, "MAP buffers for %d pairs failed", nm);
@@ -1073,11 +1077,14 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
     a.mmat = h->d_mmat.p;
     a.stats = h->d_stats.p;
     a.fb = h->d_fb.p;
+    a.bb = h->d_bb.p;
     a.btck = h->d_btck.p;
     a.pairf = h->d_pairf.p;
     a.pairc = h->d_pairc.p;
     a.bnd = h->d_bnd.p;
     a.prog = h->d_prog.p;
+    a.bnd_b = h->d_bnd.p + h->bnd_half;   // the backward sweep's halves of the scratch
+    a.prog_b = h->d_prog.p + h->prog_half;
     a.pairk = h->d_pairk.p;
     a.items = h->d_mapitems.p;
     a.status = h->d_status.p;

@@ -182,28 +182,15 @@ __device__ __forceinline__ void pf_scores(const MapArgs& a, const MapPair& P, in
 // ---------------------------------------------------------------------------
 // forward sweep: F for every cell; F.MM stored column-major in fb.  Work
 // items are (pair, strip); see the strip pipeline in c2_device.cuh.
-__global__ void __launch_bounds__(MAPW * 32) map_fwd_kernel(MapArgs a, const float* __restrict__ qtrn,
-                                                      const float* __restrict__ dtrn,
-                                                      const float* __restrict__ qcf)
+__device__ __forceinline__ void map_fwd_item(const MapArgs& a, const float* __restrict__ qtrn,
+                                             const float* __restrict__ dtrn, const float* __restrict__ qcf, int m,
+                                             int s, int lane, float (*rin)[33], float (*rout)[33], float* trs,
+                                             bool& broken)
 {
-    __shared__ float rings[MAPW][2][32][33];
-    __shared__ __align__(16) float trings[MAPW][64 * MTRS];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    float(*rin)[33] = rings[wid][0];
-    float(*rout)[33] = rings[wid][1];
-    float* trs = trings[wid];
     const int Lq = a.Lq;
     const int nstrips = (Lq + 31) >> 5;
-    const int nitems = a.nmap * nstrips;
     const S5 INIT = {0.f, MLOG0, MLOG0, MLOG0, MLOG0};
-    bool broken = false;
-    for (;;) {
-        int item = 0;
-        if (lane == 0) item = atomicAdd(a.counter, 1);
-        item = __shfl_sync(FULL, item, 0);
-        if (item >= nitems) break;
-        const int iv = a.items[item];
-        const int m = iv / nstrips, s = iv - m * nstrips;
+    {
         const MapPair P = map_pair(a, qtrn, m);
         const int L = P.L;
         const float* __restrict__ dt0 = dtrn + P.toff;
@@ -345,31 +332,18 @@ __global__ void __launch_bounds__(256) map_z_kernel(MapArgs a)
 // ---------------------------------------------------------------------------
 // backward sweep on the mirrored matrix (row Lq-1-r', column L-1-j'); adds
 // B.MM to fb, giving F+B per cell.  Work items are (pair, mirrored strip).
-__global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const float* __restrict__ qtrn,
-                                                      const float* __restrict__ dtrn)
+__device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __restrict__ qtrn,
+                                             const float* __restrict__ dtrn, int m, int s, int lane,
+                                             float (*rin)[33], float (*rout)[33], float* trs, bool& broken)
 {
-    __shared__ float rings[MAPW][2][32][33];
-    __shared__ __align__(16) float trings[MAPW][64 * MTRS];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    float(*rin)[33] = rings[wid][0];
-    float(*rout)[33] = rings[wid][1];
-    float* trs = trings[wid];
     const int Lq = a.Lq;
     const int nstrips = (Lq + 31) >> 5;
-    const int nitems = a.nmap * nstrips;
     const S5 INIT = {0.f, MLOG0, MLOG0, MLOG0, MLOG0};
-    bool broken = false;
-    for (;;) {
-        int item = 0;
-        if (lane == 0) item = atomicAdd(a.counter, 1);
-        item = __shfl_sync(FULL, item, 0);
-        if (item >= nitems) break;
-        const int iv = a.items[item];
-        const int m = iv / nstrips, s = iv - m * nstrips;
+    {
         const MapPair P = map_pair(a, qtrn, m);
         const int L = P.L;
         const float* __restrict__ dt0 = dtrn + P.toff;
-        float* fb = a.fb + P.base;
+        float* bb = a.bb + P.base;
         // column transitions: chunk 0 into the ring, chunk 1 into registers
         float tnx[7];
         {
@@ -380,10 +354,10 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
             map_trn_col<true>(dt0, 32 + lane, L, tnx);
             __syncwarp();
         }
-        float* bnd = a.bnd + (P.base / Lq) * 10;
+        float* bnd = a.bnd_b + (P.base / Lq) * 10;
         const float* botr = bnd + ((s + 1) & 1) * 5 * L;   // last row of mirrored strip s-1
         float* botw = bnd + (s & 1) * 5 * L;
-        int* pf = a.prog + (long long)m * nstrips;
+        int* pf = a.prog_b + (long long)m * nstrips;
         {
             const int rm = s * 32 + lane;       // mirrored row
             const int r = Lq - 1 - rm;          // actual row
@@ -404,17 +378,14 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
             }
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             const bool hasdn = act && r + 1 < Lq;
-            // loads of mirrored column k (diagonal-successor score, transitions,
-            // and the F value to add B to) are issued one step ahead
-            // (from L2: each chunk's columns are prefetched a chunk earlier; the
-            // strip's actual rows are [Lq - 32 s - 32, Lq - 32 s), successors one below)
+            // the diagonal-successor score of mirrored column k is loaded one step
+            // ahead, from L2: each chunk's columns are prefetched a chunk earlier
+            // (the strip's actual rows are [Lq - 32 s - 32, Lq - 32 s), successors
+            // one below)
             const int arow0 = Lq - 32 * s - 32;
             pf_scores<true>(a, P, 0, Lq, arow0 + 1, lane);
             pf_scores<true>(a, P, 32, Lq, arow0 + 1, lane);
-            pf_cols(fb, L - 1 - lane, L, Lq, arow0);
-            pf_cols(fb, L - 33 - lane, L, Lq, arow0);
             float nsc = hasdn ? map_score(a, P, (long long)(L - 1) * Lq + r + 1) : MLOG0;
-            float nfb = act ? fb[(long long)(L - 1) * Lq + r] : 0.f;
             for (int k = 0; k < L + 31; k++) {
                 const int j = k - lane;         // mirrored column
                 // diagonal-successor score of column j, read before this step's
@@ -470,21 +441,46 @@ __global__ void __launch_bounds__(MAPW * 32) map_bwd_kernel(MapArgs a, const flo
                 mine = nw;
                 upp = dn;
                 const int cfl = k - 31;
-                if (cfl >= 0 && cfl < L && act) {
-                    fb[(long long)(L - 1 - cfl) * Lq + r] = nfb + rout[cfl & 31][lane];
-                    if (cfl + 1 < L) nfb = fb[(long long)(L - 2 - cfl) * Lq + r];
-                }
+                if (cfl >= 0 && cfl < L && act) bb[(long long)(L - 1 - cfl) * Lq + r] = rout[cfl & 31][lane];
                 if ((k & 31) == 31) {
                     // mirrored columns of chunk k / 32 + 1 into the ring, the next chunk into registers
                     __syncwarp();
                     map_trn_store(trs, k + 1 + lane, tnx);
                     map_trn_col<true>(dt0, k + 33 + lane, L, tnx);
                     pf_scores<true>(a, P, k + 33, Lq, arow0 + 1, lane);
-                    pf_cols(fb, L - 1 - (k + 33 + lane), L, Lq, arow0);
                 }
                 __syncwarp();
             }
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Forward and backward sweeps in one launch: the two are independent (the
+// backward sweep writes B beside F), so their strip chains run side by side;
+// item 2 i is the forward sweep's work item i, 2 i + 1 the backward one's.
+__global__ void __launch_bounds__(MAPW * 32) map_fb_kernel(MapArgs a, const float* __restrict__ qtrn,
+                                                     const float* __restrict__ dtrn, const float* __restrict__ qcf)
+{
+    __shared__ float rings[MAPW][2][32][33];
+    __shared__ __align__(16) float trings[MAPW][64 * MTRS];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nstrips = (a.Lq + 31) >> 5;
+    const int nitems = 2 * a.nmap * nstrips;
+    bool broken = false;
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.counter, 1);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= nitems) break;
+        const int iv = a.items[item >> 1];
+        const int m = iv / nstrips, s = iv - m * nstrips;
+        __syncwarp();
+        if (item & 1)
+            map_bwd_item(a, qtrn, dtrn, m, s, lane, rings[wid][0], rings[wid][1], trings[wid], broken);
+        else
+            map_fwd_item(a, qtrn, dtrn, qcf, m, s, lane, rings[wid][0], rings[wid][1], trings[wid], broken);
+        __syncwarp();
     }
 }
 
@@ -523,6 +519,7 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
         const int L = a.plen[p];
         const long long base = a.cand_off[c];
         const float* fb = a.fb + base;
+        const float* bb = a.bb + base;
         signed char* bt = a.btck + base;
         const float logZ = a.pairf[m * 4 + 1];
         const int edge = corner_edge_m(Lq, L);
@@ -540,15 +537,17 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
             float bcur = (s > 0 && lane < L) ? __ldcg(botr + lane) : 0.f;
             float bnxt = (s > 0 && 32 + lane < L) ? __ldcg(botr + 32 + lane) : 0.f;
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
-            // column k is loaded one step ahead, from L2: each chunk's columns are
-            // prefetched a chunk earlier
+            // F + B of column k is loaded one step ahead, from L2: each chunk's
+            // columns are prefetched a chunk earlier
             pf_cols(fb, lane, L, Lq, s * 32);
             pf_cols(fb, 32 + lane, L, Lq, s * 32);
-            float nfb = act ? fb[r] : 0.f;
+            pf_cols(bb, lane, L, Lq, s * 32);
+            pf_cols(bb, 32 + lane, L, Lq, s * 32);
+            float nfb = act ? fb[r] + bb[r] : 0.f;
             for (int k = 0; k < L + 31; k++) {
                 if (k < L) {
                     rin[k & 31][lane] = nfb;
-                    if (k + 1 < L) nfb = act ? fb[(long long)(k + 1) * Lq + r] : 0.f;
+                    if (k + 1 < L) nfb = act ? fb[(long long)(k + 1) * Lq + r] + bb[(long long)(k + 1) * Lq + r] : 0.f;
                 }
                 float up = __shfl_up_sync(FULL, mine, 1);
                 {
@@ -561,6 +560,7 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
                         const int cc = k + 33 + lane;
                         bnxt = (s > 0 && cc < L) ? __ldcg(botr + cc) : 0.f;
                         pf_cols(fb, cc, L, Lq, s * 32);
+                        pf_cols(bb, cc, L, Lq, s * 32);
                     }
                 }
                 __syncwarp();
@@ -703,14 +703,14 @@ cudaError_t launch_map(const MapArgs& a, const float* qtrn, const float* dtrn, c
     if ((e = cudaMemsetAsync(a.pairf, 0, (size_t)a.nmap * 4 * sizeof(float), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(a.pairk, 0, (size_t)a.nmap * sizeof(unsigned long long), st)) != cudaSuccess) return e;
     if ((e = reset()) != cudaSuccess) return e;
-    map_fwd_kernel<<<g, MAPW * 32, 0, st>>>(a, qtrn, dtrn, qcf);
+    if ((e = cudaMemsetAsync(a.prog_b, 0, progb, st)) != cudaSuccess) return e;
+    const int gfb = (int)std::min<long long>(grid, (2 * nitems + MAPW - 1) / MAPW);
+    map_fb_kernel<<<gfb, MAPW * 32, 0, st>>>(a, qtrn, dtrn, qcf);
     map_z_kernel<<<(a.nmap + 7) / 8, 256, 0, st>>>(a);
-    if ((e = reset()) != cudaSuccess) return e;
-    map_bwd_kernel<<<g, MAPW * 32, 0, st>>>(a, qtrn, dtrn);
     if ((e = reset()) != cudaSuccess) return e;
     map_dp_kernel<<<g, MAPW * 32, 0, st>>>(a);
     map_tb_kernel<<<(a.nmap + 31) / 32, 32, 0, st>>>(a);
-    *nlaunch += 5;
+    *nlaunch += 4;
     return cudaGetLastError();
 }
 

@@ -48,12 +48,15 @@ struct MapArgs {
     const float* smat;          // [L][Lq] per candidate
     const float* mmat;          // [L][Lq] per candidate (modular scores)
     const float* stats;         // [npass][STATS_NOUT]
-    float* fb;                  // [L][Lq] per candidate: F, then F+B
+    float* fb;                  // [L][Lq] per candidate: F (MAP.MM forward values)
+    float* bb;                  // [L][Lq] per candidate: B (backward values)
     signed char* btck;          // [L][Lq] per candidate: MAP traceback codes
     float* pairf;               // [nmap][4]: maxF, logZ, map max, (unused)
     unsigned* pairc;            // [nmap]: MAP end coordinates
     float* bnd;                 // per candidate at 10 x (cand_off / Lq): two last-row buffers [5][L]
     int* prog;                  // [ncand][nstrips] finished columns per strip
+    float* bnd_b;               // backward sweep's strip-boundary rows (same layout as bnd)
+    int* prog_b;                // backward sweep's strip progress (same layout as prog)
     const int* items;           // work item -> m * nstrips + strip (ready-time order)
     unsigned long long* pairk;  // [nmap] MAP DP maximum and end cell, packed for atomicMax
     int* status;
