@@ -374,18 +374,24 @@ static inline void trn_of(const c2_profiles* d, int k, int i, float* t7)
     t7[TIM] = a[3]; t7[TII] = b[4]; t7[TDM] = a[5]; t7[TDD] = a[6];
 }
 
+// Wavefront steps by which a strip trails the one above in the sweeps' strip
+// pipeline: a strip starts a chunk once the strip above has published the
+// chunk's 32 columns, which lane 31 of that strip finishes 31 steps after
+// its lane 0.
+constexpr int STRIP_LAG = 64;
+
 // Work-item table of a strip-pipelined sweep over np pairs (in processing
 // order, lengths lens): item (p, s) at key p + K s, K = pairs started per
 // strip lag when nwarps warps are busy, so that strip s of a pair is handed
-// out about when strip s - 1 is far enough ahead (a strip needs 64 columns
-// of its predecessor, which lags ~96 wavefront steps).  Ties keep s order, so
+// out about when strip s - 1 is far enough ahead.  Ties keep s order, so
 // (p, s - 1) always precedes (p, s).
+
 static void strip_items(const std::vector<int>& lens, int nstrips, int nwarps, std::vector<int>& items)
 {
     const int np = (int)lens.size();
     double lm = 31.0;
     for (int L : lens) lm += (double)L / std::max(1, np);
-    const double K = 96.0 * nwarps / (nstrips * lm);
+    const double K = (double)STRIP_LAG * nwarps / (nstrips * lm);
     std::vector<std::pair<double, int>> key((size_t)np * nstrips);
     for (int p = 0; p < np; p++)
         for (int s = 0; s < nstrips; s++) key[(size_t)p * nstrips + s] = {p + K * s, p * nstrips + s};

@@ -435,18 +435,13 @@ p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
             float t7[7];
 #pragma unroll
             for (int i = 0; i < 7; i++) t7[i] = LOG0;
-            // strip-boundary prefetch: lane i holds column c0 + i of the row above
-            float bcur[5], bnxt[5];
-            if (s > 0) pipe_wait(pf + s - 1, min(64, L), lane, a.status, broken);
+            // row above the strip, one chunk at a time: lane i holds column 32 c + i
+            // (each chunk is waited for and loaded at the end of the one before,
+            // so a strip trails the one above by 63 wavefront steps)
+            float bcur[5];
+            if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken);
 #pragma unroll
-            for (int f = 0; f < 5; f++) {
-                bcur[f] = 0.f;
-                bnxt[f] = 0.f;
-                if (s > 0) {
-                    if (lane < L) bcur[f] = __ldcg(botr + f * L + lane);
-                    if (32 + lane < L) bnxt[f] = __ldcg(botr + f * L + 32 + lane);
-                }
-            }
+            for (int f = 0; f < 5; f++) bcur[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : 0.f;
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             const int nsteps = L + 31;
             // db column records are staged into shared memory one chunk ahead
@@ -502,12 +497,11 @@ p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
                     const float b4 = __shfl_sync(FULL, bcur[4], src);
                     if (lane == 0) up = St5{b0, b1, b2, b3, b4};
                     if (src == 31) {
-                        if (s > 0 && k + 33 < L) pipe_wait(pf + s - 1, min(k + 65, L), lane, a.status, broken);
+                        if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken);
 #pragma unroll
                         for (int f = 0; f < 5; f++) {
-                            bcur[f] = bnxt[f];
-                            const int c = k + 33 + lane;
-                            bnxt[f] = (s > 0 && c < L) ? __ldcg(botr + f * L + c) : 0.f;
+                            const int c = k + 1 + lane;
+                            bcur[f] = (s > 0 && c < L) ? __ldcg(botr + f * L + c) : 0.f;
                         }
                     }
                 }

@@ -223,14 +223,13 @@ __device__ __forceinline__ void map_fwd_item(const MapArgs& a, const float* __re
             float t7[7];
 #pragma unroll
             for (int i = 0; i < 7; i++) t7[i] = MLOG0;
-            float bcur[5], bnxt[5];
+            // row above the strip, one chunk at a time (lane i: column 32 c + i),
+            // waited for and loaded at the end of the chunk before
+            float bcur[5];
             const float binit[5] = {0.f, MLOG0, MLOG0, MLOG0, MLOG0};
-            if (s > 0) pipe_wait(pf + s - 1, min(64, L), lane, a.status, broken);
+            if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken);
 #pragma unroll
-            for (int f = 0; f < 5; f++) {
-                bcur[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : binit[f];
-                bnxt[f] = (s > 0 && 32 + lane < L) ? __ldcg(botr + f * L + 32 + lane) : binit[f];
-            }
+            for (int f = 0; f < 5; f++) bcur[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : binit[f];
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             // column k's score is loaded one step ahead, from L2: each chunk's
             // columns are prefetched a chunk earlier
@@ -256,12 +255,11 @@ __device__ __forceinline__ void map_fwd_item(const MapArgs& a, const float* __re
                     const float b4 = __shfl_sync(FULL, bcur[4], src);
                     if (lane == 0) up = S5{b0, b1, b2, b3, b4};
                     if (src == 31) {
-                        if (s > 0 && k + 33 < L) pipe_wait(pf + s - 1, min(k + 65, L), lane, a.status, broken);
+                        if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken);
 #pragma unroll
                         for (int f = 0; f < 5; f++) {
-                            bcur[f] = bnxt[f];
-                            const int cc = k + 33 + lane;
-                            bnxt[f] = (s > 0 && cc < L) ? __ldcg(botr + f * L + cc) : binit[f];
+                            const int cc = k + 1 + lane;
+                            bcur[f] = (s > 0 && cc < L) ? __ldcg(botr + f * L + cc) : binit[f];
                         }
                     }
                 }
@@ -368,14 +366,13 @@ __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __re
             float t7[7];
 #pragma unroll
             for (int i = 0; i < 7; i++) t7[i] = MLOG0;
-            float bcur[5], bnxt[5];
+            // row above the strip, one chunk at a time (lane i: column 32 c + i),
+            // waited for and loaded at the end of the chunk before
+            float bcur[5];
             const float binit[5] = {0.f, MLOG0, MLOG0, MLOG0, MLOG0};
-            if (s > 0) pipe_wait(pf + s - 1, min(64, L), lane, a.status, broken);
+            if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken);
 #pragma unroll
-            for (int f = 0; f < 5; f++) {
-                bcur[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : binit[f];
-                bnxt[f] = (s > 0 && 32 + lane < L) ? __ldcg(botr + f * L + 32 + lane) : binit[f];
-            }
+            for (int f = 0; f < 5; f++) bcur[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : binit[f];
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             const bool hasdn = act && r + 1 < Lq;
             // the diagonal-successor score of mirrored column k is loaded one step
@@ -413,12 +410,11 @@ __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __re
                     const float b4 = __shfl_sync(FULL, bcur[4], src);
                     if (lane == 0) dn = S5{b0, b1, b2, b3, b4};
                     if (src == 31) {
-                        if (s > 0 && k + 33 < L) pipe_wait(pf + s - 1, min(k + 65, L), lane, a.status, broken);
+                        if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken);
 #pragma unroll
                         for (int f = 0; f < 5; f++) {
-                            bcur[f] = bnxt[f];
-                            const int cc = k + 33 + lane;
-                            bnxt[f] = (s > 0 && cc < L) ? __ldcg(botr + f * L + cc) : binit[f];
+                            const int cc = k + 1 + lane;
+                            bcur[f] = (s > 0 && cc < L) ? __ldcg(botr + f * L + cc) : binit[f];
                         }
                     }
                 }
@@ -533,9 +529,9 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
             const int r = s * 32 + lane;
             const bool act = r < Lq;
             float mine = 0.f, upp = 0.f;
-            if (s > 0) pipe_wait(pf + s - 1, min(64, L), lane, a.status, broken);
+            // row above the strip, one chunk at a time (lane i: column 32 c + i)
+            if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken);
             float bcur = (s > 0 && lane < L) ? __ldcg(botr + lane) : 0.f;
-            float bnxt = (s > 0 && 32 + lane < L) ? __ldcg(botr + 32 + lane) : 0.f;
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             // F + B of column k is loaded one step ahead, from L2: each chunk's
             // columns are prefetched a chunk earlier
@@ -555,12 +551,10 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
                     const float b0 = __shfl_sync(FULL, bcur, src);
                     if (lane == 0) up = b0;
                     if (src == 31) {
-                        if (s > 0 && k + 33 < L) pipe_wait(pf + s - 1, min(k + 65, L), lane, a.status, broken);
-                        bcur = bnxt;
-                        const int cc = k + 33 + lane;
-                        bnxt = (s > 0 && cc < L) ? __ldcg(botr + cc) : 0.f;
-                        pf_cols(fb, cc, L, Lq, s * 32);
-                        pf_cols(bb, cc, L, Lq, s * 32);
+                        if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken);
+                        bcur = (s > 0 && k + 1 + lane < L) ? __ldcg(botr + k + 1 + lane) : 0.f;
+                        pf_cols(fb, k + 33 + lane, L, Lq, s * 32);
+                        pf_cols(bb, k + 33 + lane, L, Lq, s * 32);
                     }
                 }
                 __syncwarp();
