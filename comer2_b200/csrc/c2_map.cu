@@ -312,19 +312,27 @@ __device__ __forceinline__ void map_fwd_item(const MapArgs& a, const float* __re
 // (src/libmycu/cumapdp/CuBatchMAPDP_bwd.cuh:185-290)
 __global__ void __launch_bounds__(256) map_z_kernel(MapArgs a)
 {
-    const int lane = threadIdx.x & 31;
-    const int m = blockIdx.x * 8 + (threadIdx.x >> 5);
-    if (m >= a.nmap) return;
+    // one CTA per pair: per-thread partial sums over a strided range of the
+    // pair's cells, then a CTA reduction
+    __shared__ float part[8];
+    const int m = blockIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int c = a.map_cand[m];
     const int p = a.cand_prof[c];
     const long long n = (long long)a.Lq * a.plen[p];
     const float* fb = a.fb + a.cand_off[c];
     const float maxF = a.pairf[m * 4 + 0];
     float s = 0.f;
-    for (long long k = lane; k < n; k += 32) s += fexp(fb[k] - maxF);
+    for (long long k = threadIdx.x; k < n; k += 256) s += fexp(fb[k] - maxF);
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
-    if (lane == 0) a.pairf[m * 4 + 1] = flog(s) + maxF;
+    if (lane == 0) part[wid] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < 8; w++) t += part[w];
+        a.pairf[m * 4 + 1] = flog(t) + maxF;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -607,16 +615,27 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
 }
 
 // ---------------------------------------------------------------------------
-// traceback into alignment strings, one thread per pair
+// traceback into alignment strings, one warp per pair
 // (src/libmycu/cumapdp/CuBatchMAPDP_map_final.cu:175-330)
-__global__ void map_tb_kernel(MapArgs a)
+constexpr int TBW = 4;   // warps per CTA of the MAP traceback
+
+__global__ void __launch_bounds__(TBW * 32) map_tb_kernel(MapArgs a)
 {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= a.nmap) return;
+    // one warp per pair.  The walk from the MAP maximum towards the origin
+    // moves by one row and/or column per step; the warp stages 32 x 32 windows
+    // of the traceback codes and scores (columns x0 - 31 .. x0, rows
+    // y0 - 31 .. y0) and the letters of those rows and columns in shared
+    // memory, lane 0 walks inside the window, and the warp restages where the
+    // walk leaves it.
+    __shared__ signed char wbt[TBW][32][33];
+    __shared__ float wsm[TBW][32][33];
+    __shared__ unsigned char wq[TBW][2][32], wd[TBW][2][32];   // [residue, SS][offset]
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int m = blockIdx.x * TBW + wid;
+    if (m >= a.nmap) return;   // whole warp
     const int Lq = a.Lq;
     const int c = a.map_cand[m];
     const int p = a.cand_prof[c];
-    const int L = a.plen[p];
     const long long off = a.poff[p];
     const long long base = a.cand_off[c];
     const signed char* bt = a.btck + base;
@@ -626,55 +645,95 @@ __global__ void map_tb_kernel(MapArgs a)
     const float mbest = __uint_as_float((unsigned)(key >> 32));
     const unsigned cell = 0xffffffffu - (unsigned)(key & 0xffffffffu);
     const unsigned xx = (key != 0ull) ? (((cell & 0xffffu) << 16) | (cell >> 16)) : 0u;
-    a.pairf[m * 4 + 2] = mbest;
-    a.pairc[m] = xx;
+    if (lane == 0) {
+        a.pairf[m * 4 + 2] = mbest;
+        a.pairc[m] = xx;
+    }
     int x = (int)(xx >> 16), y = (int)(xx & 0xffff);
     char* o = a.aln + (size_t)m * 5 * a.alnstride;
     char *tq = o, *tm = o + a.alnstride, *tt = o + 2 * a.alnstride, *sq = o + 3 * a.alnstride,
          *st = o + 4 * a.alnstride;
     int n = 0, idts = 0, psts = 0, gaps = 0;
     const int cap = a.alnstride - 1;
-    while (n < cap) {
-        if (x < 0 || y < 0) break;
-        const long long k = (long long)x * Lq + y;
-        const int b = bt[k];
-        if (b == BT_STOP) break;
-        sq[n] = ' ';
-        st[n] = ' ';
-        if (b == BT_UP) {
-            gaps++;
-            tq[n] = (char)a.qaa[y]; tt[n] = '-'; tm[n] = ' ';
-            if (a.qss) sq[n] = (char)a.qss[y];
-            n++; y--;
-            continue;
+    int done = 0;
+    while (!done && n < cap && x >= 0 && y >= 0) {
+        const int x0 = x, y0 = y;
+        {
+            const int cx = x0 - lane, qy = y0 - lane;
+#pragma unroll 4
+            for (int r = 0; r < 32; r++) {
+                const int ry = y0 - r;
+                signed char b = (signed char)BT_STOP;
+                float v = 0.f;
+                if (cx >= 0 && ry >= 0) {
+                    const long long k = (long long)cx * Lq + ry;
+                    b = bt[k];
+                    v = sm[k];
+                }
+                wbt[wid][lane][r] = b;
+                wsm[wid][lane][r] = v;
+            }
+            wq[wid][0][lane] = qy >= 0 ? a.qaa[qy] : 0;
+            wq[wid][1][lane] = (a.qss && qy >= 0) ? a.qss[qy] : ' ';
+            wd[wid][0][lane] = cx >= 0 ? a.daa[off + cx] : 0;
+            wd[wid][1][lane] = (a.dss && cx >= 0) ? a.dss[off + cx] : ' ';
         }
-        if (b == BT_LEFT) {
-            gaps++;
-            tq[n] = '-'; tt[n] = (char)a.daa[off + x]; tm[n] = ' ';
-            if (a.dss) st[n] = (char)a.dss[off + x];
-            n++; x--;
-            continue;
+        __syncwarp();
+        if (lane == 0) {
+            while (n < cap) {
+                if (x < 0 || y < 0) { done = 1; break; }
+                const int dx = x0 - x, dy = y0 - y;
+                if (dx >= 32 || dy >= 32) break;   // left the window
+                const int b = wbt[wid][dx][dy];
+                if (b == BT_STOP) { done = 1; break; }
+                sq[n] = ' ';
+                st[n] = ' ';
+                if (b == BT_UP) {
+                    gaps++;
+                    tq[n] = (char)wq[wid][0][dy]; tt[n] = '-'; tm[n] = ' ';
+                    if (a.qss) sq[n] = (char)wq[wid][1][dy];
+                    n++; y--;
+                    continue;
+                }
+                if (b == BT_LEFT) {
+                    gaps++;
+                    tq[n] = '-'; tt[n] = (char)wd[wid][0][dx]; tm[n] = ' ';
+                    if (a.dss) st[n] = (char)wd[wid][1][dx];
+                    n++; x--;
+                    continue;
+                }
+                const char cq = (char)wq[wid][0][dy], cd = (char)wd[wid][0][dx];
+                tq[n] = cq;
+                tt[n] = cd;
+                if (a.qss) sq[n] = (char)wq[wid][1][dy];
+                if (a.dss) st[n] = (char)wd[wid][1][dx];
+                if (cq == cd) { tm[n] = cq; idts++; }
+                else if (wsm[wid][dx][dy] > 0.f) { tm[n] = '+'; psts++; }
+                else tm[n] = ' ';
+                n++; x--; y--;
+            }
         }
-        tq[n] = (char)a.qaa[y];
-        tt[n] = (char)a.daa[off + x];
-        if (a.qss) sq[n] = (char)a.qss[y];
-        if (a.dss) st[n] = (char)a.dss[off + x];
-        if (tq[n] == tt[n]) { tm[n] = tq[n]; idts++; }
-        else if (sm[k] > 0.f) { tm[n] = '+'; psts++; }
-        else tm[n] = ' ';
-        n++; x--; y--;
+        x = __shfl_sync(FULL, x, 0);
+        y = __shfl_sync(FULL, y, 0);
+        n = __shfl_sync(FULL, n, 0);
+        done = __shfl_sync(FULL, done, 0);
+        __syncwarp();
     }
-    // the walk produced the strings back to front
+    // the walk produced the strings back to front: reverse them across the warp
     for (int rr = 0; rr < 5; rr++) {
         char* s = o + (size_t)rr * a.alnstride;
-        for (int i = 0, jj = n - 1; i < jj; i++, jj--) { const char t = s[i]; s[i] = s[jj]; s[jj] = t; }
-        s[n] = 0;
+        for (int i = lane; i < n / 2; i += 32) {
+            const int jj = n - 1 - i;
+            const char t = s[i]; s[i] = s[jj]; s[jj] = t;
+        }
+        if (lane == 0) s[n] = 0;
     }
-    int* info = a.aln_info + (size_t)m * 8;
-    info[0] = n; info[1] = idts; info[2] = psts; info[3] = gaps;
-    info[4] = (int)(((unsigned)(x + 1) << 16) | ((unsigned)(y + 1) & 0xffffu));
-    info[5] = (int)xx;
-    (void)L;
+    if (lane == 0) {
+        int* info = a.aln_info + (size_t)m * 8;
+        info[0] = n; info[1] = idts; info[2] = psts; info[3] = gaps;
+        info[4] = (int)(((unsigned)(x + 1) << 16) | ((unsigned)(y + 1) & 0xffffu));
+        info[5] = (int)xx;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -700,10 +759,10 @@ cudaError_t launch_map(const MapArgs& a, const float* qtrn, const float* dtrn, c
     if ((e = cudaMemsetAsync(a.prog_b, 0, progb, st)) != cudaSuccess) return e;
     const int gfb = (int)std::min<long long>(grid, (2 * nitems + MAPW - 1) / MAPW);
     map_fb_kernel<<<gfb, MAPW * 32, 0, st>>>(a, qtrn, dtrn, qcf);
-    map_z_kernel<<<(a.nmap + 7) / 8, 256, 0, st>>>(a);
+    map_z_kernel<<<a.nmap, 256, 0, st>>>(a);
     if ((e = reset()) != cudaSuccess) return e;
     map_dp_kernel<<<g, MAPW * 32, 0, st>>>(a);
-    map_tb_kernel<<<(a.nmap + 31) / 32, 32, 0, st>>>(a);
+    map_tb_kernel<<<(a.nmap + TBW - 1) / TBW, TBW * 32, 0, st>>>(a);
     *nlaunch += 4;
     return cudaGetLastError();
 }

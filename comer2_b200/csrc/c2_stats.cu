@@ -309,17 +309,24 @@ __global__ void __launch_bounds__(SCF * NDS) stats_kernel(StatsArgs a)
     const int Lq = a.Lq, L = a.plen[p];
     const long long off = a.poff[p];
     const float* __restrict__ sm = a.smat + a.cand_off[c];
+    __shared__ unsigned hist[NSCALED];
     for (int k = tid; k < NSCALED + 31; k += SCF * NDS) counts[k] = 0.f;
+    for (int k = tid; k < NSCALED; k += SCF * NDS) hist[k] = 0u;
     __syncthreads();
-    // histogram of rint(32 s), s clamped to [-10, 10]
-    const long long ncell = (long long)Lq * L;
-    for (long long k = tid; k < ncell; k += SCF * NDS) {
-        const int x = (int)(k / Lq), y = (int)(k - (long long)x * Lq);
-        if (a.xuninf && (a.qaa[y] == 'X' || a.daa[off + x] == 'X')) continue;
-        float s = sm[k];
-        s = s < -10.f ? -10.f : (s > 10.f ? 10.f : s);
-        atomicAdd(&counts[(int)rintf(s * SCF) - SMIN], 1.f);
+    // histogram of rint(32 s), s clamped to [-10, 10]: warp ty takes db
+    // columns, its lanes the query rows of a column (coalesced reads)
+    for (int x = ty; x < L; x += NDS) {
+        if (a.xuninf && a.daa[off + x] == 'X') continue;
+        const float* __restrict__ col = sm + (long long)x * Lq;
+        for (int y = tx; y < Lq; y += SCF) {
+            if (a.xuninf && a.qaa[y] == 'X') continue;
+            float s = col[y];
+            s = s < -10.f ? -10.f : (s > 10.f ? 10.f : s);
+            atomicAdd(&hist[(int)rintf(s * SCF) - SMIN], 1u);
+        }
     }
+    __syncthreads();
+    for (int k = tid; k < NSCALED; k += SCF * NDS) counts[k] = (float)hist[k];
     __syncthreads();
     // probability layout: row ty holds the scaled scores of unscaled score ty-10
     const int u = ty - 10;
