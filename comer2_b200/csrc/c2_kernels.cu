@@ -663,7 +663,9 @@ __device__ __forceinline__ void wf_steps(WfLane& D, int k0, int nst, int lane, i
     const float* __restrict__ rb = ring + (k0 & (P1C_RING - 1)) * RLD + lane;
     if (!CHECK) nst = 32;
     int ub = -1;
-#pragma unroll 8
+    // the instruction cache holds both variants of both kernels at these depths
+    constexpr int UNR = CHECK ? 2 : 4;
+#pragma unroll UNR
     for (int u = 0; u < nst; u++) {
         const float S = rb[u * RLD];
         const float* __restrict__ tp =
