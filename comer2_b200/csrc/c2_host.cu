@@ -11,7 +11,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
+#include <atomic>
+#include <thread>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -57,6 +60,21 @@ struct DevBuf {
     }
 };
 
+// Device copy of an uploaded database: shared by the handles that search it
+// (c2_share_db), freed with the last of them.
+struct DbStore {
+    DevBuf<float> d_drec, d_pbkg, d_dtrn, d_peno;
+    DevBuf<int> d_plen, d_order;
+    DevBuf<long long> d_poff;
+    DevBuf<unsigned char> d_daa, d_dss;
+    // tensor-core score operands, packed on first use (under tc_mu)
+    DevBuf<unsigned> d_tcdb;
+    DevBuf<long long> d_ttile;
+    DevBuf<float> d_cold;
+    bool tc_ready = false;
+    std::mutex tc_mu;
+};
+
 struct c2_handle {
     int device = 0;
     cudaStream_t stream = nullptr;      // stream in use
@@ -66,7 +84,6 @@ struct c2_handle {
     int nsm = 0;
     int grid = 0;
     int score_mode = C2_SCORE_FP32;   // phase-1 score arithmetic (c2_set_score_mode)
-    bool tc_ready = false;            // db operands of the tensor-core path packed
     // parameters
     c2_params prm{};
     std::vector<float> ssss, cvkeys, cvvals, nnw;
@@ -80,10 +97,7 @@ struct c2_handle {
     int Lmax = 0;
     std::vector<int32_t> h_plen;
     std::vector<int64_t> h_poff;
-    DevBuf<float> d_drec, d_pbkg, d_dtrn, d_peno;
-    DevBuf<int> d_plen, d_order;
-    DevBuf<long long> d_poff;
-    DevBuf<unsigned char> d_daa, d_dss;
+    std::shared_ptr<DbStore> db;
     // query
     int Lq = 0;
     float qeno = 0.f;
@@ -119,10 +133,9 @@ struct c2_handle {
     // strip pipeline of the phase-2 sweeps: last-row buffers, progress words
     DevBuf<float> d_bnd;
     DevBuf<unsigned long long> d_tbkey;
-    // tensor-core score operands
-    DevBuf<unsigned> d_tcdb, d_qa;
-    DevBuf<long long> d_ttile;
-    DevBuf<float> d_cold, d_qaaf;
+    // tensor-core query operands
+    DevBuf<unsigned> d_qa;
+    DevBuf<float> d_qaaf;
     DevBuf<int> d_prog;
     size_t bnd_half = 0, prog_half = 0;   // floats / words of one sweep's strip-pipeline scratch
     DevBuf<float> d_fscore;
@@ -145,6 +158,8 @@ struct c2_handle {
     DevBuf<unsigned long long> d_pairk;
     DevBuf<char> d_aln;
     int alnstride = 0;
+    // worker handles of c2_search_batch (sharing this handle's database)
+    std::vector<c2_handle*> workers;
 };
 
 static c2_status fail(c2_handle* h, c2_status st, const char* fmt, ...)
@@ -334,6 +349,8 @@ extern "C" c2_status c2_create(int device, const c2_params* p, c2_handle** out)
 extern "C" c2_status c2_destroy(c2_handle* h)
 {
     if (!h) return C2_ERR_ARG;
+    for (c2_handle* w : h->workers) c2_destroy(w);
+    h->workers.clear();
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -433,6 +450,7 @@ extern "C" c2_status c2_upload_db(c2_handle* h, const c2_profiles* d, uint64_t t
     CK(cudaSetDevice(h->device));
     const int P = d->nprofiles;
     const int64_t N = d->npositions;
+    h->db = std::make_shared<DbStore>();   // handles sharing the previous database keep it
     h->nprof = P;
     h->npos = N;
     h->total_pos = tot_pos ? tot_pos : (uint64_t)N;
@@ -468,31 +486,58 @@ extern "C" c2_status c2_upload_db(c2_handle* h, const c2_profiles* d, uint64_t t
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return d->lengths[a] > d->lengths[b]; });
     std::vector<long long> poff(d->offsets, d->offsets + P);
-    if (h->d_drec.ensure(rec.size()) || h->d_pbkg.ensure(bkg.size()) || h->d_plen.ensure(P) ||
-        h->d_order.ensure(P) || h->d_poff.ensure(P) || h->d_best.ensure(P) || h->d_coords.ensure(P))
+    if (h->db->d_drec.ensure(rec.size()) || h->db->d_pbkg.ensure(bkg.size()) || h->db->d_plen.ensure(P) ||
+        h->db->d_order.ensure(P) || h->db->d_poff.ensure(P) || h->d_best.ensure(P) || h->d_coords.ensure(P))
         return fail(h, C2_ERR_NOMEM, "device allocation for %d profiles / %lld positions failed", P, (long long)N);
-    CK(cudaMemcpy(h->d_drec.p, rec.data(), rec.size() * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d_pbkg.p, bkg.data(), bkg.size() * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d_plen.p, d->lengths, (size_t)P * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d_order.p, order.data(), (size_t)P * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d_poff.p, poff.data(), (size_t)P * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->db->d_drec.p, rec.data(), rec.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->db->d_pbkg.p, bkg.data(), bkg.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->db->d_plen.p, d->lengths, (size_t)P * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->db->d_order.p, order.data(), (size_t)P * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->db->d_poff.p, poff.data(), (size_t)P * 8, cudaMemcpyHostToDevice));
     // raw transitions, residues, SS states and ENOs for the statistics and MAP stages
-    if (h->d_dtrn.ensure((size_t)(N + P) * 7) || h->d_daa.ensure((size_t)N) || h->d_dss.ensure((size_t)N) ||
-        h->d_peno.ensure((size_t)P))
+    if (h->db->d_dtrn.ensure((size_t)(N + P) * 7) || h->db->d_daa.ensure((size_t)N) || h->db->d_dss.ensure((size_t)N) ||
+        h->db->d_peno.ensure((size_t)P))
         return fail(h, C2_ERR_NOMEM, "device allocation of db side arrays failed");
-    CK(cudaMemcpy(h->d_dtrn.p, d->trn, (size_t)(N + P) * 7 * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d_daa.p, d->aa, (size_t)N, cudaMemcpyHostToDevice));
-    if (d->ssstate) CK(cudaMemcpy(h->d_dss.p, d->ssstate, (size_t)N, cudaMemcpyHostToDevice));
-    else CK(cudaMemset(h->d_dss.p, ' ', (size_t)N));
-    if (d->eno) CK(cudaMemcpy(h->d_peno.p, d->eno, (size_t)P * 4, cudaMemcpyHostToDevice));
-    else CK(cudaMemset(h->d_peno.p, 0, (size_t)P * 4));
+    CK(cudaMemcpy(h->db->d_dtrn.p, d->trn, (size_t)(N + P) * 7 * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->db->d_daa.p, d->aa, (size_t)N, cudaMemcpyHostToDevice));
+    if (d->ssstate) CK(cudaMemcpy(h->db->d_dss.p, d->ssstate, (size_t)N, cudaMemcpyHostToDevice));
+    else CK(cudaMemset(h->db->d_dss.p, ' ', (size_t)N));
+    if (d->eno) CK(cudaMemcpy(h->db->d_peno.p, d->eno, (size_t)P * 4, cudaMemcpyHostToDevice));
+    else CK(cudaMemset(h->db->d_peno.p, 0, (size_t)P * 4));
     // strip-boundary scratch: per warp slot, two rows of 5 states
     const int lm = (h->Lmax + 31) & ~31;
     h->botstride = 10LL * lm;
     if (h->d_bot.ensure((size_t)h->grid * P1_WARPS * h->botstride))
         return fail(h, C2_ERR_NOMEM, "strip-boundary scratch allocation failed");
     h->Lq = 0;
-    h->tc_ready = false;
+    h->db->tc_ready = false;
+    return C2_OK;
+}
+
+// Search the database uploaded to src from dst as well (same device; no
+// copy): dst gets its own query, result and scratch buffers.
+extern "C" c2_status c2_share_db(c2_handle* dst, const c2_handle* src)
+{
+    if (!dst || !src || dst == src) return C2_ERR_ARG;
+    c2_handle* h = dst;   // error reports go to dst
+    if (!src->db || src->nprof <= 0) return fail(dst, C2_ERR_STATE, "share_db: the source handle has no database");
+    if (dst->device != src->device) return fail(dst, C2_ERR_ARG, "share_db: handles on different devices");
+    CK(cudaSetDevice(dst->device));
+    dst->db = src->db;
+    dst->nprof = src->nprof;
+    dst->npos = src->npos;
+    dst->total_pos = src->total_pos;
+    dst->total_prof = src->total_prof;
+    dst->h_plen = src->h_plen;
+    dst->h_poff = src->h_poff;
+    dst->Lmax = src->Lmax;
+    const int P = dst->nprof;
+    const int lm = (dst->Lmax + 31) & ~31;
+    dst->botstride = 10LL * lm;
+    if (dst->d_best.ensure(P) || dst->d_coords.ensure(P) ||
+        dst->d_bot.ensure((size_t)dst->grid * P1_WARPS * dst->botstride))
+        return fail(dst, C2_ERR_NOMEM, "share_db: per-handle buffers for %d profiles failed", P);
+    dst->Lq = 0;
     return C2_OK;
 }
 
@@ -699,22 +744,23 @@ static TcConsts tc_consts(const ScoreConsts& sc)
 // Pack the db operands of the tensor-core path (once per database).
 static c2_status tc_prepare_db(c2_handle* h)
 {
-    if (h->tc_ready) return C2_OK;
+    std::lock_guard<std::mutex> lk(h->db->tc_mu);
+    if (h->db->tc_ready) return C2_OK;
     std::vector<long long> tt(h->nprof);
     long long ntiles = 0;
     for (int k = 0; k < h->nprof; k++) {
         tt[k] = ntiles;
         ntiles += (long long)((h->h_plen[k] + 31) / 32) * 4;
     }
-    if (h->d_ttile.ensure(h->nprof) || h->d_tcdb.ensure((size_t)ntiles * TC_TILE_WORDS) ||
-        h->d_cold.ensure((size_t)h->npos * P1C_TRS))
+    if (h->db->d_ttile.ensure(h->nprof) || h->db->d_tcdb.ensure((size_t)ntiles * TC_TILE_WORDS) ||
+        h->db->d_cold.ensure((size_t)h->npos * P1C_TRS))
         return fail(h, C2_ERR_NOMEM, "tensor-core db operands (%lld tiles) allocation failed", ntiles);
-    CK(cudaMemcpyAsync(h->d_ttile.p, tt.data(), (size_t)h->nprof * 8, cudaMemcpyHostToDevice, h->stream));
-    CK(launch_tc_pack(h->d_drec.p, h->d_poff.p, h->d_plen.p, h->d_ttile.p, h->nprof, h->d_tcdb.p, h->d_cold.p,
+    CK(cudaMemcpyAsync(h->db->d_ttile.p, tt.data(), (size_t)h->nprof * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(launch_tc_pack(h->db->d_drec.p, h->db->d_poff.p, h->db->d_plen.p, h->db->d_ttile.p, h->nprof, h->db->d_tcdb.p, h->db->d_cold.p,
                       h->sc.lokappa0, h->sc.ssswgt, h->stream));
     h->launches++;
     CK(cudaStreamSynchronize(h->stream));
-    h->tc_ready = true;
+    h->db->tc_ready = true;
     return C2_OK;
 }
 
@@ -740,10 +786,10 @@ static void fill_p1(c2_handle* h, P1Args& a)
     memset(&a, 0, sizeof a);
     a.qrec = h->d_qrec.p;
     a.Lq = h->Lq;
-    a.drec = h->d_drec.p;
-    a.plen = h->d_plen.p;
-    a.poff = h->d_poff.p;
-    a.pbkg = h->d_pbkg.p;
+    a.drec = h->db->d_drec.p;
+    a.plen = h->db->d_plen.p;
+    a.poff = h->db->d_poff.p;
+    a.pbkg = h->db->d_pbkg.p;
     a.counter = h->d_counter.p;
     a.ssss = h->d_ssss.p;
     a.cvvals = h->d_cvvals.p;
@@ -763,14 +809,14 @@ extern "C" c2_status c2_run_phase1(c2_handle* h)
     P1Args a;
     fill_p1(h, a);
     a.nwork = h->nprof;
-    a.order = h->d_order.p;
+    a.order = h->db->d_order.p;
     CK(cudaMemsetAsync(h->d_counter.p, 0, sizeof(int), h->stream));
     if (h->score_mode == C2_SCORE_BF16_TC) {
         c2_status st = tc_prepare_db(h);
         if (st != C2_OK) return st;
-        a.tcdb = h->d_tcdb.p;
-        a.ttile = h->d_ttile.p;
-        a.cold = h->d_cold.p;
+        a.tcdb = h->db->d_tcdb.p;
+        a.ttile = h->db->d_ttile.p;
+        a.cold = h->db->d_cold.p;
         a.qa = h->d_qa.p;
         a.qaa = h->d_qaaf.p;
         a.tc = tc_consts(h->sc);
@@ -900,7 +946,7 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     f.ncand = nc;
     f.cand_prof = h->d_cand_prof.p;
     f.cand_off = h->d_cand_off.p;
-    f.plen = h->d_plen.p;
+    f.plen = h->db->d_plen.p;
     f.btck = h->d_btck.p;
     f.smat = h->d_smat.p;
     f.best = h->d_best.p;
@@ -994,11 +1040,11 @@ extern "C" c2_status c2_run_stats(c2_handle* h, int32_t* npassed)
     a.p2_cand = h->d_p2.p;
     a.cand_prof = h->d_cand_prof.p;
     a.cand_off = h->d_cand_off.p;
-    a.plen = h->d_plen.p;
-    a.poff = h->d_poff.p;
-    a.peno = h->d_peno.p;
+    a.plen = h->db->d_plen.p;
+    a.poff = h->db->d_poff.p;
+    a.peno = h->db->d_peno.p;
     a.qaa = h->d_qaa.p;
-    a.daa = h->d_daa.p;
+    a.daa = h->db->d_daa.p;
     a.smat = h->d_smat.p;
     a.fscore = h->d_fscore.p;
     a.fpsts = h->d_fpsts.p;
@@ -1077,8 +1123,8 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
     a.map_pass = h->d_mappass.p;
     a.cand_prof = h->d_cand_prof.p;
     a.cand_off = h->d_cand_off.p;
-    a.plen = h->d_plen.p;
-    a.poff = h->d_poff.p;
+    a.plen = h->db->d_plen.p;
+    a.poff = h->db->d_poff.p;
     a.smat = h->d_smat.p;
     a.mmat = h->d_mmat.p;
     a.stats = h->d_stats.p;
@@ -1099,8 +1145,8 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
     a.modscores = (h->prm.ssswgt > 0.f || h->prm.cvswgt > 0.f) ? 1 : 0;
     a.qaa = h->d_qaa.p;
     a.qss = h->d_qss.p;
-    a.daa = h->d_daa.p;
-    a.dss = h->d_dss.p;
+    a.daa = h->db->d_daa.p;
+    a.dss = h->db->d_dss.p;
     a.aln_info = h->d_alninfo.p;
     a.aln = h->d_aln.p;
     a.alnstride = h->alnstride;
@@ -1108,7 +1154,7 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
     // the MAP sweeps run 4 warps per CTA, one boundary slot each: stay within
     // the grid x P1_WARPS slots of the strip-boundary scratch
     const int grid = h->grid * P1_WARPS / 4;
-    CK(launch_map(a, h->d_qtrn.p, h->d_dtrn.p, h->d_qcf.p, grid, h->d_counter.p, h->stream, &nl));
+    CK(launch_map(a, h->d_qtrn.p, h->db->d_dtrn.p, h->d_qcf.p, grid, h->d_counter.p, h->stream, &nl));
     h->launches += nl;
     return C2_OK;
 }
@@ -1247,7 +1293,7 @@ extern "C" c2_status c2_run_phase1_static(c2_handle* h, float* d_best, uint32_t*
     P1Args a;
     fill_p1(h, a);
     a.nwork = h->nprof;
-    a.order = h->d_order.p;
+    a.order = h->db->d_order.p;
     a.counter = (int*)base;
     a.bot = (float*)((char*)base + C2_STATIC_HDR);
     a.best = d_best;
@@ -1270,17 +1316,17 @@ static void fill_adj(c2_handle* h, AdjArgs& a)
     a.npairs = (int)h->adj_prof.size();
     a.prof = h->d_adjprof.p;
     a.off = h->d_adjoff.p;
-    a.plen = h->d_plen.p;
-    a.poff = h->d_poff.p;
+    a.plen = h->db->d_plen.p;
+    a.poff = h->db->d_poff.p;
     a.qrec = h->d_qrec.p;
-    a.drec = h->d_drec.p;
-    a.pbkg = h->d_pbkg.p;
+    a.drec = h->db->d_drec.p;
+    a.pbkg = h->db->d_pbkg.p;
     a.qbkg = h->d_qbkg.p;
     a.ssss = h->d_ssss.p;
     a.cvvals = h->d_cvvals.p;
     a.sc = h->sc;
     a.qtrn = h->d_qtrn.p;
-    a.dtrn = h->d_dtrn.p;
+    a.dtrn = h->db->d_dtrn.p;
     a.qcfx = h->d_qcfx.p;
     for (int k = 0; k < 7; k++) a.theta[k] = h->adj_theta[k];
     a.wss = h->adj_wss;
@@ -1363,5 +1409,118 @@ extern "C" c2_status c2_logz_cells(c2_handle* h, int32_t pair, float* dlogz_ds, 
         for (int j = 0; j < L; j++)
             for (int i = 0; i < Lq; i++) dst[(size_t)i * L + j] = t[(size_t)j * Lq + i];   // row-major [Lq][L]
     }
+    return C2_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Multi-query search (replaces the reference's JobDispatcher / DevCommThread
+// query loop, src/libmycu/cualn/JobDispatcher.cpp:967-1213 and
+// DevCommThread.cpp:155-356): the batch's queries go to worker handles that
+// share the database, one host thread and one CUDA stream each, taking the
+// next query as they finish one; a query's host-side steps and its
+// latency-bound phase-2 kernels overlap other queries' work.
+
+// Query k of a profile set as a one-profile set
+static c2_profiles query_view(const c2_profiles* qs, int k, const int64_t* zero)
+{
+    c2_profiles v;
+    memset(&v, 0, sizeof v);
+    const int64_t o = qs->offsets[k];
+    v.nprofiles = 1;
+    v.npositions = qs->lengths[k];
+    v.lengths = qs->lengths + k;
+    v.offsets = zero;
+    v.bkg = qs->bkg + (size_t)k * NAA;
+    v.eno = qs->eno ? qs->eno + k : nullptr;
+    v.trn = qs->trn + (size_t)(o + k) * 7;
+    v.trg = qs->trg + (size_t)o * NAA;
+    v.cv = qs->cv + (size_t)o * NCV;
+    v.cvprior = qs->cvprior + o;
+    v.cvnorm2 = qs->cvnorm2 + o;
+    v.ss = qs->ss + (size_t)o * NSS;
+    v.ssstate = qs->ssstate ? qs->ssstate + o : nullptr;
+    v.aa = qs->aa + o;
+    return v;
+}
+
+static c2_status batch_workers(c2_handle* h, int nw)
+{
+    // workers made for an earlier database are remade
+    for (size_t i = 0; i < h->workers.size(); i++)
+        if (h->workers[i]->db != h->db) {
+            for (c2_handle* w : h->workers) c2_destroy(w);
+            h->workers.clear();
+            break;
+        }
+    while ((int)h->workers.size() < nw - 1) {
+        c2_params p = h->prm;
+        p.ssss = h->ssss.data();
+        p.cvs2s_keys = h->cvkeys.data();
+        p.cvs2s_values = h->cvvals.data();
+        p.sse_nn_weights = h->nnw.empty() ? nullptr : h->nnw.data();
+        c2_handle* w = nullptr;
+        c2_status st = c2_create(h->device, &p, &w);
+        if (st != C2_OK) return fail(h, st, "batch: creating a worker handle failed");
+        if ((st = c2_share_db(w, h)) != C2_OK) {
+            std::string e = w->err;
+            c2_destroy(w);
+            return fail(h, st, "batch: %s", e.c_str());
+        }
+        h->workers.push_back(w);
+    }
+    for (c2_handle* w : h->workers) w->score_mode = h->score_mode;
+    return C2_OK;
+}
+
+extern "C" c2_status c2_search_batch(c2_handle* h, const c2_profiles* queries, int32_t nworkers, c2_batch_cb cb,
+                                     void* user)
+{
+    if (!h || !cb || nworkers < 1 || nworkers > 8) return C2_ERR_ARG;
+    if (h->nprof <= 0 || !h->db) return fail(h, C2_ERR_STATE, "search_batch needs a database");
+    c2_status st = check_profiles(h, queries);
+    if (st != C2_OK) return st;
+    const int nq = queries->nprofiles;
+    const int nw = std::min(nworkers, nq);
+    if ((st = batch_workers(h, nw)) != C2_OK) return st;
+    std::vector<c2_handle*> ws(1, h);
+    for (int i = 0; i < nw - 1; i++) ws.push_back(h->workers[i]);
+    std::atomic<int> next(0);
+    std::mutex mu;   // serialises the callbacks and the first error
+    c2_status first = C2_OK;
+    std::string first_err;
+    auto run = [&](c2_handle* w) {
+        const int64_t zero = 0;
+        std::vector<c2_hit> hits;
+        std::vector<char> alns;
+        for (;;) {
+            const int q = next.fetch_add(1);
+            if (q >= nq) break;
+            const c2_profiles v = query_view(queries, q, &zero);
+            int32_t nh = 0;
+            size_t nb = 0;
+            c2_status s = c2_search(w, &v, &nh);
+            if (s == C2_OK) s = c2_get_hits(w, nullptr, 0, nullptr, &nb);
+            if (s == C2_OK) {
+                hits.resize(std::max(1, nh));
+                alns.resize(std::max<size_t>(1, nb));
+                s = c2_get_hits(w, hits.data(), nh, alns.data(), &nb);
+            }
+            std::lock_guard<std::mutex> lk(mu);
+            if (s != C2_OK) {
+                if (first == C2_OK) {
+                    first = s;
+                    first_err = "query " + std::to_string(q) + ": " + w->err;
+                }
+                cb(user, q, s, nullptr, 0, nullptr, 0);
+            } else {
+                cb(user, q, s, hits.data(), nh, alns.data(), nb);
+            }
+        }
+    };
+    std::vector<std::thread> th;
+    for (int i = 1; i < nw; i++) th.emplace_back(run, ws[i]);
+    run(ws[0]);
+    for (auto& t : th) t.join();
+    if (first != C2_OK) return fail(h, first, "search_batch: %s", first_err.c_str());
     return C2_OK;
 }

@@ -27,8 +27,11 @@ EXPORTS = [
     "c2_get_phase1", "c2_run_finalize", "c2_get_finalize", "c2_get_thresholds", "c2_set_stream", "c2_sync",
     "c2_launch_count", "c2_run_stats", "c2_run_map", "c2_get_hits", "c2_search", "c2_get_search_space",
     "c2_run_phase1_static", "c2_set_score_mode", "c2_logz_fwd", "c2_logz_bwd", "c2_logz_cells",
-    "c2_db2bin_info", "c2_db2bin_read",
+    "c2_db2bin_info", "c2_db2bin_read", "c2_share_db", "c2_search_batch",
 ]
+
+# c2_batch_cb
+BATCH_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_int32, C.c_int, C.c_void_p, C.c_int32, C.c_void_p, C.c_size_t)
 
 SCORE_FP32 = 0
 SCORE_BF16_TC = 1
@@ -120,6 +123,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.c2_db2bin_info.argtypes = [C.c_char_p, _i32p, _i64p, C.c_char_p, C.c_size_t]
     lib.c2_db2bin_read.argtypes = [C.c_char_p, _i32p, _i64p, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _u8p, _u8p,
                                    C.c_char_p, C.c_size_t]
+    lib.c2_share_db.argtypes = [C.c_void_p, C.c_void_p]
+    lib.c2_search_batch.argtypes = [C.c_void_p, P(c2_profiles), C.c_int32, BATCH_CB, C.c_void_p]
     for n in EXPORTS:
         getattr(lib, n).restype = C.c_int
     _lib = lib
@@ -353,6 +358,38 @@ class Handle:
         n = C.c_int32()
         self._ck(self.lib.c2_search(self._h, C.byref(s), C.byref(n)), "c2_search")
         return self.hits_arrays(n.value) if arrays else self.hits(n.value)
+
+    def search_batch(self, queries: ProfileSet, nworkers: int = 2):
+        """Search every profile of queries over the uploaded database with nworkers
+        worker handles sharing it (c2_search_batch).  Returns one (records,
+        alignments) pair per query, as hits_arrays() gives them."""
+        k = _Keep()
+        s = make_profiles(queries, k)
+        out = [None] * queries.nprofiles
+        errs = []
+
+        def cb(user, q, status, hits, nhits, alns, nbytes):
+            if status != C2_OK:
+                errs.append((q, status))
+                return
+            rec = np.zeros(nhits, dtype=HIT_DTYPE)
+            if nhits:
+                C.memmove(rec.ctypes.data, hits, nhits * HIT_DTYPE.itemsize)
+            buf = np.zeros(nbytes, np.uint8)
+            if nbytes:
+                C.memmove(buf.ctypes.data, alns, nbytes)
+            out[q] = (rec, buf)
+
+        fn = BATCH_CB(cb)
+        self._ck(self.lib.c2_search_batch(self._h, C.byref(s), int(nworkers), fn, None), "c2_search_batch")
+        if errs:
+            raise C2Error("c2_search_batch: queries failed: %s" % errs)
+        return out
+
+    def share_db(self, src: "Handle"):
+        """Search the database uploaded to src from this handle as well (c2_share_db)."""
+        self._ck(self.lib.c2_share_db(self._h, src._h), "c2_share_db")
+        self.nprof = src.nprof
 
     def launch_count(self) -> int:
         n = C.c_uint64()

@@ -188,6 +188,25 @@ c2_status c2_get_hits(c2_handle* h, c2_hit* hits, int32_t n, char* alns, size_t*
  * *nhits receives the number of hits; copy them with c2_get_hits. */
 c2_status c2_search(c2_handle* h, const c2_profiles* query, int32_t* nhits);
 
+/* Search the database uploaded to src from dst as well (same device, no
+ * copy); dst keeps its own query, results and scratch.  No reference
+ * counterpart (the reference copies each db chunk to every worker's device
+ * heap, CuDeviceMemory.cu:1073). */
+c2_status c2_share_db(c2_handle* dst, const c2_handle* src);
+
+/* Results of one query of a batch: hits and alignment strings as c2_get_hits
+ * returns them (valid during the call); status != C2_OK: the query failed. */
+typedef void (*c2_batch_cb)(void* user, int32_t query, c2_status status, const c2_hit* hits, int32_t nhits,
+                            const char* alns, size_t aln_bytes);
+
+/* Search every profile of queries (one query each) over the uploaded
+ * database with nworkers (1..8) worker handles sharing it, one host thread
+ * and CUDA stream each; cb receives each query's results as it completes
+ * (serialised, from the worker threads).  Replaces the query loop of the
+ * reference's JobDispatcher and DevCommThread
+ * (src/libmycu/cualn/JobDispatcher.cpp:967-1213, DevCommThread.cpp:155-356). */
+c2_status c2_search_batch(c2_handle* h, const c2_profiles* queries, int32_t nworkers, c2_batch_cb cb, void* user);
+
 /* Effective search space and length adjustment used for the current query
  * (AbstractScoreMatrix::ComputeLengthAdjustment,
  * src/libpro/srcsco/AbstractScoreMatrix.cpp:247-380). */
