@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_lib", "libcomer2_b200.so")
-SOURCES = ["c2_host.cu", "c2_kernels.cu", "c2_stats.cu", "c2_map.cu", "c2_adj.cu", "c2_dbio.cpp"]
+SOURCES = ["c2_host.cu", "c2_kernels.cu", "c2_stats.cu", "c2_map.cu", "c2_adj.cu", "c2_dbio.cpp", "c2_report.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

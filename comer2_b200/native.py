@@ -27,8 +27,11 @@ EXPORTS = [
     "c2_get_phase1", "c2_run_finalize", "c2_get_finalize", "c2_get_thresholds", "c2_set_stream", "c2_sync",
     "c2_launch_count", "c2_run_stats", "c2_run_map", "c2_get_hits", "c2_search", "c2_get_search_space",
     "c2_run_phase1_static", "c2_set_score_mode", "c2_logz_fwd", "c2_logz_bwd", "c2_logz_cells",
-    "c2_db2bin_info", "c2_db2bin_read", "c2_share_db", "c2_search_batch",
+    "c2_db2bin_info", "c2_db2bin_read", "c2_share_db", "c2_search_batch", "c2_format_report",
 ]
+
+REPORT_PLAIN = 0
+REPORT_JSON = 1
 
 # c2_batch_cb
 BATCH_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_int32, C.c_int, C.c_void_p, C.c_int32, C.c_void_p, C.c_size_t)
@@ -85,6 +88,80 @@ HIT_DTYPE = np.dtype([(k, {C.c_int32: np.int32, C.c_float: np.float32, C.c_uint3
                            C.c_int64: np.int64}[t]) for k, t in c2_hit._fields_], align=True)
 assert HIT_DTYPE.itemsize == C.sizeof(c2_hit)
 
+
+class c2_report_info(C.Structure):
+    _fields_ = [
+        ("progname", C.c_char_p), ("progversion", C.c_char_p), ("references", C.POINTER(C.c_char_p)),
+        ("query_desc", C.c_char_p), ("query_length", C.c_int32), ("query_eno", C.c_float),
+        ("query_has_ss", C.c_int32), ("db_names", C.POINTER(C.c_char_p)), ("n_db_names", C.c_int32),
+        ("db_positions", C.c_uint64), ("db_profiles", C.c_uint64), ("logevthld", C.c_float),
+        ("searchspace", C.c_double), ("deltalen", C.c_int32), ("ref_lambda", C.c_float), ("ref_K", C.c_float),
+        ("gapped_lambda", C.c_float), ("gapped_K", C.c_float), ("print_ss", C.c_int32), ("dsclen", C.c_int32),
+        ("dscwidth", C.c_int32), ("alnwidth", C.c_int32), ("show", C.c_int32), ("nhits", C.c_int32),
+        ("nalns", C.c_int32), ("db_desc", C.POINTER(C.c_char_p)), ("db_lengths", C.POINTER(C.c_int32)),
+        ("db_eno", C.POINTER(C.c_float)), ("db_has_ss", C.POINTER(C.c_uint8)),
+    ]
+
+
+def _cstrs(seq, terminate=False):
+    arr = (C.c_char_p * (len(seq) + (1 if terminate else 0)))()
+    for i, x in enumerate(seq):
+        arr[i] = None if x is None else x.encode()
+    return arr
+
+
+def format_report(fmt: int, hits: np.ndarray, alns: np.ndarray, *, query_length: int, query_eno: float,
+                  db_lengths, db_eno, db_desc=None, db_has_ss=None, query_desc=None, query_has_ss=True,
+                  db_names=("db",), db_positions=0, db_profiles=0, logevthld=0.0, searchspace=0.0, deltalen=0,
+                  ref_lambda=0.0, ref_K=0.0, gapped_lambda=0.0, gapped_K=0.0, print_ss=True, dsclen=1024,
+                  dscwidth=80, alnwidth=60, show=1, nhits=700, nalns=700, progname=None, progversion=None,
+                  references=None) -> str:
+    """One query's result file in the reference's Plain (REPORT_PLAIN) or JSON
+    (REPORT_JSON) format from hits_arrays()-style records (c2_format_report)."""
+    lib = load()
+    keep = []
+    r = c2_report_info()
+    r.progname = progname.encode() if progname else None
+    r.progversion = progversion.encode() if progversion else None
+    if references is not None:
+        refs = _cstrs(list(references), terminate=True)
+        keep.append(refs)
+        r.references = refs
+    r.query_desc = query_desc.encode() if query_desc is not None else None
+    r.query_length, r.query_eno, r.query_has_ss = int(query_length), float(query_eno), int(bool(query_has_ss))
+    names = _cstrs(list(db_names))
+    keep.append(names)
+    r.db_names, r.n_db_names = names, len(db_names)
+    r.db_positions, r.db_profiles = int(db_positions), int(db_profiles)
+    r.logevthld, r.searchspace, r.deltalen = float(logevthld), float(searchspace), int(deltalen)
+    r.ref_lambda, r.ref_K, r.gapped_lambda, r.gapped_K = (float(ref_lambda), float(ref_K), float(gapped_lambda),
+                                                          float(gapped_K))
+    r.print_ss, r.dsclen, r.dscwidth, r.alnwidth = int(bool(print_ss)), int(dsclen), int(dscwidth), int(alnwidth)
+    r.show, r.nhits, r.nalns = int(show), int(nhits), int(nalns)
+    dl = np.ascontiguousarray(db_lengths, np.int32)
+    de = np.ascontiguousarray(db_eno, np.float32)
+    keep += [dl, de]
+    r.db_lengths, r.db_eno = _ptr(dl, _i32p), _ptr(de, _fp)
+    if db_desc is not None:
+        dd = _cstrs(list(db_desc))
+        keep.append(dd)
+        r.db_desc = dd
+    if db_has_ss is not None:
+        ds = np.ascontiguousarray(db_has_ss, np.uint8)
+        keep.append(ds)
+        r.db_has_ss = _ptr(ds, _u8p)
+    hits = np.ascontiguousarray(hits, HIT_DTYPE)
+    alns = np.ascontiguousarray(alns, np.uint8)
+    n = C.c_size_t(0)
+    st = lib.c2_format_report(int(fmt), C.byref(r), hits.ctypes.data, len(hits), alns.ctypes.data, None, C.byref(n))
+    if st != C2_OK:
+        raise C2Error("c2_format_report(size): %s" % STATUS_NAMES.get(st, st))
+    buf = C.create_string_buffer(n.value)
+    st = lib.c2_format_report(int(fmt), C.byref(r), hits.ctypes.data, len(hits), alns.ctypes.data, buf, C.byref(n))
+    if st != C2_OK:
+        raise C2Error("c2_format_report: %s" % STATUS_NAMES.get(st, st))
+    return buf.value.decode("latin-1")
+
 _lib: Optional[C.CDLL] = None
 
 
@@ -123,6 +200,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.c2_db2bin_info.argtypes = [C.c_char_p, _i32p, _i64p, C.c_char_p, C.c_size_t]
     lib.c2_db2bin_read.argtypes = [C.c_char_p, _i32p, _i64p, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _u8p, _u8p,
                                    C.c_char_p, C.c_size_t]
+    lib.c2_format_report.argtypes = [C.c_int32, P(c2_report_info), C.c_void_p, C.c_int32, C.c_void_p, C.c_char_p,
+                                     P(C.c_size_t)]
     lib.c2_share_db.argtypes = [C.c_void_p, C.c_void_p]
     lib.c2_search_batch.argtypes = [C.c_void_p, P(c2_profiles), C.c_int32, BATCH_CB, C.c_void_p]
     for n in EXPORTS:

@@ -207,6 +207,44 @@ typedef void (*c2_batch_cb)(void* user, int32_t query, c2_status status, const c
  * (src/libmycu/cualn/JobDispatcher.cpp:967-1213, DevCommThread.cpp:155-356). */
 c2_status c2_search_batch(c2_handle* h, const c2_profiles* queries, int32_t nworkers, c2_batch_cb cb, void* user);
 
+/* Result files in the reference's formats (-f 0 Plain, -f 1 JSON): the
+ * writers' inputs besides the hits, as the comer program has them. */
+enum { C2_REPORT_PLAIN = 0, C2_REPORT_JSON = 1 };
+
+typedef struct {
+    const char* progname;           /* program name, may be NULL */
+    const char* progversion;        /* may be NULL */
+    const char* const* references;  /* NULL-terminated citation lines, may be NULL */
+    const char* query_desc;         /* query description, may be NULL */
+    int32_t query_length;
+    float query_eno;
+    int32_t query_has_ss;           /* the query carries SS predictions */
+    const char* const* db_names;    /* database names */
+    int32_t n_db_names;
+    uint64_t db_positions;          /* database size (positions) */
+    uint64_t db_profiles;           /* number of database profiles */
+    float logevthld;                /* log of the E-value threshold */
+    double searchspace;             /* effective search space (c2_get_search_space) */
+    int32_t deltalen;               /* length adjustment (c2_get_search_space) */
+    float ref_lambda, ref_K;        /* ungapped reference lambda and K */
+    float gapped_lambda, gapped_K;  /* expected gapped lambda and K */
+    int32_t print_ss;               /* SS lines in Plain alignments (SS weight > 0) */
+    int32_t dsclen, dscwidth, alnwidth, show, nhits, nalns;  /* options DSCLEN DSCWIDTH ALNWIDTH SHOW NOHITS NOALNS */
+    /* per database profile, indexed by c2_hit.profile */
+    const char* const* db_desc;     /* descriptions, may be NULL */
+    const int32_t* db_lengths;
+    const float* db_eno;
+    const uint8_t* db_has_ss;       /* SS predictions present; NULL: all have them */
+} c2_report_info;
+
+/* Format one query's result file from its hits (as c2_get_hits returns them,
+ * sorted by log E-value).  out == NULL: *out_bytes receives the size needed
+ * (with the terminating NUL).  Replaces the reference's result writers
+ * (src/libmycu/cupro/CuBatchProcessingFinalizerPlain.cpp, ...JSON.cpp and
+ * src/libmycu/cualn/AlnWriterPlain.cpp, AlnWriterJSON.cpp).  No GPU needed. */
+c2_status c2_format_report(int32_t format, const c2_report_info* info, const c2_hit* hits, int32_t nhits,
+                           const char* alns, char* out, size_t* out_bytes);
+
 /* Effective search space and length adjustment used for the current query
  * (AbstractScoreMatrix::ComputeLengthAdjustment,
  * src/libpro/srcsco/AbstractScoreMatrix.cpp:247-380). */

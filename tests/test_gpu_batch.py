@@ -58,3 +58,33 @@ def test_shared_database_and_reupload(params):
     b = h.search_batch(S.concat(w2.queries[:2]), nworkers=2)
     for qq, got in zip(w2.queries[:2], b):
         _same(h.search(qq, arrays=True), got)
+
+
+def test_search_to_result_files(params):
+    """A search's hits written in both reference formats: the JSON parses and
+    carries every hit's alignment; the Plain file lists the same hits."""
+    import json
+    from comer2_b200 import native as N
+    w = S.config(1, seed=3, scale=0.003)
+    h = N.Handle(params, 0)
+    h.upload_db(w.db)
+    q = w.queries[0]
+    rec, alns = h.search(q, arrays=True)
+    assert len(rec) > 0
+    ss, dl = h.search_space()
+    thld, logevthld = h.thresholds()
+    kw = dict(query_length=int(q.lengths[0]), query_eno=float(q.eno[0]), db_lengths=w.db.lengths,
+              db_eno=w.db.eno, db_desc=["profile %d" % k for k in range(w.db.nprofiles)],
+              db_positions=int(w.db.npositions), db_profiles=int(w.db.nprofiles), logevthld=logevthld,
+              searchspace=float(ss), deltalen=int(dl), ref_lambda=params.ungapped_lambda, ref_K=params.ungapped_K,
+              gapped_lambda=params.gapped_lambda, gapped_K=params.gapped_K)
+    d = json.loads(N.format_report(N.REPORT_JSON, rec, alns, **kw))["comer_search"]
+    assert len(d["search_hits"]) == len(rec)
+    for r, hit in zip(d["search_hits"], rec):
+        a = r["hit_record"]["alignment"]
+        o = int(hit["aln_offset"])
+        L = int(hit["alnlen"])
+        assert a["query_aln"] == bytes(alns[o:o + L]).decode()
+        assert r["hit_record"]["target_description"] == "profile %d" % int(hit["profile"])
+    plain = N.format_report(N.REPORT_PLAIN, rec, alns, **kw)
+    assert plain.count("\n>profile ") == len(rec)
