@@ -33,6 +33,8 @@ cudaError_t launch_p1(const P1Args& a, const float* qbkg, int which, int grid, c
 int p1_blocks_per_sm(int cvcard);
 int p1c_blocks_per_sm(int cvcard);
 int p1t_blocks_per_sm(int cvcard, cudaError_t* err);
+cudaError_t launch_aln_pack(const char* aln, int alnstride, const int* info, const long long* off, int nm, char* dst,
+                            cudaStream_t st);
 cudaError_t launch_tc_pack(const float* drec, const long long* poff, const int* plen, const long long* ttile,
                            int nprof, unsigned* tcdb, float* cold, float lok, float wss, cudaStream_t st);
 cudaError_t launch_fin(const FinArgs& a, cudaStream_t st);
@@ -156,7 +158,8 @@ struct c2_handle {
     DevBuf<float> d_fb, d_bb, d_pairf;
     DevBuf<unsigned> d_pairc;
     DevBuf<unsigned long long> d_pairk;
-    DevBuf<char> d_aln;
+    DevBuf<char> d_aln, d_alnpack;
+    DevBuf<long long> d_alnoff;
     int alnstride = 0;
     // worker handles of c2_search_batch (sharing this handle's database)
     std::vector<c2_handle*> workers;
@@ -409,14 +412,28 @@ static void strip_items(const std::vector<int>& lens, int nstrips, int nwarps, s
     double lm = 31.0;
     for (int L : lens) lm += (double)L / std::max(1, np);
     const double K = (double)STRIP_LAG * nwarps / (nstrips * lm);
-    std::vector<std::pair<double, int>> key((size_t)np * nstrips);
-    for (int p = 0; p < np; p++)
-        for (int s = 0; s < nstrips; s++) key[(size_t)p * nstrips + s] = {p + K * s, p * nstrips + s};
-    std::stable_sort(key.begin(), key.end(), [&](const std::pair<double, int>& x, const std::pair<double, int>& y) {
-        return x.first < y.first;
-    });
-    items.resize(key.size());
-    for (size_t i = 0; i < key.size(); i++) items[i] = key[i].second;
+    // key(p, s) = p + K s = b + f_s with bucket b = p + floor(K s) and
+    // f_s = frac(K s): each bucket holds one item per strip, ordered by f_s
+    // and, for equal f_s, larger s first (its p is smaller); the same order
+    // in every bucket, so the table is emitted bucket by bucket in linear time
+    std::vector<long long> fl(nstrips);
+    std::vector<double> fr(nstrips);
+    for (int s = 0; s < nstrips; s++) {
+        const double ks = K * s;
+        fl[s] = (long long)std::floor(ks);
+        fr[s] = ks - (double)fl[s];
+    }
+    std::vector<int> perm(nstrips);
+    std::iota(perm.begin(), perm.end(), 0);
+    std::sort(perm.begin(), perm.end(), [&](int x, int y) { return fr[x] < fr[y] || (fr[x] == fr[y] && x > y); });
+    items.clear();
+    items.reserve((size_t)np * nstrips);
+    const long long bmax = (long long)np - 1 + fl[nstrips - 1];
+    for (long long b = 0; b <= bmax; b++)
+        for (int s : perm) {
+            const long long p = b - fl[s];
+            if (p >= 0 && p < np) items.push_back((int)p * nstrips + s);
+        }
 }
 
 // candidate margin and traceback tolerance of the BF16 score mode (relative)
@@ -1177,8 +1194,7 @@ extern "C" c2_status c2_get_hits(c2_handle* h, c2_hit* hits, int32_t n, char* al
         return (hits || alns) ? C2_ERR_ARG : C2_OK;
     }
     if (n < nm || *aln_bytes < need) return fail(h, C2_ERR_ARG, "output buffers too small (%d hits, %zu bytes)", nm, need);
-    std::vector<char> raw((size_t)nm * per);
-    if (nm > 0) CK(cudaMemcpy(raw.data(), h->d_aln.p, raw.size(), cudaMemcpyDeviceToHost));
+    (void)per;
     std::vector<int> order(nm);
     std::iota(order.begin(), order.end(), 0);
     auto logE = [&](int m) { return h->h_stats[(size_t)h->h_mappass[m] * STATS_NOUT + ST_LOGE]; };
@@ -1188,6 +1204,24 @@ extern "C" c2_status c2_get_hits(c2_handle* h, c2_hit* hits, int32_t n, char* al
         if (ex != ey) return ex < ey;
         return prof(x) < prof(y);
     });
+    // the strings, packed on the device in hit order (only their bytes cross PCIe)
+    std::vector<long long> off((size_t)std::max(nm, 1));
+    {
+        size_t p = 0;
+        for (int i = 0; i < nm; i++) {
+            off[order[i]] = (long long)p;
+            p += (size_t)5 * (info[(size_t)order[i] * 8] + 1);
+        }
+    }
+    if (nm > 0) {
+        if (h->d_alnoff.ensure((size_t)nm) || h->d_alnpack.ensure(need))
+            return fail(h, C2_ERR_NOMEM, "alignment packing buffers failed");
+        CK(cudaMemcpyAsync(h->d_alnoff.p, off.data(), (size_t)nm * 8, cudaMemcpyHostToDevice, h->stream));
+        CK(launch_aln_pack(h->d_aln.p, h->alnstride, h->d_alninfo.p, h->d_alnoff.p, nm, h->d_alnpack.p, h->stream));
+        h->launches++;
+        CK(cudaMemcpyAsync(alns, h->d_alnpack.p, need, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
     size_t pos = 0;
     for (int i = 0; i < nm; i++) {
         const int m = order[i];
@@ -1213,12 +1247,7 @@ extern "C" c2_status c2_get_hits(c2_handle* h, c2_hit* hits, int32_t n, char* al
         o.beg = (uint32_t)in[4];
         o.end = (uint32_t)in[5];
         o.aln_offset = (int64_t)pos;
-        for (int r = 0; r < 5; r++) {
-            const char* src = raw.data() + (size_t)m * per + (size_t)r * h->alnstride;
-            memcpy(alns + pos, src, (size_t)in[0]);
-            alns[pos + in[0]] = 0;
-            pos += (size_t)in[0] + 1;
-        }
+        pos += (size_t)5 * (in[0] + 1);
     }
     return C2_OK;
 }

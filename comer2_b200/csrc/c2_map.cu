@@ -737,6 +737,32 @@ __global__ void __launch_bounds__(TBW * 32) map_tb_kernel(MapArgs a)
 }
 
 // ---------------------------------------------------------------------------
+// Pack the hits' alignment strings for the host: pair m's five strings
+// (alnlen bytes each at stride alnstride) to dst + off[m], each followed by
+// a NUL; one warp per pair
+__global__ void __launch_bounds__(128) aln_pack_kernel(const char* __restrict__ aln, int alnstride,
+                                                      const int* __restrict__ info, const long long* __restrict__ off,
+                                                      int nm, char* __restrict__ dst)
+{
+    const int lane = threadIdx.x & 31;
+    const int m = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (m >= nm) return;
+    const int L = info[(size_t)m * 8];
+    const char* src = aln + (size_t)m * 5 * alnstride;
+    char* o = dst + off[m];
+    for (int r = 0; r < 5; r++) {
+        for (int i = lane; i <= L; i += 32) o[(size_t)r * (L + 1) + i] = (i < L) ? src[(size_t)r * alnstride + i] : 0;
+    }
+}
+
+cudaError_t launch_aln_pack(const char* aln, int alnstride, const int* info, const long long* off, int nm, char* dst,
+                            cudaStream_t st)
+{
+    if (nm <= 0) return cudaSuccess;
+    aln_pack_kernel<<<(nm + 3) / 4, 128, 0, st>>>(aln, alnstride, info, off, nm, dst);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_map(const MapArgs& a, const float* qtrn, const float* dtrn, const float* qcf, int grid,
                        int* counter, cudaStream_t st, int* nlaunch)
 {
