@@ -52,6 +52,7 @@ constexpr int REC_CHUNK = 8, REC_CHUNK_LOG = 3, REC_SLOTS = 16;
 // shared memory per warp: score ring [32][32], SS row table [32][32], record ring
 constexpr int P1_WARP_FLOATS = 32 * 32 + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE;
 constexpr int MAX_CVCARD = 256;
+constexpr int P1TB_CVREP = 16;   // CV table replicas of the traceback sweep
 // Tensor-core (BF16 split) phase-1 kernel.  The three contractions of a cell
 // score -- amino acids (K = 20), context vectors (K = 19) and the SS table
 // (K = card <= 32, the db side a 3-hot vector of SS probabilities) -- run as

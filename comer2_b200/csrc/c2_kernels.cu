@@ -359,12 +359,16 @@ p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int cvcard = a.sc.cvcard;
     const int card = a.sc.ssss_card;
-    float* cvtab = smem;                                      // [cvcard][32]
-    float* wb = smem + cvcard * 32 + wid * P1_WARP_FLOATS;
+    // traceback codes of the last 32 columns per lane: each lane writes its
+    // cell of column j at step j + lane and the warp stores column k - 31 at
+    // step k, one coalesced 32-byte segment
+    __shared__ signed char btr[P1_WARPS][32][33];
+    float* cvtab = smem;                                      // [cvcard][P1TB_CVREP]
+    float* wb = smem + cvcard * P1TB_CVREP + wid * P1_WARP_FLOATS;
     float* ring = wb;                                         // [32][32]
     float* U = wb + 32 * 32;                                  // [card][32]
     float* rec = U + MAX_SSSS_CARD * 32;                      // [REC_SLOTS][DR_STRIDE] db records
-    for (int i = threadIdx.x; i < cvcard * 32; i += blockDim.x) cvtab[i] = a.cvvals[i >> 5];
+    for (int i = threadIdx.x; i < cvcard * P1TB_CVREP; i += blockDim.x) cvtab[i] = a.cvvals[i / P1TB_CVREP];
     __syncthreads();
 
     const int Lq = a.Lq;
@@ -457,7 +461,7 @@ p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
                 if (k < L) {
                     const float4* rp = reinterpret_cast<const float4*>(rec + (k & (REC_SLOTS - 1)) * DR_STRIDE);
                     float mod;
-                    float S = cell_score<32>(R, rp, U, cvtab, sc, lane, mod);
+                    float S = cell_score<P1TB_CVREP>(R, rp, U, cvtab, sc, lane, mod);
                     if (!act) S = -9.f;
                     ring[(k & 31) * 32 + lane] = S;
                     if (act) {
@@ -535,7 +539,11 @@ p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
                     if (mx < nw.IM) { mx = nw.IM; b = BT_LEFT; }
                     if (mx < nw.DN) { mx = nw.DN; b = BT_UP; }
                     if (mx < nw.ND) { b = BT_LEFT; }
-                    bt[(long long)j * Lq + r] = (signed char)b;
+                    btr[wid][j & 31][lane] = (signed char)b;
+                }
+                {
+                    const int cfl = k - 31;
+                    if (act && cfl >= 0 && cfl < L) bt[(long long)cfl * Lq + r] = btr[wid][cfl & 31][lane];
                 }
                 if (wr_bot && j >= 0 && j < L) {
                     botw[0 * L + j] = nw.MM;
@@ -1550,6 +1558,13 @@ size_t p1_smem_bytes(int cvcard)
     return (size_t)(cvcard * 32 + P1_WARPS * P1_WARP_FLOATS) * sizeof(float);
 }
 
+// the traceback sweep: fewer CV table replicas make room for its traceback
+// ring, keeping two CTAs per SM
+size_t p1tb_smem_bytes(int cvcard)
+{
+    return (size_t)(cvcard * P1TB_CVREP + P1_WARPS * P1_WARP_FLOATS) * sizeof(float);
+}
+
 cudaError_t launch_p1(const P1Args& a, const float* qbkg, int which, int grid, cudaStream_t st)
 {
     if (which == P1K_TENSOR) {
@@ -1566,8 +1581,9 @@ cudaError_t launch_p1(const P1Args& a, const float* qbkg, int which, int grid, c
     }
     const size_t sm = p1_smem_bytes(a.sc.cvcard);
     if (which == P1K_TRACEBACK) {
-        cudaFuncSetAttribute(p1tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        p1tb_kernel<<<grid, P1_WARPS * 32, sm, st>>>(a, qbkg);
+        const size_t smt = p1tb_smem_bytes(a.sc.cvcard);
+        cudaFuncSetAttribute(p1tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
+        p1tb_kernel<<<grid, P1_WARPS * 32, smt, st>>>(a, qbkg);
     } else {
         cudaFuncSetAttribute(p1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         p1_kernel<<<grid, P1_WARPS * 32, sm, st>>>(a, qbkg);
