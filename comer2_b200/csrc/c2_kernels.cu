@@ -594,17 +594,11 @@ p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
 // strip, column j) sits in slot (i + j) & 63, so at step k every lane reads
 // slot k & 63 and a DP stage reads 32 consecutive slots from one base.
 
-// Packed FP32 pair add (sm_100 add.f32x2): two IEEE round-to-nearest adds,
-// bit-identical to the scalar ones.
-__device__ __forceinline__ float2 add2(float2 a, float2 b)
-{
-    float2 d;
-    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(d.x), "=f"(d.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return d;
-}
+// Pair of FP32 adds.  The packed sm_100 form (add.rn.f32x2) gives the same
+// bits with ~1 % fewer instructions here, but measured 2 % slower in the
+// tensor-core phase-1 kernel (5.53 vs 5.42 ms on 5,000 profiles), so the pairs
+// stay two scalar adds; the pairing keeps the shared sums explicit.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 
 // Maximum of three (sm_100 three-input max.f32; exact, like two fmaxf)
 __device__ __forceinline__ float max3f(float a, float b, float c)
@@ -616,8 +610,7 @@ __device__ __forceinline__ float max3f(float a, float b, float c)
 
 // One lane of the wavefront DP.  Every Viterbi candidate of the reference's
 // recurrence is (state + query transition) + db transition, evaluated in that
-// order (bit-identical to the scalar form) and issued as packed pairs where
-// two candidates share the operation:
+// order, with the sums that two candidates or two steps share computed once:
 //   X = (up.MM, up.DN) + (qMM, qDM)   W = (up.MM, up.DN) + (qMD, qDD)
 //   Y = (up.MI, up.IM) + (qMM, qIM)   z = up.ND + qMM
 // X, Y and z are the up-sums of this step and the diagonal sums of the next
@@ -665,8 +658,7 @@ __device__ __forceinline__ void wf_init(WfLane& D, const float* q7, const St5& L
 template <bool CHECK, int RLD, bool TMIRROR, int TMASK>
 __device__ __forceinline__ void wf_steps(WfLane& D, int k0, int nst, int lane, int L, bool act,
                                          const float* __restrict__ ring, const float* __restrict__ tcol,
-                                         const float* __restrict__ bnd, bool wr_bot, float* __restrict__ botw,
-                                         int Lmax)
+                                         float* __restrict__ bnd, bool wr_bot)
 {
     const float* __restrict__ rb = ring + (k0 & (P1C_RING - 1)) * RLD + lane;
     if (!CHECK) nst = 32;
@@ -718,18 +710,33 @@ __device__ __forceinline__ void wf_steps(WfLane& D, int k0, int nst, int lane, i
         // their MM stays 0 and never beats a maximum
         const bool inm = !CHECK || (j >= 0 && j < L);
         if ((!CHECK || act) && inm && nMM > D.best) { D.best = nMM; ub = u; }
-        if (wr_bot && inm) {
-            float* bw = botw + (k0 - 31 + u);
-            bw[0 * Lmax] = nMM;
-            bw[1 * Lmax] = nMI;
-            bw[2 * Lmax] = nIM;
-            bw[3 * Lmax] = nDN;
-            bw[4 * Lmax] = nND;
+        if (wr_bot) {
+            // lane 31's cell (column k0 + u - 31) into the slot lane 0 read at
+            // the top of this step; bot_flush stores the 32 columns per chunk
+            *reinterpret_cast<float4*>(bnd + u * 8) = make_float4(nMM, nMI, nIM, nDN);
+            bnd[u * 8 + 4] = nND;
         }
         D.MM = nMM; D.MI = nMI; D.IM = nIM; D.DN = nDN; D.ND = nND;
         D.X = X; D.Y = Y; D.z = z;
     }
     if (ub >= 0) D.kbest = k0 + ub;
+}
+
+// The strip's last row after a DP stage over [k0, k0 + 32): slot l of bnd
+// holds lane 31's states at column k0 - 31 + l; the warp stores the columns
+// inside the matrix to the boundary buffer, one coalesced segment per state
+__device__ __forceinline__ void bot_flush(const float* __restrict__ bnd, float* __restrict__ botw, int k0, int L,
+                                          int Lmax, int lane)
+{
+    const int c = k0 - 31 + lane;
+    if (c >= 0 && c < L) {
+        const float4 a = *reinterpret_cast<const float4*>(bnd + lane * 8);
+        botw[0 * Lmax + c] = a.x;
+        botw[1 * Lmax + c] = a.y;
+        botw[2 * Lmax + c] = a.z;
+        botw[3 * Lmax + c] = a.w;
+        botw[4 * Lmax + c] = bnd[lane * 8 + 4];
+    }
 }
 
 // Corner cells (CellYXinCorners): row r keeps S = -9 at columns j <= cA(r)
@@ -860,11 +867,11 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
                 // ---- DP stage: wavefront steps [32m, 32m + 32)
                 const int k0 = 32 * m, k1 = min(k0 + 32, kend);
                 if (m >= 1 && k0 + 31 < L && k1 == k0 + 32)
-                    wf_steps<false, 32, false, P1C_RING - 1>(D, k0, 32, lane, L, act, ring, trn, bnd, wr_bot, botw,
-                                                             Lmax);
+                    wf_steps<false, 32, false, P1C_RING - 1>(D, k0, 32, lane, L, act, ring, trn, bnd, wr_bot);
                 else
-                    wf_steps<true, 32, false, P1C_RING - 1>(D, k0, k1 - k0, lane, L, act, ring, trn, bnd, wr_bot,
-                                                            botw, Lmax);
+                    wf_steps<true, 32, false, P1C_RING - 1>(D, k0, k1 - k0, lane, L, act, ring, trn, bnd, wr_bot);
+                __syncwarp();
+                if (s + 1 < nstrips) bot_flush(bnd, botw, k0, L, Lmax, lane);
                 __syncwarp();
                 // next 32 columns of the row above the strip
                 *reinterpret_cast<float4*>(bnd + lane * 8) = make_float4(D.bnxt[0], D.bnxt[1], D.bnxt[2], D.bnxt[3]);
@@ -1375,10 +1382,11 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                 const int k0 = 32 * m, k1 = min(k0 + 32, kend);
                 const float* tcol = cring + ((k0 - lane + P1T_CMOD) % P1T_CMOD) * P1C_TRS;
                 if (m >= 1 && k0 + 31 < L && k1 == k0 + 32)
-                    wf_steps<false, P1T_RLD, true, 0>(D, k0, 32, lane, L, act, ring, tcol, bnd, wr_bot, botw, Lmax);
+                    wf_steps<false, P1T_RLD, true, 0>(D, k0, 32, lane, L, act, ring, tcol, bnd, wr_bot);
                 else
-                    wf_steps<true, P1T_RLD, true, 0>(D, k0, k1 - k0, lane, L, act, ring, tcol, bnd, wr_bot, botw,
-                                                     Lmax);
+                    wf_steps<true, P1T_RLD, true, 0>(D, k0, k1 - k0, lane, L, act, ring, tcol, bnd, wr_bot);
+                __syncwarp();
+                if (s + 1 < nstrips) bot_flush(bnd, botw, k0, L, Lmax, lane);
                 __syncwarp();
                 *reinterpret_cast<float4*>(bnd + lane * 8) = make_float4(D.bnxt[0], D.bnxt[1], D.bnxt[2], D.bnxt[3]);
                 bnd[lane * 8 + 4] = D.bnxt[4];
