@@ -1096,15 +1096,24 @@ __global__ void __launch_bounds__(128) tc_pack_kernel(const float* __restrict__ 
 //         table is not uniform), S = s0 + (ss + cvm)
 // (cell_score is the FP32 form; src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cu)
 constexpr float C2_LN2 = 0.693147180559945309f;
+// hardware base-2 logarithm, denormal inputs flushed (the arguments here, an
+// amino-acid odds sum and a CV determinant, are far above the denormal range)
+__device__ __forceinline__ float lg2_ftz(float x)
+{
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+template <bool CVUNIF>
 __device__ __forceinline__ float tc_cell(float daa, float dot, float ss, float cq, float pq2, float cd, float pd2,
                                          const float* __restrict__ cvl, const TcConsts& tc)
 {
-    const float s0 = fmaf(__log2f(daa), C2_LN2, -tc.shift);
+    const float s0 = fmaf(lg2_ftz(daa), C2_LN2, -tc.shift);
     const float det = fmaf(-dot, dot, cq * cd);
-    const float x = (fmaf(tc.p2l, __log2f(det), tc.c2) - pq2) - pd2;
+    const float x = (fmaf(tc.p2l, lg2_ftz(det), tc.c2) - pq2) - pd2;
     const int ix = min(max(__float2int_rn(x), tc.ilo), tc.ihi);
     float cvm = cvl[ix * P1T_CVREP];
-    if (!tc.uniform) {
+    if (!CVUNIF) {
         cvm = (tc.kl2 <= x) ? tc.vlw : cvm;
         cvm = (x <= tc.kf2) ? tc.vfw : cvm;
     }
@@ -1135,6 +1144,8 @@ __device__ __forceinline__ void stage_cols(float* cring, const float* __restrict
 // layout: lane (g, q) holds rows g, g + 8 of each 16-row tile and columns
 // 2q, 2q + 1 of each 8-column tile), applies the epilogue per cell, writes the
 // scores into the ring, then advances the same wavefront DP as p1c_kernel.
+// CVUNIF: the CV table's key range coincides with its index clamp (TcConsts)
+template <bool CVUNIF>
 __global__ void __launch_bounds__(P1T_WARPS * 32, 1)
 p1t_kernel(P1Args a, const float* __restrict__ qbkg)
 {
@@ -1360,20 +1371,24 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                                 }
                             // epilogue: cell (row 16 mt + g + 8 hh, column 32 m + cl + e) is
                             // register 2 hh + e; its score goes to anti-diagonal row + column
+                            float S[4];
 #pragma unroll
-                            for (int hh = 0; hh < 2; hh++)
+                            for (int i = 0; i < 4; i++)
+                                S[i] = tc_cell<CVUNIF>(acc[0][i], acc[1][i], acc[2][i], rq[mt][i >> 1][0],
+                                                       rq[mt][i >> 1][1], cd[i & 1], pd[i & 1], cvl, tc);
+                            if (hasc) {
 #pragma unroll
-                                for (int e = 0; e < 2; e++) {
-                                    const int i = 2 * hh + e;
-                                    const int row = 16 * mt + g + 8 * hh;
-                                    float S = tc_cell(acc[0][i], acc[1][i], acc[2][i], rq[mt][hh][0], rq[mt][hh][1],
-                                                      cd[e], pd[e], cvl, tc);
-                                    if (hasc) {
-                                        const int rr = 32 * s + row, cc = 32 * m + cl + e;
-                                        if (cc <= corner_a(rr, Lq, edge) || cc >= corner_b(rr, L, edge)) S = -9.f;
-                                    }
-                                    ring[((cl + e + row) ^ ((m & 1) << 5)) * P1T_RLD + row] = S;   // (32 m + cl + e + row) & 63
+                                for (int i = 0; i < 4; i++) {
+                                    const int rr = 32 * s + 16 * mt + g + 8 * (i >> 1), cc = 32 * m + cl + (i & 1);
+                                    if (cc <= corner_a(rr, Lq, edge) || cc >= corner_b(rr, L, edge)) S[i] = -9.f;
                                 }
+                            }
+#pragma unroll
+                            for (int i = 0; i < 4; i++) {
+                                const int row = 16 * mt + g + 8 * (i >> 1);
+                                // anti-diagonal (32 m + cl + e + row) & 63
+                                ring[((cl + (i & 1) + row) ^ ((m & 1) << 5)) * P1T_RLD + row] = S[i];
+                            }
                         }
                     }
                 }
@@ -1533,8 +1548,9 @@ int p1t_blocks_per_sm(int cvcard, cudaError_t* err)
 {
     int n = 0;
     const size_t sm = p1t_smem_bytes(cvcard);
-    cudaError_t e = cudaFuncSetAttribute(p1t_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, p1t_kernel, P1T_WARPS * 32, sm);
+    cudaError_t e = cudaFuncSetAttribute(p1t_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(p1t_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, p1t_kernel<true>, P1T_WARPS * 32, sm);
     if (err) *err = e;
     return n;
 }
@@ -1577,8 +1593,13 @@ cudaError_t launch_p1(const P1Args& a, const float* qbkg, int which, int grid, c
 {
     if (which == P1K_TENSOR) {
         const size_t sm = p1t_smem_bytes(a.sc.cvcard);
-        cudaFuncSetAttribute(p1t_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        p1t_kernel<<<grid, P1T_WARPS * 32, sm, st>>>(a, qbkg);
+        if (a.tc.uniform) {
+            cudaFuncSetAttribute(p1t_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            p1t_kernel<true><<<grid, P1T_WARPS * 32, sm, st>>>(a, qbkg);
+        } else {
+            cudaFuncSetAttribute(p1t_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            p1t_kernel<false><<<grid, P1T_WARPS * 32, sm, st>>>(a, qbkg);
+        }
         return cudaGetLastError();
     }
     if (which == P1K_CHUNKED) {
