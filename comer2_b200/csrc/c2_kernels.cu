@@ -1380,7 +1380,9 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
 #pragma unroll
                                 for (int i = 0; i < 4; i++) {
                                     const int rr = 32 * s + 16 * mt + g + 8 * (i >> 1), cc = 32 * m + cl + (i & 1);
-                                    if (cc <= corner_a(rr, Lq, edge) || cc >= corner_b(rr, L, edge)) S[i] = -9.f;
+                                    // (padding columns past L keep -inf)
+                                    if (cc < L && (cc <= corner_a(rr, Lq, edge) || cc >= corner_b(rr, L, edge)))
+                                        S[i] = -9.f;
                                 }
                             }
 #pragma unroll
@@ -1393,10 +1395,14 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                     }
                 }
                 __syncwarp();
-                // ---- DP stage: wavefront steps [32m, 32m + 32)
+                // ---- DP stage: wavefront steps [32m, 32m + 32).  A full stage
+                // after the first runs without bounds checks also where it passes
+                // the matrix edge: the last chunk's padding columns (zero operands)
+                // score -inf, so MM stays 0 there, and their other states reach
+                // only cells past the edge
                 const int k0 = 32 * m, k1 = min(k0 + 32, kend);
                 const float* tcol = cring + ((k0 - lane + P1T_CMOD) % P1T_CMOD) * P1C_TRS;
-                if (m >= 1 && k0 + 31 < L && k1 == k0 + 32)
+                if (m >= 1 && k1 == k0 + 32)
                     wf_steps<false, P1T_RLD, true, 0>(D, k0, 32, lane, L, act, ring, tcol, bnd, wr_bot);
                 else
                     wf_steps<true, P1T_RLD, true, 0>(D, k0, k1 - k0, lane, L, act, ring, tcol, bnd, wr_bot);

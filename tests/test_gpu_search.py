@@ -153,3 +153,27 @@ def test_hits_arrays_match_dicts(params):
         o, L = int(r["aln_offset"]), int(r["alnlen"])
         assert [raw[o + k * (L + 1):o + k * (L + 1) + L].decode() for k in range(5)] == x["strings"]
     h.close()
+
+
+def test_bf16_form_with_a_cv_table_off_its_index_range(params):
+    """A CV table whose key range is narrower than its index clamp (keys moved
+    by +1) takes the tensor kernel's explicit range tests; its hits must equal
+    the FP32 form's."""
+    import copy
+    from comer2_b200.native import Handle
+    p = copy.deepcopy(params)
+    p.cvs2s_keys = np.asarray(p.cvs2s_keys, np.float32) + np.float32(1.0)
+    w = S.config(1, seed=4, scale=0.003)
+    out = []
+    for mode in (0, 1):
+        h = Handle(p, 0)
+        h.set_score_mode(mode)
+        h.upload_db(w.db)
+        rec, alns = h.search(w.queries[0], arrays=True)
+        out.append((rec, bytes(alns)))
+    (r0, a0), (r1, a1) = out
+    assert len(r0) > 0
+    assert list(r0["profile"]) == list(r1["profile"])
+    assert np.allclose(r0["score"], r1["score"], rtol=1e-4, atol=1e-4)
+    assert np.allclose(r0["logE"], r1["logE"], atol=1e-3)
+    assert a0 == a1
