@@ -931,6 +931,17 @@ __device__ __forceinline__ void bf16_split(float x, unsigned& hi, unsigned& lo)
 }
 
 // D += A * B, m16n8k16, BF16 inputs, FP32 accumulation
+// first product of a chain: C = 0 (no accumulator zeroing)
+__device__ __forceinline__ void mma_bf16_z(float* d, const unsigned* a, unsigned b0, unsigned b1)
+{
+    const float z = 0.f;
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%10,%10,%10,%10};\n"
+        : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1), "f"(z));
+}
+
 __device__ __forceinline__ void mma_bf16(float* d, const unsigned* a, unsigned b0, unsigned b1)
 {
     asm volatile(
@@ -1348,12 +1359,9 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                         for (int mt = 0; mt < 2; mt++) {
                             float acc[3][4];
 #pragma unroll
-                            for (int d = 0; d < 3; d++)
-#pragma unroll
-                                for (int i = 0; i < 4; i++) acc[d][i] = 0.f;
-#pragma unroll
                             for (int kt = 0; kt < 2; kt++) {
-                                mma_bf16(acc[0], Aaa[mt][kt][1], B[0][kt][0].x, B[0][kt][0].y);
+                                if (kt == 0) mma_bf16_z(acc[0], Aaa[mt][kt][1], B[0][kt][0].x, B[0][kt][0].y);
+                                else mma_bf16(acc[0], Aaa[mt][kt][1], B[0][kt][0].x, B[0][kt][0].y);
                                 mma_bf16(acc[0], Aaa[mt][kt][0], B[0][kt][1].x, B[0][kt][1].y);
                                 mma_bf16(acc[0], Aaa[mt][kt][0], B[0][kt][0].x, B[0][kt][0].y);
                             }
@@ -1365,7 +1373,8 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                                 for (int kt = 0; kt < 2; kt++) {
                                     const unsigned* Ah = Q + (((d - 1) * 2 + kt) * 2 + 0) * 4;
                                     const unsigned* Al = Q + (((d - 1) * 2 + kt) * 2 + 1) * 4;
-                                    mma_bf16(acc[d], Al, B[d][kt][0].x, B[d][kt][0].y);
+                                    if (kt == 0) mma_bf16_z(acc[d], Al, B[d][kt][0].x, B[d][kt][0].y);
+                                    else mma_bf16(acc[d], Al, B[d][kt][0].x, B[d][kt][0].y);
                                     mma_bf16(acc[d], Ah, B[d][kt][1].x, B[d][kt][1].y);
                                     mma_bf16(acc[d], Ah, B[d][kt][0].x, B[d][kt][0].y);
                                 }

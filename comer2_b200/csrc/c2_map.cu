@@ -37,7 +37,15 @@ __device__ __forceinline__ float flog(float x)
     return (float)(__float_as_int(x) - 1064631197) * 8.2629582959339e-08f;
 }
 
-__device__ __forceinline__ float hmax(float a, float b) { return a < b ? b : a; }
+// maximum of two (inputs are never NaN here; a +0/-0 tie, the only case where
+// fmaxf and the reference's a < b ? b : a differ, gives the same sums below)
+__device__ __forceinline__ float hmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ float hmax3(float a, float b, float c)
+{
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
 
 __device__ __forceinline__ float lse2(float a, float b)
 {
@@ -48,8 +56,7 @@ __device__ __forceinline__ float lse2(float a, float b)
 // log(sum of five terms + 1): the 1 is the local start (forward) or end (backward)
 __device__ __forceinline__ float lse5p1(float v1, float v2, float v3, float v4, float v5)
 {
-    float mx = 0.f;
-    mx = hmax(mx, v1); mx = hmax(mx, v2); mx = hmax(mx, v3); mx = hmax(mx, v4); mx = hmax(mx, v5);
+    const float mx = hmax(hmax3(0.f, v1, v2), hmax3(v3, v4, v5));
     return flog(fexp(v1 - mx) + fexp(v2 - mx) + fexp(v3 - mx) + fexp(v4 - mx) + fexp(v5 - mx) + fexp(-mx)) + mx;
 }
 
