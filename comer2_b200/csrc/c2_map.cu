@@ -109,6 +109,7 @@ __device__ __forceinline__ void trn_bwd(const float* __restrict__ t0, int i, int
 // [k - 31, k]; chunk m (columns [32m, 32m + 32)) is written at the end of
 // step 32m - 1, into the half of chunk m - 2, whose last use was step 32m - 2.
 constexpr int MTRS = 12;
+constexpr int MAPFB_WARP_FLOATS = 2 * 32 * 33 + 64 * MTRS + 32 * 8;   // 12,544 B, a multiple of 16
 
 template <bool BWD>
 __device__ __forceinline__ void map_trn_col(const float* __restrict__ t0, int j, int L, float* t7)
@@ -192,7 +193,7 @@ __device__ __forceinline__ void pf_scores(const MapArgs& a, const MapPair& P, in
 __device__ __forceinline__ void map_fwd_item(const MapArgs& a, const float* __restrict__ qtrn,
                                              const float* __restrict__ dtrn, const float* __restrict__ qcf, int m,
                                              int s, int lane, float (*rin)[33], float (*rout)[33], float* trs,
-                                             bool& broken)
+                                             float* rab, bool& broken)
 {
     const int Lq = a.Lq;
     const int nstrips = (Lq + 31) >> 5;
@@ -230,13 +231,20 @@ __device__ __forceinline__ void map_fwd_item(const MapArgs& a, const float* __re
             float t7[7];
 #pragma unroll
             for (int i = 0; i < 7; i++) t7[i] = MLOG0;
-            // row above the strip, one chunk at a time (lane i: column 32 c + i),
-            // waited for and loaded at the end of the chunk before
-            float bcur[5];
+            // row above the strip, one chunk at a time, in the warp's shared
+            // buffer rab[32][8] (slot i: column 32 c + i), waited for and loaded
+            // at the end of the chunk before
             const float binit[5] = {0.f, MLOG0, MLOG0, MLOG0, MLOG0};
             if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken);
+            {
+                float v[5];
 #pragma unroll
-            for (int f = 0; f < 5; f++) bcur[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : binit[f];
+                for (int f = 0; f < 5; f++) v[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : binit[f];
+                __syncwarp();
+                *reinterpret_cast<float4*>(rab + lane * 8) = make_float4(v[0], v[1], v[2], v[3]);
+                rab[lane * 8 + 4] = v[4];
+                __syncwarp();
+            }
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             // column k's score is loaded one step ahead, from L2: each chunk's
             // columns are prefetched a chunk earlier
@@ -257,23 +265,28 @@ __device__ __forceinline__ void map_fwd_item(const MapArgs& a, const float* __re
                 up.ND = __shfl_up_sync(FULL, mine.ND, 1);
                 {
                     const int src = k & 31;
-                    const float b0 = __shfl_sync(FULL, bcur[0], src), b1 = __shfl_sync(FULL, bcur[1], src);
-                    const float b2 = __shfl_sync(FULL, bcur[2], src), b3 = __shfl_sync(FULL, bcur[3], src);
-                    const float b4 = __shfl_sync(FULL, bcur[4], src);
-                    if (lane == 0) up = S5{b0, b1, b2, b3, b4};
+                    const float4 ba = *reinterpret_cast<const float4*>(rab + src * 8);
+                    const float b4 = rab[src * 8 + 4];
+                    if (lane == 0) up = S5{ba.x, ba.y, ba.z, ba.w, b4};
                     if (src == 31) {
                         if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken);
+                        float v[5];
 #pragma unroll
                         for (int f = 0; f < 5; f++) {
                             const int cc = k + 1 + lane;
-                            bcur[f] = (s > 0 && cc < L) ? __ldcg(botr + f * L + cc) : binit[f];
+                            v[f] = (s > 0 && cc < L) ? __ldcg(botr + f * L + cc) : binit[f];
                         }
+                        __syncwarp();
+                        *reinterpret_cast<float4*>(rab + lane * 8) = make_float4(v[0], v[1], v[2], v[3]);
+                        rab[lane * 8 + 4] = v[4];
                     }
                 }
                 __syncwarp();
                 const int j = k - lane;
                 S5 left = mine, diag = upp;
-                if (j == 0) { left = LB; diag = DB; }
+                if (k < 32) {   // column 0 is within a strip's first 32 steps
+                    if (j == 0) { left = LB; diag = DB; }
+                }
                 const float sc = (j >= 0 && j < L) ? rin[j & 31][lane] : MLOG0;
                 S5 nw;
                 nw.MM = lse5p1(((diag.MI + q7[TMM]) + t7[TIM]) + sc, ((diag.IM + q7[TIM]) + t7[TMM]) + sc,
@@ -347,7 +360,8 @@ __global__ void __launch_bounds__(256) map_z_kernel(MapArgs a)
 // B.MM to fb, giving F+B per cell.  Work items are (pair, mirrored strip).
 __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __restrict__ qtrn,
                                              const float* __restrict__ dtrn, int m, int s, int lane,
-                                             float (*rin)[33], float (*rout)[33], float* trs, bool& broken)
+                                             float (*rin)[33], float (*rout)[33], float* trs, float* rab,
+                                             bool& broken)
 {
     const int Lq = a.Lq;
     const int nstrips = (Lq + 31) >> 5;
@@ -381,13 +395,20 @@ __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __re
             float t7[7];
 #pragma unroll
             for (int i = 0; i < 7; i++) t7[i] = MLOG0;
-            // row above the strip, one chunk at a time (lane i: column 32 c + i),
-            // waited for and loaded at the end of the chunk before
-            float bcur[5];
+            // row above the strip, one chunk at a time, in the warp's shared
+            // buffer rab[32][8] (slot i: column 32 c + i), waited for and loaded
+            // at the end of the chunk before
             const float binit[5] = {0.f, MLOG0, MLOG0, MLOG0, MLOG0};
             if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken);
+            {
+                float v[5];
 #pragma unroll
-            for (int f = 0; f < 5; f++) bcur[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : binit[f];
+                for (int f = 0; f < 5; f++) v[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : binit[f];
+                __syncwarp();
+                *reinterpret_cast<float4*>(rab + lane * 8) = make_float4(v[0], v[1], v[2], v[3]);
+                rab[lane * 8 + 4] = v[4];
+                __syncwarp();
+            }
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             const bool hasdn = act && r + 1 < Lq;
             // the diagonal-successor score of mirrored column k is loaded one step
@@ -420,22 +441,27 @@ __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __re
                 dn.ND = __shfl_up_sync(FULL, mine.ND, 1);
                 {
                     const int src = k & 31;
-                    const float b0 = __shfl_sync(FULL, bcur[0], src), b1 = __shfl_sync(FULL, bcur[1], src);
-                    const float b2 = __shfl_sync(FULL, bcur[2], src), b3 = __shfl_sync(FULL, bcur[3], src);
-                    const float b4 = __shfl_sync(FULL, bcur[4], src);
-                    if (lane == 0) dn = S5{b0, b1, b2, b3, b4};
+                    const float4 ba = *reinterpret_cast<const float4*>(rab + src * 8);
+                    const float b4 = rab[src * 8 + 4];
+                    if (lane == 0) dn = S5{ba.x, ba.y, ba.z, ba.w, b4};
                     if (src == 31) {
                         if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken);
+                        float v[5];
 #pragma unroll
                         for (int f = 0; f < 5; f++) {
                             const int cc = k + 1 + lane;
-                            bcur[f] = (s > 0 && cc < L) ? __ldcg(botr + f * L + cc) : binit[f];
+                            v[f] = (s > 0 && cc < L) ? __ldcg(botr + f * L + cc) : binit[f];
                         }
+                        __syncwarp();
+                        *reinterpret_cast<float4*>(rab + lane * 8) = make_float4(v[0], v[1], v[2], v[3]);
+                        rab[lane * 8 + 4] = v[4];
                     }
                 }
                 __syncwarp();
                 S5 rt = mine, dg = upp;         // successor to the right, diagonal successor
-                if (j == 0) { rt = INIT; dg = INIT; }
+                if (k < 32) {   // mirrored column 0 is within a strip's first 32 steps
+                    if (j == 0) { rt = INIT; dg = INIT; }
+                }
                 S5 nw;
                 nw.MM = lse5p1((dn.MI + q7[TMM]) + t7[TMI], (rt.IM + q7[TMI]) + t7[TMM], dn.DN + q7[TMD],
                                rt.ND + t7[TMD], ((dg.MM + q7[TMM]) + t7[TMM]) + sco);
@@ -473,9 +499,15 @@ __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __re
 __global__ void __launch_bounds__(MAPW * 32) map_fb_kernel(MapArgs a, const float* __restrict__ qtrn,
                                                      const float* __restrict__ dtrn, const float* __restrict__ qcf)
 {
-    __shared__ float rings[MAPW][2][32][33];
-    __shared__ __align__(16) float trings[MAPW][64 * MTRS];
+    // per warp: score ring, output ring [32][33] each, column transitions
+    // [64][MTRS], row above the strip for the current chunk [32][8]
+    extern __shared__ __align__(16) float fbsm[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float* wsm = fbsm + wid * MAPFB_WARP_FLOATS;
+    float(*rin)[33] = reinterpret_cast<float(*)[33]>(wsm);
+    float(*rout)[33] = reinterpret_cast<float(*)[33]>(wsm + 32 * 33);
+    float* trs = wsm + 2 * 32 * 33;
+    float* rab = trs + 64 * MTRS;
     const int nstrips = (a.Lq + 31) >> 5;
     const int nitems = 2 * a.nmap * nstrips;
     bool broken = false;
@@ -488,9 +520,9 @@ __global__ void __launch_bounds__(MAPW * 32) map_fb_kernel(MapArgs a, const floa
         const int m = iv / nstrips, s = iv - m * nstrips;
         __syncwarp();
         if (item & 1)
-            map_bwd_item(a, qtrn, dtrn, m, s, lane, rings[wid][0], rings[wid][1], trings[wid], broken);
+            map_bwd_item(a, qtrn, dtrn, m, s, lane, rin, rout, trs, rab, broken);
         else
-            map_fwd_item(a, qtrn, dtrn, qcf, m, s, lane, rings[wid][0], rings[wid][1], trings[wid], broken);
+            map_fwd_item(a, qtrn, dtrn, qcf, m, s, lane, rin, rout, trs, rab, broken);
         __syncwarp();
     }
 }
@@ -791,7 +823,10 @@ cudaError_t launch_map(const MapArgs& a, const float* qtrn, const float* dtrn, c
     if ((e = reset()) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(a.prog_b, 0, progb, st)) != cudaSuccess) return e;
     const int gfb = (int)std::min<long long>(grid, (2 * nitems + MAPW - 1) / MAPW);
-    map_fb_kernel<<<gfb, MAPW * 32, 0, st>>>(a, qtrn, dtrn, qcf);
+    const size_t fbs = (size_t)MAPW * MAPFB_WARP_FLOATS * sizeof(float);
+    if ((e = cudaFuncSetAttribute(map_fb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fbs)) != cudaSuccess)
+        return e;
+    map_fb_kernel<<<gfb, MAPW * 32, fbs, st>>>(a, qtrn, dtrn, qcf);
     map_z_kernel<<<a.nmap, 256, 0, st>>>(a);
     if ((e = reset()) != cudaSuccess) return e;
     map_dp_kernel<<<g, MAPW * 32, 0, st>>>(a);
