@@ -1514,7 +1514,8 @@ extern "C" c2_status c2_search_batch(c2_handle* h, const c2_profiles* queries, i
     std::vector<c2_handle*> ws(1, h);
     for (int i = 0; i < nw - 1; i++) ws.push_back(h->workers[i]);
     std::atomic<int> next(0);
-    std::mutex mu;   // serialises the callbacks and the first error
+    std::mutex mu;       // serialises the callbacks and the first error
+    std::mutex gpu_mu;   // one query's kernel sequence at a time (see below)
     c2_status first = C2_OK;
     std::string first_err;
     auto run = [&](c2_handle* w) {
@@ -1527,7 +1528,21 @@ extern "C" c2_status c2_search_batch(c2_handle* h, const c2_profiles* queries, i
             const c2_profiles v = query_view(queries, q, &zero);
             int32_t nh = 0;
             size_t nb = 0;
-            c2_status s = c2_search(w, &v, &nh);
+            // The query's host-side preparation, and below its hit copy and
+            // callback, overlap other workers; its kernels run alone: the
+            // phase-1 kernels hold every SM with one persistent CTA, and a
+            // strip-pipelined phase-2 sweep started beside them would run on
+            // the few SMs left and stall its own chains.
+            c2_status s = c2_set_query(w, &v);
+            if (s == C2_OK) {
+                std::lock_guard<std::mutex> g(gpu_mu);
+                int32_t n = 0;
+                if (s == C2_OK) s = c2_run_phase1(w);
+                if (s == C2_OK) s = c2_run_finalize(w, &n);
+                if (s == C2_OK) s = c2_run_stats(w, &n);
+                if (s == C2_OK) s = c2_run_map(w, &nh);
+                if (s == C2_OK && cudaStreamSynchronize(w->stream) != cudaSuccess) s = C2_ERR_CUDA;
+            }
             if (s == C2_OK) s = c2_get_hits(w, nullptr, 0, nullptr, &nb);
             if (s == C2_OK) {
                 hits.resize(std::max(1, nh));

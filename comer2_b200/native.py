@@ -438,7 +438,7 @@ class Handle:
         self._ck(self.lib.c2_search(self._h, C.byref(s), C.byref(n)), "c2_search")
         return self.hits_arrays(n.value) if arrays else self.hits(n.value)
 
-    def search_batch(self, queries: ProfileSet, nworkers: int = 2):
+    def search_batch(self, queries: ProfileSet, nworkers: int = 1):
         """Search every profile of queries over the uploaded database with nworkers
         worker handles sharing it (c2_search_batch).  Returns one (records,
         alignments) pair per query, as hits_arrays() gives them."""
