@@ -16,6 +16,8 @@ method (the C restatement, float, one thread per host core) on a bounded
 sample of the same workload; the reference has no CPU search path of its own.
 Multi-GPU runs (torchrun) give every rank its own database of the same size
 (weak scaling, no collective on the data path); times are the max over ranks.
+--workload 0 / 4 measure the other single-query configurations the same way;
+--workload 2 times the 64-query configuration end to end through the batch call.
 """
 import argparse
 import json
@@ -33,6 +35,13 @@ sys.path.insert(0, ROOT)
 METRIC = "GCUPS (score+DP+MAP)"
 UNIT = "GCUPS"
 WORKLOAD = "1 query L=400 vs 100000 db profiles LN(200,0.6)[30,2000], 2% planted homologs"
+# --workload n: the synthetic configuration n (synth.config); 1 is the headline
+WORKLOADS = {
+    0: "1 query L=150 vs 2000 db profiles U[50,500]",
+    1: WORKLOAD,
+    2: "64 queries LN(250,0.6)[50,1500] vs 20000 db profiles LN(200,0.6)[30,2000], 2% homologs of query 0",
+    4: "1 query L=3000 (6 domains) vs 50000 db profiles LN(300,0.6)[30,2000], 5% planted homologs",
+}
 
 
 def _peaks():
@@ -150,6 +159,45 @@ def cpu_port_gcups(w, params, seconds=12.0, threads=None):
         len(ks), w.db.nprofiles, cells)
 
 
+def batch_workload(args):
+    """Configuration 2: 64 queries through c2_search_batch, timed end to end
+    (queries from host memory, every query's hits and alignments back)."""
+    import torch
+    from comer2_b200 import params as P, synth as S
+    from comer2_b200.native import Handle, SCORE_BF16_TC, SCORE_FP32, C2Error  # noqa: F401
+    prm = P.load_default()
+    w = S.config(2, seed=0, scale=args.scale)
+    qs = S.concat(w.queries)
+    cells = float(qs.npositions) * float(w.db.npositions)
+    h = Handle(prm, 0)
+    h.upload_db(w.db)
+    out = {}
+    for name, mode in (("bf16", SCORE_BF16_TC), ("fp32", SCORE_FP32)):
+        h.set_score_mode(mode)
+        for _ in range(max(1, args.warmup)):
+            h.search_batch(S.concat(w.queries[:4]))
+        ts, nh = [], 0
+        for _ in range(max(1, args.steps)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = h.search_batch(qs)
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+            nh = int(sum(len(x[0]) for x in r))
+        out[name] = {"value": cells / float(np.mean(ts)) / 1e9, "s_per_step": float(np.mean(ts)), "hits": nh}
+    main_r = out[args.score_mode]
+    line = {"metric": METRIC, "value": main_r["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": main_r["s_per_step"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16" if args.score_mode == "bf16" else "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOADS[2], "queries": len(w.queries), "cells": cells, "scale": args.scale,
+                       "timing": "end to end through c2_search_batch (one worker)"},
+            "e2e": {"value": main_r["value"], "unit": UNIT}, "hits": main_r["hits"],
+            "score_forms": out}
+    print(json.dumps(line))
+    h.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -161,7 +209,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--score-mode", default="bf16", choices=["fp32", "bf16"],
                     help="phase-1 score contractions: FP32 CUDA cores or split-BF16 tensor cores")
+    ap.add_argument("--workload", type=int, default=1, choices=sorted(WORKLOADS),
+                    help="synthetic configuration (1: the headline; 2: 64 queries through the batch call)")
     args = ap.parse_args()
+    if args.workload == 2:
+        return batch_workload(args)
+    if args.workload != 1:
+        global WORKLOAD
+        WORKLOAD = WORKLOADS[args.workload]
     world, rank, local = _dist()
     from comer2_b200 import params as P, synth as S
     prm = P.load_default()
@@ -169,7 +224,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        w = S.config(1, seed=0, scale=args.scale)
+        w = S.config(args.workload, seed=0, scale=args.scale)
         vals = []
         thr = samp = None
         for _ in range(max(1, args.steps)):
@@ -196,7 +251,7 @@ def main():
     torch.cuda.set_device(local)
     from comer2_b200.native import Handle
 
-    w = S.config(1, seed=rank, scale=args.scale)
+    w = S.config(args.workload, seed=rank, scale=args.scale)
     q = w.queries[0]
     Lq = int(q.lengths[0])
     cells = Lq * int(w.db.lengths.sum())
