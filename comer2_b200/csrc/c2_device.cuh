@@ -130,6 +130,7 @@ struct P1Args {
     int* counter;           // work-queue head
     const float* ssss;      // [card][card]
     const float* cvvals;    // [cvcard]
+    const float* qU;        // [strip][MAX_SSSS_CARD][32] SS row tables of the query rows
     ScoreConsts sc;
     float* bot;             // strip-boundary rows: per warp slot 2 x 5 x Lmax
     long long botstride;    // floats per warp slot

@@ -104,7 +104,7 @@ struct c2_handle {
     int Lq = 0;
     float qeno = 0.f;
     std::vector<float> h_qrec;
-    DevBuf<float> d_qrec, d_qbkg, d_qtrn, d_qcf, d_qcfx;
+    DevBuf<float> d_qrec, d_qbkg, d_qtrn, d_qcf, d_qcfx, d_qU;
     // differentiable alignment (c2_logz_fwd / c2_logz_bwd)
     std::vector<int> adj_prof;
     std::vector<long long> adj_off;
@@ -613,6 +613,17 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
                 U[(size_t)r * 32 + c] = s3[0] * h->ssss[(size_t)i0 * card + c] + s3[1] * h->ssss[(size_t)i1 * card + c] +
                                         s3[2] * h->ssss[(size_t)i2 * card + c];
         }
+        // the same tables per strip, [strip][MAX_SSSS_CARD][32] (lane = row), for
+        // the FP32 kernels
+        {
+            std::vector<float> qU((size_t)ns * MAX_SSSS_CARD * 32, 0.f);
+            for (int r = 0; r < Lq; r++)
+                for (int c = 0; c < card; c++)
+                    qU[((size_t)(r / 32) * MAX_SSSS_CARD + c) * 32 + (r % 32)] = U[(size_t)r * 32 + c];
+            if (h->d_qU.ensure(qU.size())) return fail(h, C2_ERR_NOMEM, "query SS table allocation failed");
+            CK(cudaMemcpyAsync(h->d_qU.p, qU.data(), qU.size() * 4, cudaMemcpyHostToDevice, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+        }
         auto aval = [&](int d, int r, int k) -> float {
             if (r >= Lq) return 0.f;
             if (d == 0) return k < NCV ? q->cv[(size_t)r * NCV + k] : (k == NCV ? 1.f : 0.f);
@@ -810,6 +821,7 @@ static void fill_p1(c2_handle* h, P1Args& a)
     a.counter = h->d_counter.p;
     a.ssss = h->d_ssss.p;
     a.cvvals = h->d_cvvals.p;
+    a.qU = h->d_qU.p;
     a.sc = h->sc;
     a.bot = h->d_bot.p;
     a.botstride = h->botstride;

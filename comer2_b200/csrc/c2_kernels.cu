@@ -198,11 +198,10 @@ p1_kernel(P1Args a, const float* __restrict__ qbkg)
             R.pq = qr[QR_PRIOR];
             R.hq = qr[QR_HQ];
             {
-                const float q0 = qr[QR_SS], q1 = qr[QR_SS + 1], q2 = qr[QR_SS + 2];
-                const int i0 = (int)(q0 * 9.999f), i1 = 10 + (int)(q1 * 9.999f), i2 = 20 + (int)(q2 * 9.999f);
-                for (int c = 0; c < card; c++)
-                    U[c * 32 + lane] = q0 * __ldg(a.ssss + i0 * card + c) + q1 * __ldg(a.ssss + i1 * card + c) +
-                                       q2 * __ldg(a.ssss + i2 * card + c);
+                // this strip's SS row tables (built once per query, c2_set_query)
+                const float* __restrict__ us = a.qU + (long long)s * MAX_SSSS_CARD * 32 + lane;
+#pragma unroll 8
+                for (int c = 0; c < card; c++) U[c * 32 + lane] = __ldg(us + c * 32);
             }
             float q7[7];
 #pragma unroll
@@ -416,11 +415,10 @@ p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
             R.pq = qr[QR_PRIOR];
             R.hq = qr[QR_HQ];
             {
-                const float q0 = qr[QR_SS], q1 = qr[QR_SS + 1], q2 = qr[QR_SS + 2];
-                const int i0 = (int)(q0 * 9.999f), i1 = 10 + (int)(q1 * 9.999f), i2 = 20 + (int)(q2 * 9.999f);
-                for (int c = 0; c < card; c++)
-                    U[c * 32 + lane] = q0 * __ldg(a.ssss + i0 * card + c) + q1 * __ldg(a.ssss + i1 * card + c) +
-                                       q2 * __ldg(a.ssss + i2 * card + c);
+                // this strip's SS row tables (built once per query, c2_set_query)
+                const float* __restrict__ us = a.qU + (long long)s * MAX_SSSS_CARD * 32 + lane;
+#pragma unroll 8
+                for (int c = 0; c < card; c++) U[c * 32 + lane] = __ldg(us + c * 32);
             }
             float q7[7];
 #pragma unroll
@@ -798,11 +796,10 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
             R.pq = qr[QR_PRIOR];
             R.hq = qr[QR_HQ];
             {
-                const float q0 = qr[QR_SS], q1 = qr[QR_SS + 1], q2 = qr[QR_SS + 2];
-                const int i0 = (int)(q0 * 9.999f), i1 = 10 + (int)(q1 * 9.999f), i2 = 20 + (int)(q2 * 9.999f);
-                for (int c = 0; c < card; c++)
-                    U[c * 32 + lane] = q0 * __ldg(a.ssss + i0 * card + c) + q1 * __ldg(a.ssss + i1 * card + c) +
-                                       q2 * __ldg(a.ssss + i2 * card + c);
+                // this strip's SS row tables (built once per query, c2_set_query)
+                const float* __restrict__ us = a.qU + (long long)s * MAX_SSSS_CARD * 32 + lane;
+#pragma unroll 8
+                for (int c = 0; c < card; c++) U[c * 32 + lane] = __ldg(us + c * 32);
             }
             WfLane D;
             float q7[7];
