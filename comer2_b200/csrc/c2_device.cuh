@@ -91,23 +91,26 @@ __host__ __device__ constexpr int dpt_src(int i) { return (int)((DPT_SRC >> (4 *
 // ring of 64 columns x 32 rows, a transition ring of 64 columns (stride 12
 // floats: the two 16-byte reads of 8 lanes at consecutive columns cover 32
 // distinct banks), the SS row table, the record staging ring and the row
-// above the strip for the current chunk ([32][8])
+// above the strip for the current chunk
 constexpr int P1C_WARPS = 11;
 // phase-1 kernel variants of launch_p1
 enum : int { P1K_STRIP = 0, P1K_CHUNKED = 1, P1K_TRACEBACK = 2, P1K_TENSOR = 3 };
 constexpr int P1C_RING = 64, P1C_TRS = 12, P1C_CVREP = 16;
+// row above the strip in the shared-memory DP kernels: [32][4] + [32] floats
+constexpr int BND_ND = 32 * 4, BND_FLOATS = 32 * 5;
 constexpr int P1C_WARP_FLOATS =
-    P1C_RING * 32 + P1C_RING * P1C_TRS + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE + 32 * 8;
+    P1C_RING * 32 + P1C_RING * P1C_TRS + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE + BND_FLOATS;
 // tensor-core kernel: score ring of 64 anti-diagonals with 36 floats each (the
 // fragment-layout writes and the per-lane wavefront reads are both free of
 // bank conflicts), a column-record ring of 3 chunks plus a mirror of its first
 // chunk (slots 96..127), so that the 32 records a lane reads in one DP stage
-// never wrap, the row above the strip and two slots for db operand tiles
-// (bulk async copies, one mbarrier each)
-constexpr int P1T_WARPS = 10;
+// never wrap, the row above the strip and one slot for the db operand tile
+// (a bulk async copy, one mbarrier); 12 warps fit with a CV table of up to
+// 106 entries
+constexpr int P1T_WARPS = 12;
 constexpr int P1T_RLD = 36, P1T_CRING = 128, P1T_CMOD = 96, P1T_CVREP = 8;
 constexpr unsigned P1T_TMEM_COLS = 512;   // TMEM columns of a CTA (3 warps x 128 per lane quarter)
-constexpr int P1T_WARP_FLOATS = P1C_RING * P1T_RLD + P1T_CRING * P1C_TRS + 32 * 8 + 2 * TC_TILE_WORDS + 4;
+constexpr int P1T_WARP_FLOATS = P1C_RING * P1T_RLD + P1T_CRING * P1C_TRS + BND_FLOATS + TC_TILE_WORDS + 4;
 
 // Epilogue constants of the tensor-core form: x = 2 x (CV score argument)
 // = (2 pownu0 ln2) log2(det) + 2 cterm - 2 prior_q - 2 prior_d, compared

@@ -647,6 +647,14 @@ __device__ __forceinline__ void wf_init(WfLane& D, const float* q7, const St5& L
     D.kbest = 0;
 }
 
+// Row above the strip, 32 column slots: states MM, MI, IM, DN as a float4
+// per slot ([32][4]), ND after them ([32] at BND_ND)
+__device__ __forceinline__ void bnd_put(float* bnd, int slot, float mm, float mi, float im, float dn, float nd)
+{
+    *reinterpret_cast<float4*>(bnd + slot * 4) = make_float4(mm, mi, im, dn);
+    bnd[BND_ND + slot] = nd;
+}
+
 // Wavefront steps [k0, k0 + nst) of a strip (k0 a multiple of 32, nst <= 32;
 // 32 when !CHECK).  ring: diagonal-indexed scores, RLD floats per slot.
 // Column records (DPT_N transitions, P1C_TRS floats apart): with TMIRROR,
@@ -678,8 +686,8 @@ __device__ __forceinline__ void wf_steps(WfLane& D, int k0, int nst, int lane, i
         float uND = __shfl_up_sync(FULL, D.ND, 1);
         {
             // row above the strip at column k (lane 0's column), broadcast reads
-            const float4 ba = *reinterpret_cast<const float4*>(bnd + u * 8);
-            const float b4 = bnd[u * 8 + 4];
+            const float4 ba = *reinterpret_cast<const float4*>(bnd + u * 4);
+            const float b4 = bnd[BND_ND + u];
             if (lane == 0) { uMM = ba.x; uMI = ba.y; uIM = ba.z; uDN = ba.w; uND = b4; }
         }
         const int j = k0 + u - lane;
@@ -711,8 +719,7 @@ __device__ __forceinline__ void wf_steps(WfLane& D, int k0, int nst, int lane, i
         if (wr_bot) {
             // lane 31's cell (column k0 + u - 31) into the slot lane 0 read at
             // the top of this step; bot_flush stores the 32 columns per chunk
-            *reinterpret_cast<float4*>(bnd + u * 8) = make_float4(nMM, nMI, nIM, nDN);
-            bnd[u * 8 + 4] = nND;
+            bnd_put(bnd, u, nMM, nMI, nIM, nDN, nND);
         }
         D.MM = nMM; D.MI = nMI; D.IM = nIM; D.DN = nDN; D.ND = nND;
         D.X = X; D.Y = Y; D.z = z;
@@ -728,12 +735,12 @@ __device__ __forceinline__ void bot_flush(const float* __restrict__ bnd, float* 
 {
     const int c = k0 - 31 + lane;
     if (c >= 0 && c < L) {
-        const float4 a = *reinterpret_cast<const float4*>(bnd + lane * 8);
+        const float4 a = *reinterpret_cast<const float4*>(bnd + lane * 4);
         botw[0 * Lmax + c] = a.x;
         botw[1 * Lmax + c] = a.y;
         botw[2 * Lmax + c] = a.z;
         botw[3 * Lmax + c] = a.w;
-        botw[4 * Lmax + c] = bnd[lane * 8 + 4];
+        botw[4 * Lmax + c] = bnd[BND_ND + lane];
     }
 }
 
@@ -755,7 +762,7 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
     float* trn = ring + P1C_RING * 32;                        // [P1C_RING][P1C_TRS] transitions
     float* U = trn + P1C_RING * P1C_TRS;                      // [card][32]
     float* rec = U + MAX_SSSS_CARD * 32;                      // [REC_SLOTS][DR_STRIDE] db records
-    float* bnd = rec + REC_SLOTS * DR_STRIDE;                 // [32][8] row above the strip
+    float* bnd = rec + REC_SLOTS * DR_STRIDE;                 // [BND_FLOATS] row above the strip
     for (int i = threadIdx.x; i < cvcard * P1C_CVREP; i += blockDim.x) cvtab[i] = a.cvvals[i / P1C_CVREP];
     __syncthreads();
 
@@ -829,8 +836,7 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             __syncwarp();
             // columns [0, 32) of the row above, lane i holding column i
-            *reinterpret_cast<float4*>(bnd + lane * 8) = make_float4(bc[0], bc[1], bc[2], bc[3]);
-            bnd[lane * 8 + 4] = bc[4];
+            bnd_put(bnd, lane, bc[0], bc[1], bc[2], bc[3], bc[4]);
             stage_chunk(rec, dr, 0, L, lane);
             stage_chunk(rec, dr, 1, L, lane);
             const int nch = (L + 31) >> 5;        // chunks holding columns
@@ -871,8 +877,7 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
                 if (s + 1 < nstrips) bot_flush(bnd, botw, k0, L, Lmax, lane);
                 __syncwarp();
                 // next 32 columns of the row above the strip
-                *reinterpret_cast<float4*>(bnd + lane * 8) = make_float4(D.bnxt[0], D.bnxt[1], D.bnxt[2], D.bnxt[3]);
-                bnd[lane * 8 + 4] = D.bnxt[4];
+                bnd_put(bnd, lane, D.bnxt[0], D.bnxt[1], D.bnxt[2], D.bnxt[3], D.bnxt[4]);
 #pragma unroll
                 for (int f = 0; f < 5; f++) {
                     const int cc = k0 + 64 + lane;
@@ -1164,15 +1169,14 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
     float* wb = smem + cvcard * P1T_CVREP + wid * P1T_WARP_FLOATS;
     float* ring = wb;                                         // [64 anti-diagonals][P1T_RLD] scores
     float* cring = ring + P1C_RING * P1T_RLD;                 // [P1T_CRING][P1C_TRS] column records
-    float* bnd = cring + P1T_CRING * P1C_TRS;                 // [32][8] row above the strip
-    unsigned* btile = reinterpret_cast<unsigned*>(bnd + 32 * 8);   // [2][TC_TILE_WORDS] db operand tiles
-    unsigned long long* tbar = reinterpret_cast<unsigned long long*>(btile + 2 * TC_TILE_WORDS);  // [2]
+    float* bnd = cring + P1T_CRING * P1C_TRS;                 // [BND_FLOATS] row above the strip
+    unsigned* btile = reinterpret_cast<unsigned*>(bnd + BND_FLOATS);   // [TC_TILE_WORDS] db operand tile
+    unsigned long long* tbar = reinterpret_cast<unsigned long long*>(btile + TC_TILE_WORDS);
     for (int i = threadIdx.x; i < cvcard * P1T_CVREP; i += blockDim.x)
         cvtab[i] = a.cvvals[i / P1T_CVREP] * a.sc.cvswgt;
     __shared__ unsigned tmem_base;
     if (lane == 0) {
         mbar_init(tbar, 1);
-        mbar_init(tbar + 1, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     // query CV / SS A fragments of the current strip live in TMEM (64 columns
@@ -1182,7 +1186,7 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
     __syncthreads();
     tmem_fence_after();
     const unsigned tq = tmem_base + ((unsigned)(32 * (wid & 3)) << 16) + (unsigned)((wid >> 2) * 128);
-    unsigned tph0 = 0, tph1 = 0;   // phase parity of the two tile slots
+    unsigned tph = 0;   // phase parity of the tile slot's barrier
 
     const long long slotw = (long long)blockIdx.x * P1T_WARPS + wid;
     const int Lmax = (int)(a.botstride / 10);
@@ -1301,18 +1305,16 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
             }
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             __syncwarp();
-            *reinterpret_cast<float4*>(bnd + lane * 8) = make_float4(bc[0], bc[1], bc[2], bc[3]);
-            bnd[lane * 8 + 4] = bc[4];
+            bnd_put(bnd, lane, bc[0], bc[1], bc[2], bc[3], bc[4]);
             stage_cols(cring, cold, 0, L, lane);
             stage_cols(cring, cold, 1, L, lane);
             const int nch = (L + 31) >> 5;
             const int kend = L + 31;
-            // db operand tiles T = 4m + nt stream through the two slots, two tiles ahead
+            // db operand tiles T = 4m + nt stream through the slot, one tile ahead:
+            // tile T + 1 loads while tile T's products and epilogue run (and
+            // the first tile of a chunk during the DP stage before it)
             const int ntile = 4 * nch;
-            if (lane == 0) {
-                bulk_load(btile, tb0, TC_TILE_WORDS * 4, tbar);
-                bulk_load(btile + TC_TILE_WORDS, tb0 + TC_TILE_WORDS, TC_TILE_WORDS * 4, tbar + 1);
-            }
+            if (lane == 0) bulk_load(btile, tb0, TC_TILE_WORDS * 4, tbar);
             for (int m = 0; 32 * m < kend; m++) {
                 if (m < nch) {
                     cp_async_wait_1();   // column records of chunk m have landed
@@ -1330,11 +1332,11 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                     // ---- score stage: 32 x 32 tile of chunk m on the tensor cores
 #pragma unroll 1
                     for (int nt = 0; nt < 4; nt++) {
-                        const int T = 4 * m + nt, sl = T & 1;
-                        const bool got = mbar_wait(tbar + sl, sl ? tph1 : tph0);
-                        if (sl) tph1 ^= 1u; else tph0 ^= 1u;
+                        const int T = 4 * m + nt;
+                        const bool got = mbar_wait(tbar, tph);
+                        tph ^= 1u;
                         if (!got && lane == 0 && a.status) atomicCAS(a.status, 0, PIPE_ERR_TIMEOUT);
-                        const unsigned* bt = btile + sl * TC_TILE_WORDS + lane * 2;
+                        const unsigned* bt = btile + lane * 2;
                         uint2 B[3][2][2];
 #pragma unroll
                         for (int d = 0; d < 3; d++)
@@ -1343,11 +1345,13 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
 #pragma unroll
                                 for (int sp = 0; sp < 2; sp++)
                                     B[d][kt][sp] = *reinterpret_cast<const uint2*>(bt + ((d * 2 + kt) * 2 + sp) * 64);
-                        // slot free once every lane holds its fragments: tile T + 2 into it
+                        // slot free once every lane holds its fragments: tile T + 1 into it
                         __syncwarp();
-                        if (lane == 0 && T + 2 < ntile)
-                            bulk_load(btile + sl * TC_TILE_WORDS, tb0 + (long long)(T + 2) * TC_TILE_WORDS,
-                                      TC_TILE_WORDS * 4, tbar + sl);
+                        if (lane == 0 && T + 1 < ntile) {
+                            // the warp's reads of the slot before the async-proxy write
+                            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                            bulk_load(btile, tb0 + (long long)(T + 1) * TC_TILE_WORDS, TC_TILE_WORDS * 4, tbar);
+                        }
                         const int cl = 8 * nt + 2 * q;   // column within the chunk
                         const float* cr0 = cbase + cl * P1C_TRS;
                         const float cd[2] = {cr0[CO_CD], cr0[P1C_TRS + CO_CD]};
@@ -1415,8 +1419,7 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                 __syncwarp();
                 if (s + 1 < nstrips) bot_flush(bnd, botw, k0, L, Lmax, lane);
                 __syncwarp();
-                *reinterpret_cast<float4*>(bnd + lane * 8) = make_float4(D.bnxt[0], D.bnxt[1], D.bnxt[2], D.bnxt[3]);
-                bnd[lane * 8 + 4] = D.bnxt[4];
+                bnd_put(bnd, lane, D.bnxt[0], D.bnxt[1], D.bnxt[2], D.bnxt[3], D.bnxt[4]);
 #pragma unroll
                 for (int f = 0; f < 5; f++) {
                     const int cc = k0 + 64 + lane;
