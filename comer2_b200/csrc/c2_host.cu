@@ -26,7 +26,7 @@
 
 namespace c2 {
 cudaError_t launch_stats(const StatsArgs& a, cudaStream_t st);
-cudaError_t launch_map(const MapArgs& a, const float* qtrn, const float* dtrn, const float* qcf, int grid,
+cudaError_t launch_map(const MapArgs& a, const float* qtrn, const float* dtrn, const float* qcf, int nsm,
                        int* counter, cudaStream_t st, int* nlaunch);
 size_t p1_smem_bytes(int cvcard);
 cudaError_t launch_p1(const P1Args& a, const float* qbkg, int which, int grid, cudaStream_t st);
@@ -1180,10 +1180,7 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
     a.aln = h->d_aln.p;
     a.alnstride = h->alnstride;
     int nl = 0;
-    // the MAP sweeps run 4 warps per CTA, one boundary slot each: stay within
-    // the grid x P1_WARPS slots of the strip-boundary scratch
-    const int grid = h->grid * P1_WARPS / 4;
-    CK(launch_map(a, h->d_qtrn.p, h->db->d_dtrn.p, h->d_qcf.p, grid, h->d_counter.p, h->stream, &nl));
+    CK(launch_map(a, h->d_qtrn.p, h->db->d_dtrn.p, h->d_qcf.p, h->nsm, h->d_counter.p, h->stream, &nl));
     h->launches += nl;
     return C2_OK;
 }

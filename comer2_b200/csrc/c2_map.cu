@@ -23,7 +23,8 @@ namespace c2 {
 
 #define FULL 0xffffffffu
 constexpr float MLOG0 = -99.f;
-constexpr int MAPW = 4;   // warps per CTA of the MAP sweeps
+constexpr int MAPW = 4;     // warps per CTA of the MAP DP sweep
+constexpr int MAPFBW = 3;   // warps per CTA of the forward-backward sweeps (6 CTAs per SM fit)
 
 __device__ __forceinline__ float fexp(float x)
 {
@@ -496,7 +497,7 @@ __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __re
 // Forward and backward sweeps in one launch: the two are independent (the
 // backward sweep writes B beside F), so their strip chains run side by side;
 // item 2 i is the forward sweep's work item i, 2 i + 1 the backward one's.
-__global__ void __launch_bounds__(MAPW * 32) map_fb_kernel(MapArgs a, const float* __restrict__ qtrn,
+__global__ void __launch_bounds__(MAPFBW * 32) map_fb_kernel(MapArgs a, const float* __restrict__ qtrn,
                                                      const float* __restrict__ dtrn, const float* __restrict__ qcf)
 {
     // per warp: score ring, output ring [32][33] each, column transitions
@@ -802,14 +803,12 @@ cudaError_t launch_aln_pack(const char* aln, int alnstride, const int* info, con
     return cudaGetLastError();
 }
 
-cudaError_t launch_map(const MapArgs& a, const float* qtrn, const float* dtrn, const float* qcf, int grid,
+cudaError_t launch_map(const MapArgs& a, const float* qtrn, const float* dtrn, const float* qcf, int nsm,
                        int* counter, cudaStream_t st, int* nlaunch)
 {
     if (a.nmap <= 0) return cudaSuccess;
     const int nstrips = (a.Lq + 31) >> 5;
     const long long nitems = (long long)a.nmap * nstrips;
-    // grid: persistent CTAs of MAPW warps, at most one warp per work item
-    const int g = (int)std::min<long long>(grid, (nitems + MAPW - 1) / MAPW);
     const size_t progb = (size_t)nitems * sizeof(int);
     cudaError_t e;
     // per sweep: fresh work counter and strip progress words
@@ -818,15 +817,24 @@ cudaError_t launch_map(const MapArgs& a, const float* qtrn, const float* dtrn, c
         if (r == cudaSuccess) r = cudaMemsetAsync(a.prog, 0, progb, st);
         return r;
     };
+    // grids: persistent CTAs, as many as fit on the SMs at once (the strip
+    // pipeline is latency bound: every resident warp adds a wavefront in
+    // flight), at most one warp per work item
+    const size_t fbs = (size_t)MAPFBW * MAPFB_WARP_FLOATS * sizeof(float);
+    if ((e = cudaFuncSetAttribute(map_fb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fbs)) != cudaSuccess)
+        return e;
+    int ofb = 0, odp = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ofb, map_fb_kernel, MAPFBW * 32, fbs)) != cudaSuccess)
+        return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&odp, map_dp_kernel, MAPW * 32, 0)) != cudaSuccess)
+        return e;
+    const int gfb = (int)std::min<long long>((long long)std::max(ofb, 1) * nsm, (2 * nitems + MAPFBW - 1) / MAPFBW);
+    const int g = (int)std::min<long long>((long long)std::max(odp, 1) * nsm, (nitems + MAPW - 1) / MAPW);
     if ((e = cudaMemsetAsync(a.pairf, 0, (size_t)a.nmap * 4 * sizeof(float), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(a.pairk, 0, (size_t)a.nmap * sizeof(unsigned long long), st)) != cudaSuccess) return e;
     if ((e = reset()) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(a.prog_b, 0, progb, st)) != cudaSuccess) return e;
-    const int gfb = (int)std::min<long long>(grid, (2 * nitems + MAPW - 1) / MAPW);
-    const size_t fbs = (size_t)MAPW * MAPFB_WARP_FLOATS * sizeof(float);
-    if ((e = cudaFuncSetAttribute(map_fb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fbs)) != cudaSuccess)
-        return e;
-    map_fb_kernel<<<gfb, MAPW * 32, fbs, st>>>(a, qtrn, dtrn, qcf);
+    map_fb_kernel<<<gfb, MAPFBW * 32, fbs, st>>>(a, qtrn, dtrn, qcf);
     map_z_kernel<<<a.nmap, 256, 0, st>>>(a);
     if ((e = reset()) != cudaSuccess) return e;
     map_dp_kernel<<<g, MAPW * 32, 0, st>>>(a);
