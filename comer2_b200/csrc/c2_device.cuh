@@ -52,7 +52,6 @@ constexpr int REC_CHUNK = 8, REC_CHUNK_LOG = 3, REC_SLOTS = 16;
 // shared memory per warp: score ring [32][32], SS row table [32][32], record ring
 constexpr int P1_WARP_FLOATS = 32 * 32 + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE;
 constexpr int MAX_CVCARD = 256;
-constexpr int P1TB_CVREP = 16;   // CV table replicas of the traceback sweep
 // Tensor-core (BF16 split) phase-1 kernel.  The three contractions of a cell
 // score -- amino acids (K = 20), context vectors (K = 19) and the SS table
 // (K = card <= 32, the db side a 3-hot vector of SS probabilities) -- run as
@@ -100,6 +99,9 @@ constexpr int P1C_RING = 64, P1C_TRS = 12, P1C_CVREP = 16;
 constexpr int BND_ND = 32 * 4, BND_FLOATS = 32 * 5;
 constexpr int P1C_WARP_FLOATS =
     P1C_RING * 32 + P1C_RING * P1C_TRS + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE + BND_FLOATS;
+// chunked traceback sweep: p1c_kernel's per-warp layout plus a [32][33]-byte
+// traceback column ring; 11 warps per SM with CV table replicas of 8
+constexpr int P1TC_WARPS = 11, P1TC_CVREP = 8;
 // tensor-core kernel: score ring of 64 anti-diagonals with 36 floats each (the
 // fragment-layout writes and the per-lane wavefront reads are both free of
 // bank conflicts), a column-record ring of 3 chunks plus a mirror of its first

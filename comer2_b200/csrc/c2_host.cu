@@ -942,7 +942,7 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
                          [&](int x, int y) { return h->h_plen[h->h_cand[x]] > h->h_plen[h->h_cand[y]]; });
         std::vector<int> lens(nc), items;
         for (int i = 0; i < nc; i++) lens[i] = h->h_plen[h->h_cand[wo[i]]];
-        strip_items(lens, (h->Lq + 31) / 32, h->grid * P1_WARPS, items);
+        strip_items(lens, (h->Lq + 31) / 32, h->nsm * P1TC_WARPS, items);
         if (h->d_worder.ensure(nc) || h->d_tbitems.ensure(items.size()))
             return fail(h, C2_ERR_NOMEM, "candidate order allocation failed");
         CK(cudaMemcpyAsync(h->d_worder.p, wo.data(), (size_t)nc * 4, cudaMemcpyHostToDevice, h->stream));
@@ -966,8 +966,8 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     CK(cudaMemsetAsync(h->d_counter.p, 0, sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_prog.p, 0, (size_t)nitems * sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_tbkey.p, 0, (size_t)nc * sizeof(unsigned long long), h->stream));
-    // one warp per (candidate, strip) work item at most
-    const int grid = (int)std::min<long long>(h->grid, (nitems + P1_WARPS - 1) / P1_WARPS);
+    // one CTA of P1TC_WARPS warps per SM, one warp per (candidate, strip) work item at most
+    const int grid = (int)std::min<long long>(h->nsm, (nitems + P1TC_WARPS - 1) / P1TC_WARPS);
     CK(launch_p1(a, h->d_qbkg.p, P1K_TRACEBACK, grid, h->stream));
     h->launches++;
     FinArgs f;

@@ -18,7 +18,7 @@
 //    transitions passed down the lanes the same way;
 //  * the strip's last row is handed to the next strip through a per-warp
 //    boundary buffer (global memory, L2 resident).
-// The traceback variant (p1tb_kernel) recomputes the same DP for the pairs
+// The traceback sweep (p1tc_kernel) recomputes the same DP for the pairs
 // that pass the phase-1 threshold and stores their scores and btck codes
 // column-major for the finalisation, statistics and MAP stages.
 #include <cuda_bf16.h>
@@ -345,240 +345,6 @@ p1_kernel(P1Args a, const float* __restrict__ qbkg)
     }
 }
 
-// Traceback variant for the candidate pairs: the same score and DP
-// arithmetic as p1_kernel, storing the score matrix, the modular scores and
-// the btck codes column-major.  Work items are (candidate, strip) as in the
-// phase-2 strip pipeline (c2_device.cuh), so a long pair is swept by several
-// warps at once; the pair maximum and its cell are collected in tbkey for the check
-// against phase 1.
-__global__ void __launch_bounds__(P1_WARPS * 32, 2)
-p1tb_kernel(P1Args a, const float* __restrict__ qbkg)
-{
-    extern __shared__ float smem[];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int cvcard = a.sc.cvcard;
-    const int card = a.sc.ssss_card;
-    // traceback codes of the last 32 columns per lane: each lane writes its
-    // cell of column j at step j + lane and the warp stores column k - 31 at
-    // step k, one coalesced 32-byte segment
-    __shared__ signed char btr[P1_WARPS][32][33];
-    float* cvtab = smem;                                      // [cvcard][P1TB_CVREP]
-    float* wb = smem + cvcard * P1TB_CVREP + wid * P1_WARP_FLOATS;
-    float* ring = wb;                                         // [32][32]
-    float* U = wb + 32 * 32;                                  // [card][32]
-    float* rec = U + MAX_SSSS_CARD * 32;                      // [REC_SLOTS][DR_STRIDE] db records
-    for (int i = threadIdx.x; i < cvcard * P1TB_CVREP; i += blockDim.x) cvtab[i] = a.cvvals[i / P1TB_CVREP];
-    __syncthreads();
-
-    const int Lq = a.Lq;
-    const int nstrips = (Lq + 31) >> 5;
-    const int nitems = a.nwork * nstrips;
-    const ScoreConsts sc = a.sc;
-    bool broken = false;
-
-    for (;;) {
-        int item = 0;
-        if (lane == 0) item = atomicAdd(a.counter, 1);
-        item = __shfl_sync(FULL, item, 0);
-        if (item >= nitems) break;
-        const int iv = a.items[item];
-        const int rank = iv / nstrips, s = iv - rank * nstrips;
-        const int cand = a.worder[rank];
-        const int p = a.order[cand];
-        const int L = a.plen[p];
-        const long long off = a.poff[p];
-        const float* __restrict__ dr = a.drec + off * DR_STRIDE;
-        const float* __restrict__ bd = a.pbkg + (long long)p * NAA;
-        const int edge = corner_edge(Lq, L);
-        const long long coff = a.cand_off[cand];
-        signed char* bt = a.btck + coff;
-        float* smt = a.smat + coff;
-        float* mmt = a.mmat + coff;
-        float* bnd = a.bnd + (coff / Lq) * 10;
-        const float* botr = bnd + ((s + 1) & 1) * 5 * L;   // last row of strip s-1
-        float* botw = bnd + (s & 1) * 5 * L;
-        int* pf = a.prog + (long long)cand * nstrips;
-        float best = 0.f;
-        int bcol = 0x7fffffff;
-        int brow = 0x7fffffff;
-        {
-            const int r = s * 32 + lane;
-            const bool act = r < Lq;
-            const float* __restrict__ qr = a.qrec + (long long)(act ? r : Lq - 1) * QR_STRIDE;
-            RowOps R;
-#pragma unroll
-            for (int i = 0; i < NAA; i++)
-                R.Qt[i] = __fdividef(qr[QR_TRG + i], 0.5f * (qbkg[i] + bd[i]));
-#pragma unroll
-            for (int i = 0; i < NCV; i++) R.qcv[i] = qr[QR_CV + i];
-            R.cq = qr[QR_CN];
-            R.pq = qr[QR_PRIOR];
-            R.hq = qr[QR_HQ];
-            {
-                // this strip's SS row tables (built once per query, c2_set_query)
-                const float* __restrict__ us = a.qU + (long long)s * MAX_SSSS_CARD * 32 + lane;
-#pragma unroll 8
-                for (int c = 0; c < card; c++) U[c * 32 + lane] = __ldg(us + c * 32);
-            }
-            float q7[7];
-#pragma unroll
-            for (int i = 0; i < 7; i++) q7[i] = act ? qr[QR_TRN + i] : LOG0;
-            // column -1 boundary states of this row and of the row above
-            const bool z_left = (lane == 31);
-            const bool z_diag = (lane == 31 || lane == 0);
-            const St5 LB = z_left ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
-                                  : St5{0.f, qr[QR_C + 0], qr[QR_C + 1], qr[QR_C + 2], LOG0};
-            const St5 DB = z_diag ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
-                                  : St5{0.f, qr[QR_CP + 0], qr[QR_CP + 1], qr[QR_CP + 2], LOG0};
-            __syncwarp();
-
-            St5 mine = {0.f, 0.f, 0.f, 0.f, 0.f};
-            St5 upp = {0.f, 0.f, 0.f, 0.f, 0.f};
-            float t7[7];
-#pragma unroll
-            for (int i = 0; i < 7; i++) t7[i] = LOG0;
-            // row above the strip, one chunk at a time: lane i holds column 32 c + i
-            // (each chunk is waited for and loaded at the end of the one before,
-            // so a strip trails the one above by 63 wavefront steps)
-            float bcur[5];
-            if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken);
-#pragma unroll
-            for (int f = 0; f < 5; f++) bcur[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : 0.f;
-            const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
-            const int nsteps = L + 31;
-            // db column records are staged into shared memory one chunk ahead
-            stage_chunk(rec, dr, 0, L, lane);
-            stage_chunk(rec, dr, 1, L, lane);
-            for (int k = 0; k < nsteps; k++) {
-                if ((k & (REC_CHUNK - 1)) == 0 && k < L) {
-                    cp_async_wait_1();
-                    __syncwarp();
-                }
-                // ---- score stage: column k for every lane's row
-                float tc[7];
-                if (k < L) {
-                    const float4* rp = reinterpret_cast<const float4*>(rec + (k & (REC_SLOTS - 1)) * DR_STRIDE);
-                    float mod;
-                    float S = cell_score<P1TB_CVREP>(R, rp, U, cvtab, sc, lane, mod);
-                    if (!act) S = -9.f;
-                    ring[(k & 31) * 32 + lane] = S;
-                    if (act) {
-                        smt[(long long)k * Lq + r] = S;
-                        mmt[(long long)k * Lq + r] = mod;
-                    }
-                    const float4 ta = rp[12], tb = rp[13];
-                    tc[0] = ta.x; tc[1] = ta.y; tc[2] = ta.z; tc[3] = ta.w;
-                    tc[4] = tb.x; tc[5] = tb.y; tc[6] = tb.z;
-                    if ((k & (REC_CHUNK - 1)) == REC_CHUNK - 1) {
-                        // chunk fully read by every lane: refill its slots two chunks ahead
-                        __syncwarp();
-                        stage_chunk(rec, dr, (k >> REC_CHUNK_LOG) + 2, L, lane);
-                    }
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 7; i++) tc[i] = LOG0;
-                }
-                // ---- DP stage: column j = k - lane
-#pragma unroll
-                for (int i = 0; i < 7; i++) {
-                    const float x = __shfl_up_sync(FULL, t7[i], 1);
-                    t7[i] = (lane == 0) ? tc[i] : x;
-                }
-                St5 up;
-                up.MM = __shfl_up_sync(FULL, mine.MM, 1);
-                up.MI = __shfl_up_sync(FULL, mine.MI, 1);
-                up.IM = __shfl_up_sync(FULL, mine.IM, 1);
-                up.DN = __shfl_up_sync(FULL, mine.DN, 1);
-                up.ND = __shfl_up_sync(FULL, mine.ND, 1);
-                {
-                    const int src = k & 31;
-                    const float b0 = __shfl_sync(FULL, bcur[0], src);
-                    const float b1 = __shfl_sync(FULL, bcur[1], src);
-                    const float b2 = __shfl_sync(FULL, bcur[2], src);
-                    const float b3 = __shfl_sync(FULL, bcur[3], src);
-                    const float b4 = __shfl_sync(FULL, bcur[4], src);
-                    if (lane == 0) up = St5{b0, b1, b2, b3, b4};
-                    if (src == 31) {
-                        if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken);
-#pragma unroll
-                        for (int f = 0; f < 5; f++) {
-                            const int c = k + 1 + lane;
-                            bcur[f] = (s > 0 && c < L) ? __ldcg(botr + f * L + c) : 0.f;
-                        }
-                    }
-                }
-                const int j = k - lane;
-                St5 left = mine, diag = upp;
-                if (j == 0) { left = LB; diag = DB; }
-                float S = -9.f;
-                if (j >= 0 && j < L) {
-                    S = ring[(j & 31) * 32 + lane];
-                    if (in_corner(Lq, L, edge, r, j)) S = -9.f;
-                }
-                St5 nw;
-                {
-                    float v = fmaxf((diag.MI + q7[TMM]) + t7[TIM], (diag.IM + q7[TIM]) + t7[TMM]);
-                    v = fmaxf(v, (diag.DN + q7[TDM]) + t7[TMM]);
-                    v = fmaxf(v, (diag.ND + q7[TMM]) + t7[TDM]);
-                    v = fmaxf(v, (diag.MM + q7[TMM]) + t7[TMM]);
-                    nw.MM = fmaxf(v + S, 0.f);
-                    nw.MI = fmaxf((up.MM + q7[TMM]) + t7[TMI], (up.MI + q7[TMM]) + t7[TII]);
-                    nw.IM = fmaxf((left.MM + q7[TMI]) + t7[TMM], (left.IM + q7[TII]) + t7[TMM]);
-                    nw.DN = fmaxf(up.MM + q7[TMD], up.DN + q7[TDD]);
-                    nw.ND = fmaxf(left.MM + t7[TMD], left.ND + t7[TDD]);
-                }
-                const bool valid = act && j >= 0 && j < L;
-                if (valid && nw.MM > best) { best = nw.MM; bcol = j; }
-                if (valid) {
-                    int b = BT_STOP;
-                    float mx = nw.MM;
-                    if (nw.MM != 0.f) b = BT_DIAG;
-                    if (mx < nw.MI) { mx = nw.MI; b = BT_UP; }
-                    if (mx < nw.IM) { mx = nw.IM; b = BT_LEFT; }
-                    if (mx < nw.DN) { mx = nw.DN; b = BT_UP; }
-                    if (mx < nw.ND) { b = BT_LEFT; }
-                    btr[wid][j & 31][lane] = (signed char)b;
-                }
-                {
-                    const int cfl = k - 31;
-                    if (act && cfl >= 0 && cfl < L) bt[(long long)cfl * Lq + r] = btr[wid][cfl & 31][lane];
-                }
-                if (wr_bot && j >= 0 && j < L) {
-                    botw[0 * L + j] = nw.MM;
-                    botw[1 * L + j] = nw.MI;
-                    botw[2 * L + j] = nw.IM;
-                    botw[3 * L + j] = nw.DN;
-                    botw[4 * L + j] = nw.ND;
-                    pipe_publish(pf + s, j, L);
-                }
-                mine = nw;
-                upp = up;
-            }
-            cp_async_wait_all();
-            __syncwarp();
-        }
-        if (best > 0.f) brow = s * 32 + lane;
-#pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) {
-            const float ob = __shfl_xor_sync(FULL, best, o);
-            const int orr = __shfl_xor_sync(FULL, brow, o);
-            const int oc = __shfl_xor_sync(FULL, bcol, o);
-            if (ob > best || (ob == best && (orr < brow || (orr == brow && oc < bcol)))) {
-                best = ob; brow = orr; bcol = oc;
-            }
-        }
-        // pair maximum over strips: largest value, then smallest row, then
-        // smallest column, as one 64-bit key (best >= 0 orders by its bits)
-        if (lane == 0 && best > 0.f) {
-            const unsigned cell = ((unsigned)brow << 16) | ((unsigned)bcol & 0xffffu);
-            atomicMax(a.tbkey + cand,
-                      ((unsigned long long)__float_as_uint(best) << 32) | (unsigned long long)(0xffffffffu - cell));
-        }
-        __syncwarp();
-    }
-}
-
-
 // ---------------------------------------------------------------------------
 // Phase 1, chunked: the same arithmetic as p1_kernel, scheduled in chunks of
 // 32 db columns.  Per chunk, every lane first scores its query row against
@@ -661,10 +427,15 @@ __device__ __forceinline__ void bnd_put(float* bnd, int slot, float mm, float mi
 // tcol points at this lane's record for step k0 and the next 31 follow
 // without wrapping; otherwise tcol is a ring of TMASK + 1 records indexed by
 // column & TMASK.  bnd: row above the strip for columns [k0, k0 + 32).
-template <bool CHECK, int RLD, bool TMIRROR, int TMASK>
+// TB (traceback sweep): each cell's traceback code also goes to the warp's
+// column ring btr (column j in slot j & 31, the lane's own row), and column
+// k - 31, complete for every row at step k, is stored to the pair's code
+// matrix bt (column-major, Lq rows; r = this lane's query row).
+template <bool CHECK, int RLD, bool TMIRROR, int TMASK, bool TB = false>
 __device__ __forceinline__ void wf_steps(WfLane& D, int k0, int nst, int lane, int L, bool act,
                                          const float* __restrict__ ring, const float* __restrict__ tcol,
-                                         float* __restrict__ bnd, bool wr_bot)
+                                         float* __restrict__ bnd, bool wr_bot, signed char (*btr)[33] = nullptr,
+                                         signed char* __restrict__ bt = nullptr, int Lq = 0, int r = 0)
 {
     const float* __restrict__ rb = ring + (k0 & (P1C_RING - 1)) * RLD + lane;
     if (!CHECK) nst = 32;
@@ -716,6 +487,22 @@ __device__ __forceinline__ void wf_steps(WfLane& D, int k0, int nst, int lane, i
         // their MM stays 0 and never beats a maximum
         const bool inm = !CHECK || (j >= 0 && j < L);
         if ((!CHECK || act) && inm && nMM > D.best) { D.best = nMM; ub = u; }
+        if (TB) {
+            // ExecDP_Btck's code: DIAG if MM > 0, then the first strictly larger
+            // of MI (UP), IM (LEFT), DN (UP), ND (LEFT)
+            if (act && inm) {
+                int b = BT_STOP;
+                float mx = nMM;
+                if (nMM != 0.f) b = BT_DIAG;
+                if (mx < nMI) { mx = nMI; b = BT_UP; }
+                if (mx < nIM) { mx = nIM; b = BT_LEFT; }
+                if (mx < nDN) { mx = nDN; b = BT_UP; }
+                if (mx < nND) b = BT_LEFT;
+                btr[j & 31][lane] = (signed char)b;
+            }
+            const int cfl = k0 + u - 31;
+            if (act && (!CHECK || (cfl >= 0 && cfl < L))) bt[(long long)cfl * Lq + r] = btr[cfl & 31][lane];
+        }
         if (wr_bot) {
             // lane 31's cell (column k0 + u - 31) into the slot lane 0 read at
             // the top of this step; bot_flush stores the 32 columns per chunk
@@ -911,6 +698,197 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
             const unsigned xy = (pbest > 0.f) ? (((unsigned)pcol << 16) | ((unsigned)prow & 0xffffu)) : 0u;
             a.best[p] = pbest;
             a.coords[p] = xy;
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Traceback sweep, chunked: the DP finalisation's FP32 recomputation of the
+// candidates (ExecDP_Btck_Unroll32x, src/libmycu/cudp/CuBatchDP_init_btck.cu:
+// 303-360) with p1c_kernel's schedule -- per 32-column chunk the scores of the
+// strip (also stored to the pair's score and modular-score matrices, column-
+// major, coalesced) and then 32 wavefront steps that also store the traceback
+// codes.  Work items are (candidate, strip) in the strip pipeline of
+// c2_device.cuh: strip s waits, before DP stage m, for the strip above to have
+// published the columns of chunk m + 1 of its last row (loaded into registers
+// during the stage) and publishes its own last row once per chunk.  The
+// arithmetic is p1c_kernel's, so the maxima equal phase 1's in the FP32 form.
+__global__ void __launch_bounds__(P1TC_WARPS * 32, 1)
+p1tc_kernel(P1Args a, const float* __restrict__ qbkg)
+{
+    extern __shared__ float smem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int cvcard = a.sc.cvcard;
+    const int card = a.sc.ssss_card;
+    __shared__ signed char btr_all[P1TC_WARPS][32][33];
+    signed char(*btr)[33] = btr_all[wid];
+    float* cvtab = smem;                                      // [cvcard][P1TC_CVREP]
+    float* wb = smem + cvcard * P1TC_CVREP + wid * P1C_WARP_FLOATS;
+    float* ring = wb;                                         // [P1C_RING][32] scores
+    float* trn = ring + P1C_RING * 32;                        // [P1C_RING][P1C_TRS] transitions
+    float* U = trn + P1C_RING * P1C_TRS;                      // [card][32]
+    float* rec = U + MAX_SSSS_CARD * 32;                      // [REC_SLOTS][DR_STRIDE] db records
+    float* bnd = rec + REC_SLOTS * DR_STRIDE;                 // [BND_FLOATS] row above the strip
+    for (int i = threadIdx.x; i < cvcard * P1TC_CVREP; i += blockDim.x) cvtab[i] = a.cvvals[i / P1TC_CVREP];
+    __syncthreads();
+
+    const int Lq = a.Lq;
+    const int nstrips = (Lq + 31) >> 5;
+    const int nitems = a.nwork * nstrips;
+    const ScoreConsts sc = a.sc;
+    bool broken = false;
+
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.counter, 1);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= nitems) break;
+        const int iv = a.items[item];
+        const int rank = iv / nstrips, s = iv - rank * nstrips;
+        const int cand = a.worder[rank];
+        const int p = a.order[cand];
+        const int L = a.plen[p];
+        const long long off = a.poff[p];
+        const float* __restrict__ dr = a.drec + off * DR_STRIDE;
+        const float* __restrict__ bd = a.pbkg + (long long)p * NAA;
+        const int edge = corner_edge(Lq, L);
+        const long long coff = a.cand_off[cand];
+        signed char* bt = a.btck + coff;
+        float* smt = a.smat + coff;
+        float* mmt = a.mmat + coff;
+        float* pb = a.bnd + (coff / Lq) * 10;
+        const float* botr = pb + ((s + 1) & 1) * 5 * L;   // last row of strip s-1
+        float* botw = pb + (s & 1) * 5 * L;
+        int* pf = a.prog + (long long)cand * nstrips;
+        const int r = s * 32 + lane;
+        const bool act = r < Lq;
+        const float* __restrict__ qr = a.qrec + (long long)(act ? r : Lq - 1) * QR_STRIDE;
+        RowOps R;
+#pragma unroll
+        for (int i = 0; i < NAA; i++)
+            R.Qt[i] = __fdividef(qr[QR_TRG + i], 0.5f * (qbkg[i] + bd[i]));
+#pragma unroll
+        for (int i = 0; i < NCV; i++) R.qcv[i] = qr[QR_CV + i];
+        R.cq = qr[QR_CN];
+        R.pq = qr[QR_PRIOR];
+        R.hq = qr[QR_HQ];
+        {
+            // this strip's SS row tables (built once per query, c2_set_query)
+            const float* __restrict__ us = a.qU + (long long)s * MAX_SSSS_CARD * 32 + lane;
+#pragma unroll 8
+            for (int c = 0; c < card; c++) U[c * 32 + lane] = __ldg(us + c * 32);
+        }
+        WfLane D;
+        {
+            float q7[7];
+#pragma unroll
+            for (int i = 0; i < 7; i++) q7[i] = act ? qr[QR_TRN + i] : LOG0;
+            const bool z_left = (lane == 31);
+            const bool z_diag = (lane == 31 || lane == 0);
+            const St5 LB = z_left ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
+                                  : St5{0.f, qr[QR_C + 0], qr[QR_C + 1], qr[QR_C + 2], LOG0};
+            const St5 DB = z_diag ? St5{0.f, 0.f, 0.f, 0.f, 0.f}
+                                  : St5{0.f, qr[QR_CP + 0], qr[QR_CP + 1], qr[QR_CP + 2], LOG0};
+            wf_init(D, q7, LB, DB);
+        }
+        const int cA = corner_a(r, Lq, edge);
+        const int cB = corner_b(r, L, edge);
+        // columns [0, 32) of the row above, lane i holding column i
+        float bc[5];
+        if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken);
+#pragma unroll
+        for (int f = 0; f < 5; f++) {
+            bc[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : 0.f;
+            D.bnxt[f] = 0.f;
+        }
+        const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
+        __syncwarp();
+        bnd_put(bnd, lane, bc[0], bc[1], bc[2], bc[3], bc[4]);
+        stage_chunk(rec, dr, 0, L, lane);
+        stage_chunk(rec, dr, 1, L, lane);
+        const int nch = (L + 31) >> 5;
+        const int kend = L + 31;
+        for (int m = 0; 32 * m < kend; m++) {
+            // ---- score stage: columns [32m, min(32m + 32, L))
+            if (m < nch) {
+                const int c0 = 32 * m, c1 = min(c0 + 32, L);
+                const bool hasc = __any_sync(FULL, cA >= c0 || cB < c1);
+                for (int c = c0; c < c1; c++) {
+                    if ((c & (REC_CHUNK - 1)) == 0) {
+                        cp_async_wait_1();
+                        __syncwarp();
+                    }
+                    const float* rc = rec + (c & (REC_SLOTS - 1)) * DR_STRIDE;
+                    float mod;
+                    float Sc = cell_score<P1TC_CVREP>(R, reinterpret_cast<const float4*>(rc), U, cvtab, sc, lane, mod);
+                    if (act) {
+                        smt[(long long)c * Lq + r] = Sc;
+                        mmt[(long long)c * Lq + r] = mod;
+                    }
+                    if (hasc && (c <= cA || c >= cB)) Sc = -9.f;
+                    ring[((c + lane) & (P1C_RING - 1)) * 32 + lane] = Sc;
+                    if (lane < DPT_N) trn[(c & (P1C_RING - 1)) * P1C_TRS + lane] = rc[DR_TRN + dpt_src(lane)];
+                    if ((c & (REC_CHUNK - 1)) == REC_CHUNK - 1) {
+                        __syncwarp();
+                        stage_chunk(rec, dr, (c >> REC_CHUNK_LOG) + 2, L, lane);
+                    }
+                }
+            }
+            // the row above for chunk m + 1, loaded while this stage runs
+            const int k0 = 32 * m, k1 = min(k0 + 32, kend);
+            if (s > 0 && k0 + 32 < L) {
+                pipe_wait(pf + s - 1, min(k0 + 64, L), lane, a.status, broken);
+#pragma unroll
+                for (int f = 0; f < 5; f++) {
+                    const int cc = k0 + 32 + lane;
+                    D.bnxt[f] = (cc < L) ? __ldcg(botr + f * L + cc) : 0.f;
+                }
+            } else {
+#pragma unroll
+                for (int f = 0; f < 5; f++) D.bnxt[f] = 0.f;
+            }
+            __syncwarp();
+            // ---- DP stage: wavefront steps [32m, 32m + 32), traceback codes stored
+            if (m >= 1 && k0 + 31 < L && k1 == k0 + 32)
+                wf_steps<false, 32, false, P1C_RING - 1, true>(D, k0, 32, lane, L, act, ring, trn, bnd, wr_bot, btr,
+                                                               bt, Lq, r);
+            else
+                wf_steps<true, 32, false, P1C_RING - 1, true>(D, k0, k1 - k0, lane, L, act, ring, trn, bnd, wr_bot,
+                                                              btr, bt, Lq, r);
+            __syncwarp();
+            if (s + 1 < nstrips) {
+                // last row of columns [k0 - 31, k0] to the pair's buffer, then published
+                bot_flush(bnd, botw, k0, L, L, lane);
+                __syncwarp();
+                if (lane == 0) {
+                    __threadfence();
+                    pipe_st_release(pf + s, min(k1 - 31, L));
+                }
+            }
+            __syncwarp();
+            bnd_put(bnd, lane, D.bnxt[0], D.bnxt[1], D.bnxt[2], D.bnxt[3], D.bnxt[4]);
+            __syncwarp();
+        }
+        cp_async_wait_all();
+        // the strip's maximum: largest score, then smallest row, then smallest column
+        float best = D.best;
+        int brow = (best > 0.f) ? r : 0x7fffffff;
+        int bcol = (best > 0.f) ? D.kbest - lane : 0x7fffffff;
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            const float ob = __shfl_xor_sync(FULL, best, o);
+            const int orr = __shfl_xor_sync(FULL, brow, o);
+            const int oc = __shfl_xor_sync(FULL, bcol, o);
+            if (ob > best || (ob == best && (orr < brow || (orr == brow && oc < bcol)))) {
+                best = ob; brow = orr; bcol = oc;
+            }
+        }
+        // pair maximum over strips as one 64-bit key (best >= 0 orders by its bits)
+        if (lane == 0 && best > 0.f) {
+            const unsigned cell = ((unsigned)brow << 16) | ((unsigned)bcol & 0xffffu);
+            atomicMax(a.tbkey + cand,
+                      ((unsigned long long)__float_as_uint(best) << 32) | (unsigned long long)(0xffffffffu - cell));
         }
         __syncwarp();
     }
@@ -1597,13 +1575,6 @@ size_t p1_smem_bytes(int cvcard)
     return (size_t)(cvcard * 32 + P1_WARPS * P1_WARP_FLOATS) * sizeof(float);
 }
 
-// the traceback sweep: fewer CV table replicas make room for its traceback
-// ring, keeping two CTAs per SM
-size_t p1tb_smem_bytes(int cvcard)
-{
-    return (size_t)(cvcard * P1TB_CVREP + P1_WARPS * P1_WARP_FLOATS) * sizeof(float);
-}
-
 cudaError_t launch_p1(const P1Args& a, const float* qbkg, int which, int grid, cudaStream_t st)
 {
     if (which == P1K_TENSOR) {
@@ -1625,9 +1596,10 @@ cudaError_t launch_p1(const P1Args& a, const float* qbkg, int which, int grid, c
     }
     const size_t sm = p1_smem_bytes(a.sc.cvcard);
     if (which == P1K_TRACEBACK) {
-        const size_t smt = p1tb_smem_bytes(a.sc.cvcard);
-        cudaFuncSetAttribute(p1tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
-        p1tb_kernel<<<grid, P1_WARPS * 32, smt, st>>>(a, qbkg);
+        const size_t smt = (size_t)(a.sc.cvcard * P1TC_CVREP + P1TC_WARPS * P1C_WARP_FLOATS) * sizeof(float);
+        cudaError_t e = cudaFuncSetAttribute(p1tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
+        if (e != cudaSuccess) return e;
+        p1tc_kernel<<<grid, P1TC_WARPS * 32, smt, st>>>(a, qbkg);
     } else {
         cudaFuncSetAttribute(p1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         p1_kernel<<<grid, P1_WARPS * 32, sm, st>>>(a, qbkg);
