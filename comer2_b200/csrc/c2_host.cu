@@ -1128,7 +1128,11 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
     for (int c : h->h_mapcand) cells += (long long)h->Lq * h->h_plen[h->h_cand[c]];
     (void)cells;
     h->alnstride = h->Lq + h->Lmax + 1;
-    size_t fbn = h->d_smat.n;   // same layout as the candidates' score matrices
+    // F and B in wavefront order: [nstrips][L + 31][32] per candidate, at
+    // 32 nstrips (sum of (L + 31) over the candidates before it)
+    long long skl = 0;
+    for (int c = 0; c < h->ncand; c++) skl += (long long)h->h_plen[h->h_cand[c]] + 31;
+    const size_t fbn = (size_t)32 * ((h->Lq + 31) / 32) * (size_t)skl;
     if (h->d_mapcand.ensure(nm) || h->d_mappass.ensure(nm) || h->d_fb.ensure(fbn) || h->d_bb.ensure(fbn) ||
         h->d_pairf.ensure((size_t)nm * 4) ||
         h->d_pairc.ensure(nm) || h->d_alninfo.ensure((size_t)nm * 8) || h->d_aln.ensure((size_t)nm * 5 * h->alnstride) ||

@@ -110,7 +110,17 @@ __device__ __forceinline__ void trn_bwd(const float* __restrict__ t0, int i, int
 // [k - 31, k]; chunk m (columns [32m, 32m + 32)) is written at the end of
 // step 32m - 1, into the half of chunk m - 2, whose last use was step 32m - 2.
 constexpr int MTRS = 12;
-constexpr int MAPFB_WARP_FLOATS = 2 * 32 * 33 + 64 * MTRS + 32 * 8;   // 12,544 B, a multiple of 16
+constexpr int MAPFB_WARP_FLOATS = 32 * 33 + 64 * MTRS + 32 * 8;   // 8,320 B, a multiple of 16
+
+// F and B are stored in the forward sweep's wavefront order: per candidate
+// [nstrips][L + 31][32], strip s, step k, lane i holding row 32 s + i, column
+// k - i.  The forward sweep and the MAP DP then read and write one 128-byte
+// line per step, and the backward sweep at most two.
+__device__ __forceinline__ long long skew_base(const MapArgs& a, int c)
+{
+    const int nstrips = (a.Lq + 31) >> 5;
+    return 32LL * nstrips * (a.cand_off[c] / a.Lq + 31LL * c);
+}
 
 template <bool BWD>
 __device__ __forceinline__ void map_trn_col(const float* __restrict__ t0, int j, int L, float* t7)
@@ -177,6 +187,13 @@ __device__ __forceinline__ void pf_cols(const float* __restrict__ mat, int c, in
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p + r1));
 }
 
+// L2 prefetch of wavefront row k (32 floats, one 128-byte line) of a strip
+// stored in wavefront order ([W][32])
+__device__ __forceinline__ void pf_line(const float* __restrict__ st, int k, int W)
+{
+    if (k < W) asm volatile("prefetch.global.L2 [%0];" ::"l"(st + (long long)k * 32));
+}
+
 // scores (and modular scores when they enter) of the columns of the sweep's
 // chunk starting at column c0 (actual columns; BWD: mirrored, c0 the first
 // mirrored column), rows [row0, row0 + 32)
@@ -193,8 +210,8 @@ __device__ __forceinline__ void pf_scores(const MapArgs& a, const MapPair& P, in
 // items are (pair, strip); see the strip pipeline in c2_device.cuh.
 __device__ __forceinline__ void map_fwd_item(const MapArgs& a, const float* __restrict__ qtrn,
                                              const float* __restrict__ dtrn, const float* __restrict__ qcf, int m,
-                                             int s, int lane, float (*rin)[33], float (*rout)[33], float* trs,
-                                             float* rab, bool& broken)
+                                             int s, int lane, float (*rin)[33], float* trs, float* rab,
+                                             bool& broken)
 {
     const int Lq = a.Lq;
     const int nstrips = (Lq + 31) >> 5;
@@ -203,7 +220,8 @@ __device__ __forceinline__ void map_fwd_item(const MapArgs& a, const float* __re
         const MapPair P = map_pair(a, qtrn, m);
         const int L = P.L;
         const float* __restrict__ dt0 = dtrn + P.toff;
-        float* fb = a.fb + P.base;
+        // this strip's rows of F in wavefront order
+        float* fs = a.fb + skew_base(a, P.c) + (long long)s * (L + 31) * 32;
         // column transitions: chunk 0 into the ring, chunk 1 into registers
         float tnx[7];
         {
@@ -300,7 +318,7 @@ __device__ __forceinline__ void map_fwd_item(const MapArgs& a, const float* __re
                 const bool valid = act && j >= 0 && j < L;
                 if (valid) {
                     maxF = hmax(maxF, nw.MM);
-                    rout[j & 31][lane] = nw.MM;
+                    fs[(long long)k * 32 + lane] = nw.MM;
                 }
                 if (wr_bot && j >= 0 && j < L) {
                     botw[0 * L + j] = nw.MM; botw[1 * L + j] = nw.MI; botw[2 * L + j] = nw.IM;
@@ -309,8 +327,6 @@ __device__ __forceinline__ void map_fwd_item(const MapArgs& a, const float* __re
                 }
                 mine = nw;
                 upp = up;
-                const int cfl = k - 31;
-                if (cfl >= 0 && cfl < L && act) fb[(long long)cfl * Lq + r] = rout[cfl & 31][lane];
                 if ((k & 31) == 31) {
                     // columns of chunk k / 32 + 1 into the ring, the next chunk into registers
                     __syncwarp();
@@ -340,11 +356,18 @@ __global__ void __launch_bounds__(256) map_z_kernel(MapArgs a)
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int c = a.map_cand[m];
     const int p = a.cand_prof[c];
-    const long long n = (long long)a.Lq * a.plen[p];
-    const float* fb = a.fb + a.cand_off[c];
+    const int Lq = a.Lq, L = a.plen[p], W = L + 31;
+    const int nrows = ((Lq + 31) >> 5) * W;   // (strip, step) rows of 32 lanes
+    const float* fs = a.fb + skew_base(a, c);
     const float maxF = a.pairf[m * 4 + 0];
     float s = 0.f;
-    for (long long k = threadIdx.x; k < n; k += 256) s += fexp(fb[k] - maxF);
+    // warp w takes rows w, w + 8, ...; lane i of row (strip t, step k) is cell
+    // (32 t + i, k - i)
+    for (int rw = wid; rw < nrows; rw += 8) {
+        const int t = rw / W, k = rw - t * W;
+        const int row = 32 * t + lane, col = k - lane;
+        if (row < Lq && col >= 0 && col < L) s += fexp(fs[(long long)rw * 32 + lane] - maxF);
+    }
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
     if (lane == 0) part[wid] = s;
@@ -361,8 +384,7 @@ __global__ void __launch_bounds__(256) map_z_kernel(MapArgs a)
 // B.MM to fb, giving F+B per cell.  Work items are (pair, mirrored strip).
 __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __restrict__ qtrn,
                                              const float* __restrict__ dtrn, int m, int s, int lane,
-                                             float (*rin)[33], float (*rout)[33], float* trs, float* rab,
-                                             bool& broken)
+                                             float (*rin)[33], float* trs, float* rab, bool& broken)
 {
     const int Lq = a.Lq;
     const int nstrips = (Lq + 31) >> 5;
@@ -371,7 +393,7 @@ __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __re
         const MapPair P = map_pair(a, qtrn, m);
         const int L = P.L;
         const float* __restrict__ dt0 = dtrn + P.toff;
-        float* bb = a.bb + P.base;
+        float* bsk = a.bb + skew_base(a, P.c);   // B in the forward sweep's wavefront order
         // column transitions: chunk 0 into the ring, chunk 1 into registers
         float tnx[7];
         {
@@ -470,7 +492,11 @@ __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __re
                 nw.IM = lse2(((dg.MM + q7[TIM]) + t7[TMM]) + sco, (rt.IM + q7[TII]) + t7[TMM]);
                 nw.DN = lse2(((dg.MM + q7[TDM]) + t7[TMM]) + sco, dn.DN + q7[TDD]);
                 nw.ND = lse2(((dg.MM + q7[TMM]) + t7[TDM]) + sco, rt.ND + t7[TDD]);
-                if (act && j >= 0 && j < L) rout[j & 31][lane] = nw.MM;
+                if (act && j >= 0 && j < L) {
+                    // actual cell (r, L - 1 - j): forward strip r / 32, lane r % 32, step column + lane
+                    const int lf = r & 31;
+                    bsk[((long long)(r >> 5) * (L + 31) + (L - 1 - j) + lf) * 32 + lf] = nw.MM;
+                }
                 if (wr_bot && j >= 0 && j < L) {
                     botw[0 * L + j] = nw.MM; botw[1 * L + j] = nw.MI; botw[2 * L + j] = nw.IM;
                     botw[3 * L + j] = nw.DN; botw[4 * L + j] = nw.ND;
@@ -478,8 +504,6 @@ __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __re
                 }
                 mine = nw;
                 upp = dn;
-                const int cfl = k - 31;
-                if (cfl >= 0 && cfl < L && act) bb[(long long)(L - 1 - cfl) * Lq + r] = rout[cfl & 31][lane];
                 if ((k & 31) == 31) {
                     // mirrored columns of chunk k / 32 + 1 into the ring, the next chunk into registers
                     __syncwarp();
@@ -500,14 +524,13 @@ __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __re
 __global__ void __launch_bounds__(MAPFBW * 32) map_fb_kernel(MapArgs a, const float* __restrict__ qtrn,
                                                      const float* __restrict__ dtrn, const float* __restrict__ qcf)
 {
-    // per warp: score ring, output ring [32][33] each, column transitions
-    // [64][MTRS], row above the strip for the current chunk [32][8]
+    // per warp: score ring [32][33], column transitions [64][MTRS], row above
+    // the strip for the current chunk [32][8]
     extern __shared__ __align__(16) float fbsm[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float* wsm = fbsm + wid * MAPFB_WARP_FLOATS;
     float(*rin)[33] = reinterpret_cast<float(*)[33]>(wsm);
-    float(*rout)[33] = reinterpret_cast<float(*)[33]>(wsm + 32 * 33);
-    float* trs = wsm + 2 * 32 * 33;
+    float* trs = wsm + 32 * 33;
     float* rab = trs + 64 * MTRS;
     const int nstrips = (a.Lq + 31) >> 5;
     const int nitems = 2 * a.nmap * nstrips;
@@ -521,9 +544,9 @@ __global__ void __launch_bounds__(MAPFBW * 32) map_fb_kernel(MapArgs a, const fl
         const int m = iv / nstrips, s = iv - m * nstrips;
         __syncwarp();
         if (item & 1)
-            map_bwd_item(a, qtrn, dtrn, m, s, lane, rin, rout, trs, rab, broken);
+            map_bwd_item(a, qtrn, dtrn, m, s, lane, rin, trs, rab, broken);
         else
-            map_fwd_item(a, qtrn, dtrn, qcf, m, s, lane, rin, rout, trs, rab, broken);
+            map_fwd_item(a, qtrn, dtrn, qcf, m, s, lane, rin, trs, rab, broken);
         __syncwarp();
     }
 }
@@ -539,12 +562,10 @@ __device__ __forceinline__ int corner_edge_m(int lq, int ld)
     return e > 60 ? 60 : e;
 }
 
-__global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
+__global__ void __launch_bounds__(MAPW * 32, 8) map_dp_kernel(MapArgs a)
 {
-    __shared__ float rings[MAPW][32][33];
     __shared__ signed char brings[MAPW][32][33];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    float(*rin)[33] = rings[wid];
     signed char(*bout)[33] = brings[wid];
     const int Lq = a.Lq;
     const int nstrips = (Lq + 31) >> 5;
@@ -562,8 +583,11 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
         const int p = a.cand_prof[c];
         const int L = a.plen[p];
         const long long base = a.cand_off[c];
-        const float* fb = a.fb + base;
-        const float* bb = a.bb + base;
+        const int W = L + 31;
+        // this strip's F and B in wavefront order: step k, lane i = cell (32 s + i, k - i)
+        const long long sko = skew_base(a, c) + (long long)s * W * 32;
+        const float* fs = a.fb + sko;
+        const float* bs = a.bb + sko;
         signed char* bt = a.btck + base;
         const float logZ = a.pairf[m * 4 + 1];
         const int edge = corner_edge_m(Lq, L);
@@ -581,18 +605,18 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
             if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken);
             float bcur = (s > 0 && lane < L) ? __ldcg(botr + lane) : 0.f;
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
-            // F + B of column k is loaded one step ahead, from L2: each chunk's
-            // columns are prefetched a chunk earlier
-            pf_cols(fb, lane, L, Lq, s * 32);
-            pf_cols(fb, 32 + lane, L, Lq, s * 32);
-            pf_cols(bb, lane, L, Lq, s * 32);
-            pf_cols(bb, 32 + lane, L, Lq, s * 32);
-            float nfb = act ? fb[r] + bb[r] : 0.f;
-            for (int k = 0; k < L + 31; k++) {
-                if (k < L) {
-                    rin[k & 31][lane] = nfb;
-                    if (k + 1 < L) nfb = act ? fb[(long long)(k + 1) * Lq + r] + bb[(long long)(k + 1) * Lq + r] : 0.f;
-                }
+            // F + B of the next step's cells is loaded one step ahead, from L2:
+            // each chunk of 32 steps (32 lines of 128 bytes) is prefetched a
+            // chunk earlier.  Entries of cells outside the matrix are read but
+            // not used.
+            pf_line(fs, lane, W);
+            pf_line(fs, 32 + lane, W);
+            pf_line(bs, lane, W);
+            pf_line(bs, 32 + lane, W);
+            float nfb = fs[lane] + bs[lane];
+            for (int k = 0; k < W; k++) {
+                const float fbk = nfb;   // F + B of this step's cell
+                if (k + 1 < W) nfb = fs[(long long)(k + 1) * 32 + lane] + bs[(long long)(k + 1) * 32 + lane];
                 float up = __shfl_up_sync(FULL, mine, 1);
                 {
                     const int src = k & 31;
@@ -601,8 +625,8 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
                     if (src == 31) {
                         if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken);
                         bcur = (s > 0 && k + 1 + lane < L) ? __ldcg(botr + k + 1 + lane) : 0.f;
-                        pf_cols(fb, k + 33 + lane, L, Lq, s * 32);
-                        pf_cols(bb, k + 33 + lane, L, Lq, s * 32);
+                        pf_line(fs, k + 33 + lane, W);
+                        pf_line(bs, k + 33 + lane, W);
                     }
                 }
                 __syncwarp();
@@ -614,7 +638,7 @@ __global__ void __launch_bounds__(MAPW * 32) map_dp_kernel(MapArgs a)
                 int b = BT_STOP;
                 if (j >= 0 && j < L) {
                     const bool crn = (Lq <= r + edge && j <= edge + r - Lq) || (L - edge + r <= j && r < edge);
-                    const float fbv = (!act || crn) ? 0.f : rin[j & 31][lane];
+                    const float fbv = (!act || crn) ? 0.f : fbk;
                     v = (diag + fexp(fbv - logZ)) - a.minpp;
                     if (v > 0.f) b = BT_DIAG; else v = 0.f;
                     if (valid && v > best) { best = v; brow = r; bcol = j; }

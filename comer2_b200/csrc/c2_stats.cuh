@@ -48,8 +48,9 @@ struct MapArgs {
     const float* smat;          // [L][Lq] per candidate
     const float* mmat;          // [L][Lq] per candidate (modular scores)
     const float* stats;         // [npass][STATS_NOUT]
-    float* fb;                  // [L][Lq] per candidate: F (MAP.MM forward values)
-    float* bb;                  // [L][Lq] per candidate: B (backward values)
+    float* fb;                  // F (MAP.MM forward values), per candidate [nstrips][L + 31][32] in
+                                // wavefront order (c2_map.cu, skew_base)
+    float* bb;                  // B (backward values), the same layout
     signed char* btck;          // [L][Lq] per candidate: MAP traceback codes
     float* pairf;               // [nmap][4]: maxF, logZ, map max, (unused)
     unsigned* pairc;            // [nmap]: MAP end coordinates
