@@ -1081,10 +1081,13 @@ __global__ void __launch_bounds__(128) tc_pack_kernel(const float* __restrict__ 
 // Score epilogue of one cell of the tensor-core form from its three
 // contractions (the CV one with 1/kappa0 folded in, the SS one the complete
 // weighted SS term):
-//   s0  = ln(aa) - shift
 //   x   = 2 (cterm + pownu0 ln(cq cd - dot^2) - prior_q - prior_d)
 //   cvm = w_cv T[shift + rint(x)] (T clamped; the key range tests when the
-//         table is not uniform), S = s0 + (ss + cvm)
+//         table is not uniform)
+//   S   = (ln(aa) - shift) + (ss + cvm), evaluated as ln(aa) + (ss +
+//         (cvm - shift)) with the table pre-shifted: a reassociation within
+//         the rounding of the split-BF16 products (this form only ranks the
+//         pairs; the candidates are rescored in FP32)
 // (cell_score is the FP32 form; src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cu)
 constexpr float C2_LN2 = 0.693147180559945309f;
 // hardware base-2 logarithm, denormal inputs flushed (the arguments here, an
@@ -1096,19 +1099,20 @@ __device__ __forceinline__ float lg2_ftz(float x)
     return y;
 }
 template <bool CVUNIF>
-__device__ __forceinline__ float tc_cell(float daa, float dot, float ss, float cq, float pq2, float cd, float pd2,
+__device__ __forceinline__ float tc_cell(float daa, float dot, float ss, float cq, float rq2, float cd, float pd2,
                                          const float* __restrict__ cvl, const TcConsts& tc)
 {
-    const float s0 = fmaf(lg2_ftz(daa), C2_LN2, -tc.shift);
+    // rq2 = c2 - 2 prior_q (per row); the table values and vfw, vlw carry the
+    // -shift of the amino-acid term, so the cell is ln(daa) + (ss + cv)
     const float det = fmaf(-dot, dot, cq * cd);
-    const float x = (fmaf(tc.p2l, lg2_ftz(det), tc.c2) - pq2) - pd2;
+    const float x = fmaf(tc.p2l, lg2_ftz(det), rq2) - pd2;
     const int ix = min(max(__float2int_rn(x), tc.ilo), tc.ihi);
     float cvm = cvl[ix * P1T_CVREP];
     if (!CVUNIF) {
-        cvm = (tc.kl2 <= x) ? tc.vlw : cvm;
-        cvm = (x <= tc.kf2) ? tc.vfw : cvm;
+        cvm = (tc.kl2 <= x) ? tc.vlw - tc.shift : cvm;
+        cvm = (x <= tc.kf2) ? tc.vfw - tc.shift : cvm;
     }
-    return s0 + (ss + cvm);
+    return fmaf(lg2_ftz(daa), C2_LN2, ss + cvm);
 }
 
 // Stage the column records of chunk m (32 columns) into the column ring
@@ -1151,7 +1155,7 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
     unsigned* btile = reinterpret_cast<unsigned*>(bnd + BND_FLOATS);   // [TC_TILE_WORDS] db operand tile
     unsigned long long* tbar = reinterpret_cast<unsigned long long*>(btile + TC_TILE_WORDS);
     for (int i = threadIdx.x; i < cvcard * P1T_CVREP; i += blockDim.x)
-        cvtab[i] = a.cvvals[i / P1T_CVREP] * a.sc.cvswgt;
+        cvtab[i] = a.cvvals[i / P1T_CVREP] * a.sc.cvswgt - a.tc.shift;
     __shared__ unsigned tmem_base;
     if (lane == 0) {
         mbar_init(tbar, 1);
@@ -1254,7 +1258,7 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                     const int rr = s * 32 + 16 * mt + g + 8 * hh;
                     const float* qx = a.qrec + (long long)min(rr, Lq - 1) * QR_STRIDE;
                     rq[mt][hh][0] = qx[QR_CN];
-                    rq[mt][hh][1] = 2.f * qx[QR_PRIOR];
+                    rq[mt][hh][1] = tc.c2 - 2.f * qx[QR_PRIOR];
                 }
             WfLane D;
             {
@@ -1308,7 +1312,7 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                     const bool hasc = __any_sync(FULL, cA >= 32 * m || cB < 32 * m + 32);
                     const float* cbase = cring + ((32 * m) % P1T_CMOD) * P1C_TRS;
                     // ---- score stage: 32 x 32 tile of chunk m on the tensor cores
-#pragma unroll 1
+#pragma unroll 2
                     for (int nt = 0; nt < 4; nt++) {
                         const int T = 4 * m + nt;
                         const bool got = mbar_wait(tbar, tph);
