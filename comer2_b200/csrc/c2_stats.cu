@@ -35,20 +35,48 @@ __device__ __forceinline__ float wsum(float v)
     return v;
 }
 
-// two-level sum over the 21 x 32 block; result valid in every thread
-__device__ __forceinline__ float block_sum(float v, float* tmp, float* res)
+// Two-level sums over the 21 x 32 block (each warp's butterfly, then the 21
+// warp totals by warp 0); results valid in every thread.  Calls alternate
+// between two halves of the scratch, so no trailing barrier is needed: a
+// half is rewritten two calls later, after every thread has passed the first
+// barrier of the call in between (and so has read this call's result).
+struct BlockSums {
+    float2 t[2][32];
+    float2 r[2];
+};
+
+__device__ __forceinline__ float block_sum(float v, BlockSums& S, int& ph)
 {
     v = wsum(v);
-    if (threadIdx.x == 0) tmp[threadIdx.y] = v;
+    if (threadIdx.x == 0) S.t[ph][threadIdx.y].x = v;
     __syncthreads();
     if (threadIdx.y == 0) {
-        float u = threadIdx.x < NDS ? tmp[threadIdx.x] : 0.f;
+        float u = threadIdx.x < NDS ? S.t[ph][threadIdx.x].x : 0.f;
         u = wsum(u);
-        if (threadIdx.x == 0) *res = u;
+        if (threadIdx.x == 0) S.r[ph].x = u;
     }
     __syncthreads();
-    const float r = *res;
+    const float r = S.r[ph].x;
+    ph ^= 1;
+    return r;
+}
+
+// two sums in one pass, each in block_sum's order
+__device__ __forceinline__ float2 block_sum2(float a, float b, BlockSums& S, int& ph)
+{
+    a = wsum(a);
+    b = wsum(b);
+    if (threadIdx.x == 0) S.t[ph][threadIdx.y] = make_float2(a, b);
     __syncthreads();
+    if (threadIdx.y == 0) {
+        float2 u = threadIdx.x < NDS ? S.t[ph][threadIdx.x] : make_float2(0.f, 0.f);
+        u.x = wsum(u.x);
+        u.y = wsum(u.y);
+        if (threadIdx.x == 0) S.r[ph] = u;
+    }
+    __syncthreads();
+    const float2 r = S.r[ph];
+    ph ^= 1;
     return r;
 }
 
@@ -294,13 +322,13 @@ __device__ float evalue_ss18(const StatsArgs& a, int nq, int nd, float score, fl
 }
 
 // ---- the per-pair statistics kernel
-__global__ void __launch_bounds__(SCF * NDS) stats_kernel(StatsArgs a)
+__global__ void __launch_bounds__(SCF * NDS, 2) stats_kernel(StatsArgs a)
 {
     __shared__ float counts[NSCALED + 31];
     __shared__ float P[NDS][SCF + 1];
     __shared__ float pu[NDS];
-    __shared__ float tmp[32];
-    __shared__ float res;
+    __shared__ BlockSums bsm;
+    int ph = 0;
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int tid = ty * SCF + tx;
     const int pi = blockIdx.x;              // passed-pair index
@@ -340,12 +368,12 @@ __global__ void __launch_bounds__(SCF * NDS) stats_kernel(StatsArgs a)
         if (tx == 0) pu[ty] = rs;
     }
     __syncthreads();
-    const float total = block_sum(cnt, tmp, &res);
+    const float total = block_sum(cnt, bsm, ph);
     if (ty == 0 && tx < NDS) pu[tx] = __fdividef(pu[tx], total);
     P[ty][tx] = __fdividef(P[ty][tx], total);
     __syncthreads();
     const float sc = (float)(left + tx + SMIN);
-    float E = block_sum(sc * P[ty][tx], tmp, &res);
+    float E = block_sum(sc * P[ty][tx], bsm, ph);
     // score range over nonzero probabilities (including 0)
     float vmin = P[ty][tx] != 0.f ? sc : 0.f, vmax = vmin;
 #pragma unroll
@@ -374,8 +402,14 @@ __global__ void __launch_bounds__(SCF * NDS) stats_kernel(StatsArgs a)
                 const float yy = x * s2;
                 if (LOG_SP_MIN < yy) { lf = __expf(yy) * P[ty][tx]; ldf = lf * s2; }
             }
-            float f = block_sum(lf, tmp, &res);
-            float df = dfo ? block_sum(ldf, tmp, &res) : 0.f;
+            float f, df = 0.f;
+            if (dfo) {
+                const float2 fd = block_sum2(lf, ldf, bsm, ph);
+                f = fd.x;
+                df = fd.y;
+            } else {
+                f = block_sum(lf, bsm, ph);
+            }
             float xx = x * -mx;
             if (LOG_SP_MIN < xx) { xx = __expf(xx); f -= xx; df += xx * mx; }
             if (dfo) *dfo = df;
@@ -415,7 +449,7 @@ __global__ void __launch_bounds__(SCF * NDS) stats_kernel(StatsArgs a)
             const float yy = lambda * sc;
             if (LOG_SP_MIN < yy && yy < LOG_SP_MAX - 3.f) v = __expf(yy) * yy * P[ty][tx];
         }
-        H = block_sum(v, tmp, &res);
+        H = block_sum(v, bsm, ph);
     }
     lambda *= SCF;  // rescaled even when the root search failed (-1 -> -32)
     E = __fdividef(E, SCF);
@@ -457,7 +491,7 @@ __global__ void __launch_bounds__(SCF * NDS) stats_kernel(StatsArgs a)
                 }
                 __syncthreads();
                 P[ty][tx] = pji;
-                Pj = block_sum(pj, tmp, &res);
+                Pj = block_sum(pj, bsm, ph);
                 sigma += __fdividef(Pj, (float)j);
                 minscore += minu;
                 maxscore += maxu;
