@@ -6,8 +6,9 @@ for sm_100a by ``oracle/build_ref.sh``) run on a B200:
 
   prepare  (here)       seeded workloads -> COMER text profiles -> the
                         reference's makedb + db2bin -> oracle/_ref/inputs/
-  run      (GPU box)    comer -i q.pro -d db -o out -f 1 (JSON output),
-                        options with SCOADJ = no -> gpurun_out/ref_out/
+  run      (B200 host)  comer -i q.pro -d db -o out -f 1 (JSON output),
+                        options with SCOADJ = no -> OUT (argument; default
+                        oracle/_ref/out/)
   collect  (here)       JSON outputs -> tests/golden/ref_<case>.json
 
 The workloads are regenerated from their seeds by comer2_b200.synth, so the
@@ -116,6 +117,6 @@ if __name__ == "__main__":
     if cmd == "prepare":
         prepare()
     elif cmd == "run":
-        run(sys.argv[2] if len(sys.argv) > 2 else os.path.join(ROOT, "gpurun_out", "ref_out"))
+        run(sys.argv[2] if len(sys.argv) > 2 else os.path.join(REF, "out"))
     elif cmd == "collect":
-        collect(sys.argv[2] if len(sys.argv) > 2 else os.path.join(ROOT, "gpurun_out", "ref_out"))
+        collect(sys.argv[2] if len(sys.argv) > 2 else os.path.join(REF, "out"))
