@@ -361,12 +361,16 @@ __global__ void __launch_bounds__(256) map_z_kernel(MapArgs a)
     const float* fs = a.fb + skew_base(a, c);
     const float maxF = a.pairf[m * 4 + 0];
     float s = 0.f;
-    // warp w takes rows w, w + 8, ...; lane i of row (strip t, step k) is cell
-    // (32 t + i, k - i)
+    // warp w takes rows w, w + 8, ... of the [strips x W] rows; lane i of row
+    // (strip t, step k) is cell (32 t + i, k - i).  (t, k) advance without a
+    // division: W >= 32 > 8, so k wraps at most once per step.
+    int t = 0, k = wid;
+#pragma unroll 4
     for (int rw = wid; rw < nrows; rw += 8) {
-        const int t = rw / W, k = rw - t * W;
         const int row = 32 * t + lane, col = k - lane;
         if (row < Lq && col >= 0 && col < L) s += fexp(fs[(long long)rw * 32 + lane] - maxF);
+        k += 8;
+        if (k >= W) { k -= W; t++; }
     }
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
@@ -521,7 +525,7 @@ __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __re
 // Forward and backward sweeps in one launch: the two are independent (the
 // backward sweep writes B beside F), so their strip chains run side by side;
 // item 2 i is the forward sweep's work item i, 2 i + 1 the backward one's.
-__global__ void __launch_bounds__(MAPFBW * 32) map_fb_kernel(MapArgs a, const float* __restrict__ qtrn,
+__global__ void __launch_bounds__(MAPFBW * 32, 8) map_fb_kernel(MapArgs a, const float* __restrict__ qtrn,
                                                      const float* __restrict__ dtrn, const float* __restrict__ qcf)
 {
     // per warp: score ring [32][33], column transitions [64][MTRS], row above

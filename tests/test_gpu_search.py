@@ -108,6 +108,37 @@ def test_long_query_matches_oracle(params, orc32, mode):
     h.close()
 
 
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("lq", [20, 33, 64, 97])
+def test_query_strip_edges_match_oracle(params, orc32, lq, mode):
+    """Queries of one partial strip, a one-row last strip, whole strips and
+    three strips plus one row, against short (< 32 columns) and long profiles
+    with planted homologs: the strip pipelines of the traceback and MAP
+    sweeps at their edges give the oracle's hits, E-values and alignments."""
+    rng = np.random.default_rng(500 + lq)
+    q = S.random_profiles(rng, [lq])
+    lens = np.concatenate([rng.integers(8, 32, 12), rng.integers(32, 400, 28)])
+    db, hom = S.make_db(rng, lens, q, 0.2)
+    w = S.Workload("edge", [q], db, hom)
+    h, hits, thld, logevthld, ss = _run(params, w, mode)
+    ref = _oracle_search(orc32, params, w, ss, thld, logevthld)
+    ref_hits = sorted(k for k, v in ref.items() if "map" in v)
+    assert sorted(int(x["profile"]) for x in hits) == ref_hits
+    flips = 0
+    for x in hits:
+        r = ref[int(x["profile"])]
+        if abs(x["score"] - r["score"]) > 1e-4 * max(1.0, abs(r["score"])):
+            flips += 1
+            continue
+        assert x["logE"] == pytest.approx(r["stats"]["logE"], abs=1e-3)
+        assert x["strings"] == r["map"]["strings"]
+        m = r["map"]
+        assert (x["beg"] >> 16, x["beg"] & 0xFFFF) == (m["begx"], m["begy"])
+        assert (x["end"] >> 16, x["end"] & 0xFFFF) == (m["endx"], m["endy"])
+    assert flips <= max(1, len(hits) // 20)
+    h.close()
+
+
 def test_search_space_matches_oracle(params, orc32):
     w = S.config(0, seed=4, scale=0.05)
     from comer2_b200.native import Handle
