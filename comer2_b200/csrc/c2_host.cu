@@ -459,6 +459,122 @@ static inline float bf16_to_f(uint32_t b)
 
 static inline int ss_index(int state, float prb) { return state * 10 + (int)(prb * 9.999f); }
 
+// Position record of every db position (DR_* layout) for profiles [k0, k1),
+// written from out on (out holds the record of position offsets[k0] first)
+static void pack_records(const c2_profiles* d, float lok, bool mapaln, int k0, int k1, float* out)
+{
+    const int64_t base = d->offsets[k0];
+    for (int k = k0; k < k1; k++) {
+        const int L = d->lengths[k];
+        const int64_t o = d->offsets[k];
+        for (int i = 0; i < L; i++) {
+            const int64_t pos = o + i;
+            float* r = out + (size_t)(pos - base) * DR_STRIDE;
+            memcpy(r + DR_TRG, d->trg + pos * NAA, NAA * 4);
+            memcpy(r + DR_CV, d->cv + pos * NCV, NCV * 4);
+            r[DR_CN] = (d->cvnorm2[pos] + 1.0f) + lok;
+            const float pr = d->cvprior[pos];
+            r[DR_PRIOR] = mapaln ? pr : (float)(int)pr;
+            const float* s3 = d->ss + pos * NSS;
+            r[DR_SS + 0] = s3[0]; r[DR_SS + 1] = s3[1]; r[DR_SS + 2] = s3[2];
+            const int pk = ss_index(0, s3[0]) | (ss_index(1, s3[1]) << 8) | (ss_index(2, s3[2]) << 16);
+            memcpy(r + DR_SSIDX, &pk, 4);
+            r[DR_HD] = s3[2] + 0.1f;
+            r[DR_HD + 1] = 0.f;   // pad
+            r[DR_HD + 2] = 0.f;
+            trn_of(d, k, i, r + DR_TRN);
+            r[DR_AA] = (float)d->aa[pos];
+        }
+    }
+}
+
+// Pinned staging of the record upload: two buffers and their copy events.
+// The destructor waits for copies in flight before freeing the buffers.
+namespace {
+struct RecStage {
+    float* buf[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    cudaStream_t st = nullptr;
+    bool sync = false;
+    ~RecStage()
+    {
+        if (sync) cudaStreamSynchronize(st);
+        for (int b = 0; b < 2; b++) {
+            if (ev[b]) cudaEventDestroy(ev[b]);
+            if (buf[b]) cudaFreeHost(buf[b]);
+        }
+    }
+};
+}  // namespace
+
+// The db position records to d_drec: chunks of whole profiles (up to 2^18
+// positions, 56 MiB of records) are packed by host threads into two pinned
+// buffers in turn, each copied asynchronously while the next chunk is packed
+// (the reference's reader overlaps its double-buffered pinned transfers the
+// same way: cupro/TdDataReader.cpp, CuDeviceMemory.cu:1073).
+static c2_status upload_records(c2_handle* h, const c2_profiles* d)
+{
+    const int P = d->nprofiles;
+    const int64_t N = d->npositions;
+    const int64_t cap = std::max<int64_t>(int64_t(1) << 18, h->Lmax);
+    const float lok = h->sc.lokappa0;
+    const bool mapaln = h->prm.mapaln != 0;
+    RecStage S;
+    for (int b = 0; b < 2; b++) {
+        CK(cudaHostAlloc(reinterpret_cast<void**>(&S.buf[b]), (size_t)cap * DR_STRIDE * 4, cudaHostAllocDefault));
+        CK(cudaEventCreateWithFlags(&S.ev[b], cudaEventDisableTiming));
+    }
+    S.st = h->stream;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nt = (int)std::max(1u, std::min(16u, hw));
+    const int64_t* off = d->offsets;
+    auto end_of = [&](int k) -> int64_t { return k < P ? off[k] : N; };
+    bool used[2] = {false, false};
+    int b = 0;
+    for (int k0 = 0; k0 < P;) {
+        const int64_t p0 = off[k0];
+        // profiles [k0, k1): the most whose positions fit in a buffer (at least
+        // one; cap >= Lmax).  Profiles before the first one starting past the
+        // window start inside it; only the last of them can end past it.
+        int k1 = (int)(std::upper_bound(off + k0 + 1, off + P, p0 + cap) - off);
+        while (k1 > k0 + 1 && end_of(k1) - p0 > cap) k1--;
+        const int64_t p1 = end_of(k1);
+        if (used[b]) CK(cudaEventSynchronize(S.ev[b]));
+        float* out = S.buf[b];
+        // host threads over position ranges of whole profiles
+        const int nth = (int)std::max<int64_t>(1, std::min<int64_t>(nt, (p1 - p0) / 16384));
+        std::vector<std::thread> pool;
+        int ka = k0;
+        for (int t = 0; t < nth; t++) {
+            int kb = k1;
+            if (t + 1 < nth) {
+                const int64_t tgt = p0 + (p1 - p0) * (t + 1) / nth;
+                kb = (int)(std::upper_bound(off + ka, off + k1, tgt) - off);
+                kb = std::max(kb, ka);
+            }
+            if (kb > ka) {
+                float* o = out + (size_t)(off[ka] - p0) * DR_STRIDE;
+                try {
+                    pool.emplace_back(pack_records, d, lok, mapaln, ka, kb, o);
+                } catch (...) {
+                    pack_records(d, lok, mapaln, ka, kb, o);   // no thread to be had: pack here
+                }
+            }
+            ka = kb;
+        }
+        for (auto& th : pool) th.join();
+        S.sync = true;
+        CK(cudaMemcpyAsync(h->db->d_drec.p + (size_t)p0 * DR_STRIDE, out, (size_t)(p1 - p0) * DR_STRIDE * 4,
+                           cudaMemcpyHostToDevice, h->stream));
+        CK(cudaEventRecord(S.ev[b], h->stream));
+        used[b] = true;
+        b ^= 1;
+        k0 = k1;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return C2_OK;
+}
+
 extern "C" c2_status c2_upload_db(c2_handle* h, const c2_profiles* d, uint64_t tot_pos, uint64_t tot_prof)
 {
     if (!h) return C2_ERR_ARG;
@@ -475,38 +591,15 @@ extern "C" c2_status c2_upload_db(c2_handle* h, const c2_profiles* d, uint64_t t
     h->h_plen.assign(d->lengths, d->lengths + P);
     h->h_poff.assign(d->offsets, d->offsets + P);
     h->Lmax = *std::max_element(h->h_plen.begin(), h->h_plen.end());
-    // position records
-    std::vector<float> rec((size_t)N * DR_STRIDE, 0.f);
-    const float lok = h->sc.lokappa0;
-    for (int k = 0; k < P; k++) {
-        const int L = d->lengths[k];
-        const int64_t o = d->offsets[k];
-        for (int i = 0; i < L; i++) {
-            const int64_t pos = o + i;
-            float* r = rec.data() + (size_t)pos * DR_STRIDE;
-            memcpy(r + DR_TRG, d->trg + pos * NAA, NAA * 4);
-            memcpy(r + DR_CV, d->cv + pos * NCV, NCV * 4);
-            r[DR_CN] = (d->cvnorm2[pos] + 1.0f) + lok;
-            const float pr = d->cvprior[pos];
-            r[DR_PRIOR] = h->prm.mapaln ? pr : (float)(int)pr;
-            const float* s3 = d->ss + pos * NSS;
-            r[DR_SS + 0] = s3[0]; r[DR_SS + 1] = s3[1]; r[DR_SS + 2] = s3[2];
-            const int pk = ss_index(0, s3[0]) | (ss_index(1, s3[1]) << 8) | (ss_index(2, s3[2]) << 16);
-            memcpy(r + DR_SSIDX, &pk, 4);
-            r[DR_HD] = s3[2] + 0.1f;
-            trn_of(d, k, i, r + DR_TRN);
-            r[DR_AA] = (float)d->aa[pos];
-        }
-    }
     std::vector<float> bkg(d->bkg, d->bkg + (size_t)P * NAA);
     std::vector<int> order(P);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return d->lengths[a] > d->lengths[b]; });
     std::vector<long long> poff(d->offsets, d->offsets + P);
-    if (h->db->d_drec.ensure(rec.size()) || h->db->d_pbkg.ensure(bkg.size()) || h->db->d_plen.ensure(P) ||
+    if (h->db->d_drec.ensure((size_t)N * DR_STRIDE) || h->db->d_pbkg.ensure(bkg.size()) || h->db->d_plen.ensure(P) ||
         h->db->d_order.ensure(P) || h->db->d_poff.ensure(P) || h->d_best.ensure(P) || h->d_coords.ensure(P))
         return fail(h, C2_ERR_NOMEM, "device allocation for %d profiles / %lld positions failed", P, (long long)N);
-    CK(cudaMemcpy(h->db->d_drec.p, rec.data(), rec.size() * 4, cudaMemcpyHostToDevice));
+    if ((st = upload_records(h, d)) != C2_OK) return st;
     CK(cudaMemcpy(h->db->d_pbkg.p, bkg.data(), bkg.size() * 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->db->d_plen.p, d->lengths, (size_t)P * 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->db->d_order.p, order.data(), (size_t)P * 4, cudaMemcpyHostToDevice));
