@@ -102,6 +102,14 @@ constexpr int P1C_WARP_FLOATS =
 // chunked traceback sweep: p1c_kernel's per-warp layout plus a [32][33]-byte
 // traceback column ring; 11 warps per SM with CV table replicas of 8
 constexpr int P1TC_WARPS = 11, P1TC_CVREP = 8;
+
+// Largest CV maps the shared-memory layouts hold (opt-in shared memory per CTA
+// on sm_100: 227 KB): the traceback sweep, which every search runs, and the
+// tensor-core phase-1 kernel (whose 16 bytes of static shared memory hold the
+// TMEM address).  The reference's cvs2s map has 93 entries.
+constexpr int SMEM_CTA_MAX = 227 * 1024;
+constexpr int P1TC_MAX_CVCARD =
+    (SMEM_CTA_MAX - P1TC_WARPS * 32 * 33 - P1TC_WARPS * P1C_WARP_FLOATS * 4) / (P1TC_CVREP * 4);
 // tensor-core kernel: score ring of 64 anti-diagonals with 36 floats each (the
 // fragment-layout writes and the per-lane wavefront reads are both free of
 // bank conflicts), a column-record ring of 3 chunks plus a mirror of its first
@@ -113,6 +121,7 @@ constexpr int P1T_WARPS = 12;
 constexpr int P1T_RLD = 36, P1T_CRING = 128, P1T_CMOD = 96, P1T_CVREP = 8;
 constexpr unsigned P1T_TMEM_COLS = 512;   // TMEM columns of a CTA (3 warps x 128 per lane quarter)
 constexpr int P1T_WARP_FLOATS = P1C_RING * P1T_RLD + P1T_CRING * P1C_TRS + BND_FLOATS + TC_TILE_WORDS + 4;
+constexpr int P1T_MAX_CVCARD = (SMEM_CTA_MAX - 16 - P1T_WARPS * P1T_WARP_FLOATS * 4) / (P1T_CVREP * 4);
 
 // Epilogue constants of the tensor-core form: x = 2 x (CV score argument)
 // = (2 pownu0 ln2) log2(det) + 2 cterm - 2 prior_q - 2 prior_d, compared

@@ -292,7 +292,8 @@ extern "C" c2_status c2_create(int device, const c2_params* p, c2_handle** out)
     if (!out || !p) return C2_ERR_ARG;
     *out = nullptr;
     if (!p->ssss || p->ssss_card <= 0 || p->ssss_card > MAX_SSSS_CARD || !p->cvs2s_keys ||
-        !p->cvs2s_values || p->cvs2s_card <= 1 || p->cvs2s_card > MAX_CVCARD || p->cvs2s_shift < 0)
+        !p->cvs2s_values || p->cvs2s_card <= 1 || p->cvs2s_card > std::min(MAX_CVCARD, P1TC_MAX_CVCARD) ||
+        p->cvs2s_shift < 0)
         return C2_ERR_ARG;
     if (p->ssswgt <= 0.f || p->cvswgt <= 0.f) return C2_ERR_ARG;  // SS and CV terms both in use
     c2_handle* h = new c2_handle();
@@ -897,6 +898,9 @@ extern "C" c2_status c2_set_score_mode(c2_handle* h, int32_t mode)
         for (float v : h->ssss)
             if (!(v >= SS_FOLD_MIN))
                 return fail(h, C2_ERR_ARG, "tensor-core score form needs SS table entries >= %g", (double)SS_FOLD_MIN);
+        if (h->sc.cvcard > P1T_MAX_CVCARD)
+            return fail(h, C2_ERR_ARG, "tensor-core score form holds CV maps of at most %d entries (this one: %d)",
+                        P1T_MAX_CVCARD, h->sc.cvcard);
     }
     h->score_mode = mode;
     return C2_OK;

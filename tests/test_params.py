@@ -72,3 +72,23 @@ def test_library_exports_header_symbols():
     missing = [n for n in declared if not hasattr(lib, n)]
     assert not missing, missing
     assert sorted(native.EXPORTS) == declared
+
+
+def test_create_rejects_cv_maps_beyond_shared_memory(params):
+    """c2_create refuses, before touching a device, a CV map larger than the
+    traceback sweep's shared-memory layout holds (169 entries; the reference's
+    map has 93)."""
+    import copy
+    from comer2_b200 import native
+    lib = native.load()
+    p = copy.deepcopy(params)
+    card = 200
+    p.cvs2s_keys = np.arange(card, dtype=np.float32) * 0.5 - 2.5
+    p.cvs2s_values = np.zeros(card, np.float32)
+    assert p.cvs2s_card == card
+    keep = native._Keep()
+    sp = native.make_params(p, keep)
+    h = ctypes.c_void_p()
+    st = lib.c2_create(0, ctypes.byref(sp), ctypes.byref(h))
+    assert native.STATUS_NAMES.get(st) == "C2_ERR_ARG"
+    assert not h.value
