@@ -139,7 +139,11 @@ c2_status c2_last_error(const c2_handle* h, char* buf, size_t bufsize);
  * CuBatchProcessing::TransferCPMData (CuBatchProcessing.cuh:79-82) and
  * SetDbDetails(db_len, nseqs) (:73).  db_total_positions/profiles describe
  * the whole database (for the threshold and search space); 0 means "this
- * upload is the whole database". */
+ * upload is the whole database".  The records are packed by up to 16 host
+ * threads into two pinned staging buffers (2 x 56 MiB, held for the call)
+ * and copied on the handle's stream; the call returns when the copies are
+ * done.  Profiles must be contiguous (offsets[k] = sum of earlier lengths),
+ * each of 1..65535 positions. */
 c2_status c2_upload_db(c2_handle* h, const c2_profiles* db,
                        uint64_t db_total_positions, uint64_t db_total_profiles);
 
