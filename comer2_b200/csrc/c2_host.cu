@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -494,6 +495,7 @@ static void pack_records(const c2_profiles* d, float lok, bool mapaln, int k0, i
 namespace {
 struct RecStage {
     float* buf[2] = {nullptr, nullptr};
+    bool pinned[2] = {false, false};
     cudaEvent_t ev[2] = {nullptr, nullptr};
     cudaStream_t st = nullptr;
     bool sync = false;
@@ -502,7 +504,8 @@ struct RecStage {
         if (sync) cudaStreamSynchronize(st);
         for (int b = 0; b < 2; b++) {
             if (ev[b]) cudaEventDestroy(ev[b]);
-            if (buf[b]) cudaFreeHost(buf[b]);
+            if (buf[b] && pinned[b]) cudaFreeHost(buf[b]);
+            else free(buf[b]);
         }
     }
 };
@@ -522,7 +525,16 @@ static c2_status upload_records(c2_handle* h, const c2_profiles* d)
     const bool mapaln = h->prm.mapaln != 0;
     RecStage S;
     for (int b = 0; b < 2; b++) {
-        CK(cudaHostAlloc(reinterpret_cast<void**>(&S.buf[b]), (size_t)cap * DR_STRIDE * 4, cudaHostAllocDefault));
+        const size_t bytes = (size_t)cap * DR_STRIDE * 4;
+        if (cudaHostAlloc(reinterpret_cast<void**>(&S.buf[b]), bytes, cudaHostAllocDefault) == cudaSuccess) {
+            S.pinned[b] = true;
+        } else {
+            // no pinned memory to be had: pageable staging (cudaMemcpyAsync
+            // then returns once it has taken the source over)
+            (void)cudaGetLastError();
+            S.buf[b] = static_cast<float*>(malloc(bytes));
+            if (!S.buf[b]) return fail(h, C2_ERR_NOMEM, "record staging buffer of %zu bytes", bytes);
+        }
         CK(cudaEventCreateWithFlags(&S.ev[b], cudaEventDisableTiming));
     }
     S.st = h->stream;
