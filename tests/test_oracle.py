@@ -5,6 +5,7 @@ of the reference's DP on small cases, and its float build against its double
 build; the threshold and length-adjustment formulas against direct formulas.
 """
 import math
+import os
 
 import numpy as np
 import pytest
@@ -147,6 +148,39 @@ def test_length_adjustment(orc32, params):
     ss, dl = orc32.length_adjustment(params.gapped_lambda, params.gapped_K, params.gapped_alpha,
                                      params.gapped_beta, 400, 22_000_000, 100_000)
     assert (ss, dl) == (400 * 22_000_000, 0)
+
+
+LENADJ = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "ref_lenadj")
+
+
+@pytest.mark.skipif(not os.path.exists(LENADJ), reason="reference harness not built (no reference tree)")
+def test_length_adjustment_matches_reference_code(orc32, params):
+    """The oracle's search space and length adjustment equal those of the
+    reference's own AbstractScoreMatrix::ComputeLengthAdjustment (built from
+    its source by oracle/Makefile) over seeded query and database sizes,
+    adjusted and unadjusted branches included."""
+    import subprocess
+    rng = np.random.default_rng(11)
+    cases = [(400, 24_010_873, 100_000), (3000, 15_000_000, 50_000), (2000, 1000, 3), (1, 100, 1),
+             (150, 680_000, 2000), (1000, 1_000_000, 5000)]
+    for _ in range(200):
+        m = int(rng.integers(1, 5000))
+        N = int(rng.integers(1, 200_000))
+        n = int(N * rng.integers(30, 2000))
+        cases.append((m, n, N))
+    inp = "".join("%d %d %d\n" % c for c in cases)
+    out = subprocess.run([LENADJ, repr(params.gapped_lambda), repr(params.gapped_K), repr(params.gapped_alpha),
+                          repr(params.gapped_beta)], input=inp, capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    got = [tuple(int(x) for x in ln.split()) for ln in out.stdout.strip().splitlines()]
+    assert len(got) == len(cases)
+    nadj = 0
+    for c, r in zip(cases, got):
+        o = tuple(orc32.length_adjustment(params.gapped_lambda, params.gapped_K, params.gapped_alpha,
+                                          params.gapped_beta, *c))
+        assert o == r, (c, o, r)
+        nadj += r[1] > 0
+    assert nadj >= 5   # the Gertz iteration itself is exercised
 
 
 def test_logz_model_is_the_map_forward(params, orc64):
