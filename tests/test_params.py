@@ -92,3 +92,38 @@ def test_create_rejects_cv_maps_beyond_shared_memory(params):
     st = lib.c2_create(0, ctypes.byref(sp), ctypes.byref(h))
     assert native.STATUS_NAMES.get(st) == "C2_ERR_ARG"
     assert not h.value
+
+
+REFTAB = os.path.join(ROOT, "oracle", "_ref", "ref_tables")
+
+
+@pytest.mark.skipif(not os.path.exists(REFTAB), reason="reference table harness not built (no reference tree)")
+def test_tables_match_reference_readers(params):
+    """The SS table and the smoothed CV map that the loader hands to the
+    kernels equal what the reference's own readers (SSSScores, CVS2Scores,
+    built from its source by oracle/Makefile) make of its parameter files."""
+    import subprocess
+    # the harness reads the reference tree's parameter files (the directory is
+    # fixed when oracle/Makefile builds it)
+    out = subprocess.run([REFTAB], capture_output=True, text=True, timeout=60)
+    if out.returncode != 0 and "reading the tables failed" in out.stderr:
+        pytest.skip("the reference tree's parameter files are not on this machine")
+    assert out.returncode == 0, out.stderr
+    ss, cv = out.stdout.splitlines()
+    a = ss.split()
+    card, n = int(a[1]), int(a[2])
+    tri = np.array([float(x) for x in a[3:3 + n]], np.float32)
+    assert card == params.ssss_card and n == card * (card + 1) // 2
+    # VirtScores::GetScore: entry (r, c), r >= c, at c + r (r + 1) / 2
+    full = np.zeros((card, card), np.float32)
+    for r in range(card):
+        for c in range(card):
+            hi, lo = max(r, c), min(r, c)
+            full[r, c] = tri[lo + hi * (hi + 1) // 2]
+    assert np.array_equal(full, np.asarray(params.ssss, np.float32).reshape(card, card))
+    b = cv.split()
+    shift, m = int(b[2]), int(b[3])
+    kv = np.array([float(x) for x in b[4:4 + 2 * m]], np.float32).reshape(m, 2)
+    assert (m, shift) == (params.cvs2s_card, params.cvs2s_shift)
+    assert np.array_equal(kv[:, 0], params.cvs2s_keys)
+    assert np.array_equal(kv[:, 1], params.cvs2s_values)
