@@ -9,10 +9,13 @@
 // src/env files, whose directory the build passes as REF_ENV)
 //   ssss <card> <n> v1 .. vn            (table 0 of probability level 0)
 //   cvs2s <nlevels> <shift> <n> k1 s1 .. kn sn   (level 0, after smoothing)
+//   cvconst <1/kappa0> <PowerNU0> <CTERM>        (the _TCTXVECT constants,
+//                                                 src/libpro/srcpro/TCTXVECT.cpp)
 #include <cstdio>
 
 #include "libpro/srcpro/CVS2Scores.h"
 #include "libpro/srcpro/SSSScores.h"
+#include "libpro/srcpro/TCTXVECT.h"
 
 #ifndef REF_ENV
 #define REF_ENV "."
@@ -41,6 +44,7 @@ int main(int argc, char** argv)
         printf("cvs2s %d %d %d", cc.GetNoTables(), cc.GetShift(0), k->GetSize());
         for (int i = 0; i < k->GetSize(); i++) printf(" %.9g %.9g", k->GetValueAt(i), s->GetValueAt(i));
         printf("\n");
+        printf("cvconst %.9g %.9g %.9g\n", CVS.loKAPPA0, CVS.PowerNU0, CVS.CTERM);
     } catch (...) {
         fprintf(stderr, "reading the tables failed\n");
         return 1;

@@ -109,7 +109,8 @@ def test_tables_match_reference_readers(params):
     if out.returncode != 0 and "reading the tables failed" in out.stderr:
         pytest.skip("the reference tree's parameter files are not on this machine")
     assert out.returncode == 0, out.stderr
-    ss, cv = out.stdout.splitlines()
+    lines = {ln.split()[0]: ln for ln in out.stdout.splitlines()}
+    ss, cv = lines["ssss"], lines["cvs2s"]
     a = ss.split()
     card, n = int(a[1]), int(a[2])
     tri = np.array([float(x) for x in a[3:3 + n]], np.float32)
@@ -127,3 +128,20 @@ def test_tables_match_reference_readers(params):
     assert (m, shift) == (params.cvs2s_card, params.cvs2s_shift)
     assert np.array_equal(kv[:, 0], params.cvs2s_keys)
     assert np.array_equal(kv[:, 1], params.cvs2s_values)
+
+
+@pytest.mark.skipif(not os.path.exists(REFTAB), reason="reference table harness not built (no reference tree)")
+def test_cv_constants_match_reference(orc32):
+    """1/kappa0, PowerNU0 and CTERM of the CV score as the oracle computes
+    them (c2_host.cu's cv_constants follows the same float steps) equal the
+    reference's _TCTXVECT object's values."""
+    import subprocess
+    out = subprocess.run([REFTAB], capture_output=True, text=True, timeout=60)
+    if out.returncode != 0 and "reading the tables failed" in out.stderr:
+        pytest.skip("the reference tree's parameter files are not on this machine")
+    assert out.returncode == 0, out.stderr
+    line = [ln for ln in out.stdout.splitlines() if ln.startswith("cvconst ")][0].split()
+    ref = [np.float32(float(x)) for x in line[1:4]]
+    a, b, c = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+    orc32.lib.orc_cv_constants(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+    assert [np.float32(a.value), np.float32(b.value), np.float32(c.value)] == ref
