@@ -51,7 +51,7 @@ bool read_at(FILE* f, uint64_t off, void* dst, size_t bytes)
 }
 
 struct Header {
-    uint64_t nprof = 0, npos = 0;
+    uint64_t nprof = 0, npos = 0, fsize = 0;
     uint64_t addr[kNSECTIONS] = {};
 };
 
@@ -77,8 +77,26 @@ c2_status read_header(FILE* f, Header& h, char* err, size_t errlen)
         set_err(err, errlen, "invalid number of profiles in the binary database");
         return C2_ERR_ARG;
     }
+    // every position takes more than 4 bytes of the file and every section
+    // lies inside it: a corrupt count or address is refused here, before any
+    // array is sized by it
+    if (fseeko(f, 0, SEEK_END) != 0) {
+        set_err(err, errlen, "cannot size the binary database");
+        return C2_ERR_ARG;
+    }
+    const uint64_t fsize = (uint64_t)ftello(f);
+    if (nn < np || nn > fsize / 4) {
+        set_err(err, errlen, "truncated or inconsistent binary database: number of positions");
+        return C2_ERR_ARG;
+    }
+    for (int s = 0; s < kNSECTIONS; s++)
+        if (h.addr[s] > fsize) {
+            set_err(err, errlen, "truncated or inconsistent binary database: section address");
+            return C2_ERR_ARG;
+        }
     h.nprof = np;
     h.npos = nn;
+    h.fsize = fsize;
     return C2_OK;
 }
 
@@ -102,6 +120,12 @@ extern "C" c2_status c2_db2bin_info(const char* path, int32_t* nprofiles, int64_
     return C2_OK;
 }
 
+namespace {
+c2_status read_sections(FILE* f, const Header& h, int32_t* lengths, int64_t* offsets, float* bkg, float* eno,
+                        float* trn, float* trg, float* cv, float* cvprior, float* cvnorm2, float* ss,
+                        uint8_t* ssstate, uint8_t* aa, char* err, size_t errlen);
+}  // namespace
+
 extern "C" c2_status c2_db2bin_read(const char* path, int32_t* lengths, int64_t* offsets, float* bkg, float* eno,
                                     float* trn, float* trg, float* cv, float* cvprior, float* cvnorm2, float* ss,
                                     uint8_t* ssstate, uint8_t* aa, char* err, size_t errlen)
@@ -118,8 +142,21 @@ extern "C" c2_status c2_db2bin_read(const char* path, int32_t* lengths, int64_t*
     Header h;
     c2_status st = read_header(F.f, h, err, errlen);
     if (st != C2_OK) return st;
+    try {
+        return read_sections(F.f, h, lengths, offsets, bkg, eno, trn, trg, cv, cvprior, cvnorm2, ss, ssstate, aa,
+                             err, errlen);
+    } catch (...) {
+        set_err(err, errlen, "out of host memory reading the binary database");
+        return C2_ERR_NOMEM;
+    }
+}
+
+namespace {
+c2_status read_sections(FILE* f, const Header& h, int32_t* lengths, int64_t* offsets, float* bkg, float* eno,
+                        float* trn, float* trg, float* cv, float* cvprior, float* cvnorm2, float* ss,
+                        uint8_t* ssstate, uint8_t* aa, char* err, size_t errlen)
+{
     const uint64_t P = h.nprof, N = h.npos;
-    FILE* f = F.f;
     int a = 0;
     auto fail = [&](const char* what) {
         set_err(err, errlen, std::string("truncated or inconsistent binary database: ") + what);
@@ -161,9 +198,71 @@ extern "C" c2_status c2_db2bin_read(const char* path, int32_t* lengths, int64_t*
     a += 2;   // HDP1 cluster probabilities and indices: not used by this search path
     if (!read_at(f, h.addr[a++], aa, N)) return fail("residues");
     if (!read_at(f, h.addr[a++], ssstate, N)) return fail("SS states");
+    // the description section ends the file: its last end address must be there
+    uint64_t dend = 0;
+    if (!read_at(f, h.addr[a] + (P - 1) * sizeof(uint64_t), &dend, sizeof dend) || dend < h.addr[a + 1] ||
+        dend > h.fsize)
+        return fail("descriptions");
     for (uint64_t i = 0; i < N; i++) {
         const uint8_t c = ssstate[i];
         ssstate[i] = (c >= 'a' && c <= 'z') ? (uint8_t)(c - 'a' + 'A') : c;   // ' ': no SS prediction
     }
     return C2_OK;
+}
+}  // namespace
+
+extern "C" c2_status c2_db2bin_descriptions(const char* path, char* buf, size_t* bytes, int64_t* offsets, char* err,
+                                            size_t errlen)
+{
+    if (!path || !bytes || (buf && !offsets)) return C2_ERR_ARG;
+    File F;
+    F.f = fopen(path, "rb");
+    if (!F.f) {
+        set_err(err, errlen, std::string("cannot open ") + path);
+        return C2_ERR_ARG;
+    }
+    Header h;
+    c2_status st = read_header(F.f, h, err, errlen);
+    if (st != C2_OK) return st;
+    const uint64_t P = h.nprof;
+    const uint64_t ends_at = h.addr[kNSECTIONS - 2], text_at = h.addr[kNSECTIONS - 1];
+    try {
+        std::vector<uint64_t> ends(P);
+        if (!read_at(F.f, ends_at, ends.data(), P * sizeof(uint64_t))) {
+            set_err(err, errlen, "truncated or inconsistent binary database: description addresses");
+            return C2_ERR_ARG;
+        }
+        uint64_t prev = text_at;
+        for (uint64_t k = 0; k < P; k++) {
+            if (ends[k] < prev + 1 || ends[k] > h.fsize) {
+                set_err(err, errlen, "truncated or inconsistent binary database: description addresses");
+                return C2_ERR_ARG;
+            }
+            prev = ends[k];
+        }
+        const uint64_t total = prev - text_at;   // NUL-terminated descriptions back to back
+        if (!buf) {
+            *bytes = (size_t)total;
+            return C2_OK;
+        }
+        if (*bytes < total) {
+            set_err(err, errlen, "description buffer too small");
+            return C2_ERR_ARG;
+        }
+        if (!read_at(F.f, text_at, buf, total)) {
+            set_err(err, errlen, "truncated or inconsistent binary database: descriptions");
+            return C2_ERR_ARG;
+        }
+        prev = text_at;
+        for (uint64_t k = 0; k < P; k++) {
+            offsets[k] = (int64_t)(prev - text_at);
+            buf[ends[k] - text_at - 1] = 0;   // each description ends with its NUL
+            prev = ends[k];
+        }
+        *bytes = (size_t)total;
+        return C2_OK;
+    } catch (...) {
+        set_err(err, errlen, "out of host memory reading the binary database");
+        return C2_ERR_NOMEM;
+    }
 }

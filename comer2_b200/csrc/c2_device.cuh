@@ -163,6 +163,7 @@ struct P1Args {
     unsigned long long* tbkey;  // [ncand] maximum of the traceback sweep and its cell, packed
     const int* worder;          // traceback sweep: rank -> candidate (longest first)
     const int* items;           // traceback sweep: work item -> rank * nstrips + strip
+    unsigned spin;              // polls before a strip wait gives up (pipe_wait)
     // tensor-core operands (P1K_TENSOR)
     const unsigned* tcdb;       // db B fragments
     const long long* ttile;     // [nprof] first tile of each profile
@@ -209,7 +210,7 @@ struct FinArgs {
 // instead of one.
 namespace c2 {
 constexpr int PIPE_G = 8;                 // columns per progress update
-constexpr unsigned PIPE_SPIN = 1u << 22;  // polls before a wait gives up
+constexpr unsigned PIPE_SPIN = 1u << 22;  // default polls before a wait gives up (c2_set_wait_limit)
 constexpr int PIPE_ERR_TIMEOUT = 3;       // device status of an abandoned wait
 
 __device__ __forceinline__ int pipe_ld_acquire(const int* p)
@@ -224,11 +225,13 @@ __device__ __forceinline__ void pipe_st_release(int* p, int v)
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Warp-uniform wait until *flag >= need (lane 0 polls).  After PIPE_SPIN
-// polls it records PIPE_ERR_TIMEOUT in *status, marks the warp broken (no
-// further waits) and returns; the sweep then finishes with invalid values
-// and the host reports the status.
-__device__ __forceinline__ void pipe_wait(const int* flag, int need, int lane, int* status, bool& broken)
+// Warp-uniform wait until *flag >= need (lane 0 polls).  After `spin` polls
+// (at least one) it records PIPE_ERR_TIMEOUT in *status, marks the warp
+// broken (no further waits) and returns; the sweep then finishes with invalid
+// values -- every cell index stays inside its pair, so nothing is read or
+// written out of bounds -- and the host reports the status.
+__device__ __forceinline__ void pipe_wait(const int* flag, int need, int lane, int* status, bool& broken,
+                                          unsigned spin)
 {
     if (broken) return;
     unsigned it = 0;
@@ -237,7 +240,7 @@ __device__ __forceinline__ void pipe_wait(const int* flag, int need, int lane, i
         if (lane == 0) ok = pipe_ld_acquire(flag) >= need;
         ok = __shfl_sync(0xffffffffu, ok, 0);
         if (ok) break;
-        if (++it >= PIPE_SPIN) {
+        if (++it >= spin) {
             if (lane == 0 && status) atomicCAS(status, 0, PIPE_ERR_TIMEOUT);
             broken = true;
             break;

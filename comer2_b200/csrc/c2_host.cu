@@ -87,6 +87,7 @@ struct c2_handle {
     int nsm = 0;
     int grid = 0;
     int score_mode = C2_SCORE_FP32;   // phase-1 score arithmetic (c2_set_score_mode)
+    unsigned spin = PIPE_SPIN;        // polls before a phase-2 strip wait gives up (c2_set_wait_limit)
     // parameters
     c2_params prm{};
     std::vector<float> ssss, cvkeys, cvvals, nnw;
@@ -297,6 +298,11 @@ extern "C" c2_status c2_create(int device, const c2_params* p, c2_handle** out)
         p->cvs2s_shift < 0)
         return C2_ERR_ARG;
     if (p->ssswgt <= 0.f || p->cvswgt <= 0.f) return C2_ERR_ARG;  // SS and CV terms both in use
+    // SSEMODEL 0 (observed statistics), 1 and 2 (SS18 variants) are built;
+    // MAPALN 0 (Viterbi alignments drawn by FinalizeDP_ALN instead of MAP,
+    // cupro/CuBatchProcessing.cu:477-510) is not, and is refused rather than
+    // answered with MAP alignments
+    if (p->ssemodel < 0 || p->ssemodel > 2 || p->mapaln != 1) return C2_ERR_ARG;
     c2_handle* h = new c2_handle();
     h->device = device;
     cudaError_t e = cudaSetDevice(device);
@@ -671,6 +677,11 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
     if (st != C2_OK) return st;
     if (h->nprof <= 0) return fail(h, C2_ERR_STATE, "set_query before upload_db");
     CK(cudaSetDevice(h->device));
+    // a new search starts with a clear device status word and no results
+    CK(cudaMemsetAsync(h->d_status.p, 0, sizeof(int), h->stream));
+    h->h_cand.clear();
+    h->h_cand_off.clear();
+    h->ncand = h->npass = h->nmap = 0;
     const int Lq = q->lengths[0];
     h->Lq = Lq;
     h->qeno = q->eno ? q->eno[0] : 0.f;
@@ -937,6 +948,7 @@ static void fill_p1(c2_handle* h, P1Args& a)
     a.best = h->d_best.p;
     a.coords = h->d_coords.p;
     a.status = h->d_status.p;
+    a.spin = h->spin;
 }
 
 extern "C" c2_status c2_run_phase1(c2_handle* h)
@@ -983,6 +995,13 @@ extern "C" c2_status c2_set_stream(c2_handle* h, void* stream)
     if (!h) return C2_ERR_ARG;
     CK(cudaStreamSynchronize(h->stream));
     h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+    return C2_OK;
+}
+
+extern "C" c2_status c2_set_wait_limit(c2_handle* h, uint32_t polls)
+{
+    if (!h) return C2_ERR_ARG;
+    h->spin = polls ? polls : PIPE_SPIN;
     return C2_OK;
 }
 
@@ -1128,6 +1147,31 @@ extern "C" c2_status c2_get_finalize(c2_handle* h, c2_dp_result* out, int32_t n)
         out[i].beg = bg[i];
         out[i].end = en[i];
         out[i].passed = pa[i];
+    }
+    return C2_OK;
+}
+
+// The FP32 score and modular-score matrices of one candidate pair, as the
+// traceback sweep of c2_run_finalize stored them (column-major [L][Lq] on the
+// device), copied out row-major [Lq][L].
+extern "C" c2_status c2_get_pair_scores(c2_handle* h, int32_t profile, float* scores, float* modscores)
+{
+    if (!h || (!scores && !modscores)) return C2_ERR_ARG;
+    const auto it = std::lower_bound(h->h_cand.begin(), h->h_cand.end(), profile);
+    if (it == h->h_cand.end() || *it != profile)
+        return fail(h, C2_ERR_ARG, "get_pair_scores: profile %d is not a candidate of the current query", profile);
+    const size_t c = (size_t)(it - h->h_cand.begin());
+    const int Lq = h->Lq, L = h->h_plen[profile];
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    std::vector<float> col((size_t)Lq * L);
+    for (int w = 0; w < 2; w++) {
+        float* out = w ? modscores : scores;
+        if (!out) continue;
+        const float* src = (w ? h->d_mmat.p : h->d_smat.p) + h->h_cand_off[c];
+        CK(cudaMemcpy(col.data(), src, col.size() * 4, cudaMemcpyDeviceToHost));
+        for (int x = 0; x < L; x++)
+            for (int y = 0; y < Lq; y++) out[(size_t)y * L + x] = col[(size_t)x * Lq + y];
     }
     return C2_OK;
 }
@@ -1283,6 +1327,7 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
     a.items = h->d_mapitems.p;
     a.status = h->d_status.p;
     a.counter = h->d_counter.p;
+    a.spin = h->spin;
     a.minpp = h->prm.minpp;
     a.modscores = (h->prm.ssswgt > 0.f || h->prm.cvswgt > 0.f) ? 1 : 0;
     a.qaa = h->d_qaa.p;
@@ -1396,10 +1441,13 @@ extern "C" c2_status c2_search(c2_handle* h, const c2_profiles* q, int32_t* nhit
 // and cudaFree synchronise the device and can fail under memory pressure).
 //
 // Scratch: C2_STATIC_SCRATCH_BYTES = 16 MiB; bytes [0, 256) hold the work
-// counter (zeroed by every call), the rest holds 10 x Lmax floats per warp
-// slot, Lmax being the longest db profile.  The grid shrinks to the number of
-// 8-warp blocks whose slots fit; a database whose longest profile needs more
-// than the whole array for one block (Lmax > 52,428) is rejected.
+// counter (zeroed by every call), the rest holds 10 x Lm floats per warp
+// slot, Lm being the longest db profile rounded up to a multiple of 32.  The
+// grid shrinks to the number of 8-warp blocks whose slots fit; a database
+// whose longest profile needs more than the whole array for one block
+// (Lm > 52,428, i.e. a longest profile above 52,416 positions) is rejected.
+// The kernel scores in FP32 only: a handle in the tensor-core score mode is
+// refused rather than given maxima of the other arithmetic.
 // Every call on a device shares the one array: calls whose kernels overlap on
 // the GPU (different streams, or different handles on one device) race on it.
 // The first call on a device resolves the array's address with
@@ -1418,6 +1466,9 @@ extern "C" c2_status c2_run_phase1_static(c2_handle* h, float* d_best, uint32_t*
 {
     if (!h || !d_best || !d_coords) return C2_ERR_ARG;
     if (h->nprof <= 0 || h->Lq <= 0) return fail(h, C2_ERR_STATE, "run_phase1_static needs a database and a query");
+    if (h->score_mode != C2_SCORE_FP32)
+        return fail(h, C2_ERR_STATE, "run_phase1_static scores in FP32 only; the handle is in score mode %d",
+                    h->score_mode);
     if (h->device < 0 || h->device >= C2_STATIC_MAXDEV)
         return fail(h, C2_ERR_ARG, "run_phase1_static: device %d out of range", h->device);
     CK(cudaSetDevice(h->device));
@@ -1437,9 +1488,9 @@ extern "C" c2_status c2_run_phase1_static(c2_handle* h, float* d_best, uint32_t*
     const size_t nblocks = (C2_STATIC_SCRATCH_BYTES - C2_STATIC_HDR) / per_block;
     if (nblocks < 1)
         return fail(h, C2_ERR_CAPACITY,
-                    "run_phase1_static: longest db profile (%lld positions) exceeds the static scratch limit "
+                    "run_phase1_static: longest db profile (%d positions) exceeds the static scratch limit "
                     "(%zu positions)",
-                    h->botstride / 10, (C2_STATIC_SCRATCH_BYTES - C2_STATIC_HDR) / (10 * sizeof(float) * P1_WARPS));
+                    h->Lmax, ((C2_STATIC_SCRATCH_BYTES - C2_STATIC_HDR) / (10 * sizeof(float) * P1_WARPS)) & ~size_t(31));
     const int grid = (int)std::min<size_t>((size_t)h->grid, nblocks);
     P1Args a;
     fill_p1(h, a);

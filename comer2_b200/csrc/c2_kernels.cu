@@ -796,7 +796,7 @@ p1tc_kernel(P1Args a, const float* __restrict__ qbkg)
         const int cB = corner_b(r, L, edge);
         // columns [0, 32) of the row above, lane i holding column i
         float bc[5];
-        if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken);
+        if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken, a.spin);
 #pragma unroll
         for (int f = 0; f < 5; f++) {
             bc[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : 0.f;
@@ -838,7 +838,7 @@ p1tc_kernel(P1Args a, const float* __restrict__ qbkg)
             // the row above for chunk m + 1, loaded while this stage runs
             const int k0 = 32 * m, k1 = min(k0 + 32, kend);
             if (s > 0 && k0 + 32 < L) {
-                pipe_wait(pf + s - 1, min(k0 + 64, L), lane, a.status, broken);
+                pipe_wait(pf + s - 1, min(k0 + 64, L), lane, a.status, broken, a.spin);
 #pragma unroll
                 for (int f = 0; f < 5; f++) {
                     const int cc = k0 + 32 + lane;

@@ -254,7 +254,7 @@ __device__ __forceinline__ void map_fwd_item(const MapArgs& a, const float* __re
             // buffer rab[32][8] (slot i: column 32 c + i), waited for and loaded
             // at the end of the chunk before
             const float binit[5] = {0.f, MLOG0, MLOG0, MLOG0, MLOG0};
-            if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken);
+            if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken, a.spin);
             {
                 float v[5];
 #pragma unroll
@@ -288,7 +288,7 @@ __device__ __forceinline__ void map_fwd_item(const MapArgs& a, const float* __re
                     const float b4 = rab[src * 8 + 4];
                     if (lane == 0) up = S5{ba.x, ba.y, ba.z, ba.w, b4};
                     if (src == 31) {
-                        if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken);
+                        if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken, a.spin);
                         float v[5];
 #pragma unroll
                         for (int f = 0; f < 5; f++) {
@@ -426,7 +426,7 @@ __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __re
             // buffer rab[32][8] (slot i: column 32 c + i), waited for and loaded
             // at the end of the chunk before
             const float binit[5] = {0.f, MLOG0, MLOG0, MLOG0, MLOG0};
-            if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken);
+            if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken, a.spin);
             {
                 float v[5];
 #pragma unroll
@@ -472,7 +472,7 @@ __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __re
                     const float b4 = rab[src * 8 + 4];
                     if (lane == 0) dn = S5{ba.x, ba.y, ba.z, ba.w, b4};
                     if (src == 31) {
-                        if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken);
+                        if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken, a.spin);
                         float v[5];
 #pragma unroll
                         for (int f = 0; f < 5; f++) {
@@ -606,7 +606,7 @@ __global__ void __launch_bounds__(MAPW * 32, 8) map_dp_kernel(MapArgs a)
             const bool act = r < Lq;
             float mine = 0.f, upp = 0.f;
             // row above the strip, one chunk at a time (lane i: column 32 c + i)
-            if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken);
+            if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken, a.spin);
             float bcur = (s > 0 && lane < L) ? __ldcg(botr + lane) : 0.f;
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             // F + B of the next step's cells is loaded one step ahead, from L2:
@@ -627,7 +627,7 @@ __global__ void __launch_bounds__(MAPW * 32, 8) map_dp_kernel(MapArgs a)
                     const float b0 = __shfl_sync(FULL, bcur, src);
                     if (lane == 0) up = b0;
                     if (src == 31) {
-                        if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken);
+                        if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken, a.spin);
                         bcur = (s > 0 && k + 1 + lane < L) ? __ldcg(botr + k + 1 + lane) : 0.f;
                         pf_line(fs, k + 33 + lane, W);
                         pf_line(bs, k + 33 + lane, W);

@@ -510,10 +510,19 @@ __global__ void __launch_bounds__(SCF * NDS, 2) stats_kernel(StatsArgs a)
         const float l1l2 = (float)((unsigned)Lq * (unsigned)L);
         o[ST_LOGEPA] = (lambda <= 0.f || K <= 0.f) ? __logf(a.refK * l1l2) - a.reflambda * score
                                                    : __logf(K * l1l2) - lambda * score;
-        float mu, scale;
-        predict_evd(a, Lq, L, a.qeno, a.peno[p], lambda, &mu, &scale);
-        o[ST_MU] = mu; o[ST_SCALE] = scale;
-        o[ST_LOGE] = evalue_ss18(a, Lq, L, score, psts, K, mu, scale);
+        if (a.ssemodel == 0) {
+            // observed-statistics model: the expected gapped lambda and K over
+            // the search space (CalcSignificanceObsDynPlmProfile,
+            // src/libmycu/cuss/CuBatchSS_dynplm.cu:594-676; CalculateEvalueObs,
+            // CuBatchSS_SS18.cuh:372-384)
+            o[ST_MU] = 0.f; o[ST_SCALE] = 0.f;
+            o[ST_LOGE] = __logf(a.expgK * a.searchspace) - a.expglambda * score;
+        } else {
+            float mu, scale;
+            predict_evd(a, Lq, L, a.qeno, a.peno[p], lambda, &mu, &scale);
+            o[ST_MU] = mu; o[ST_SCALE] = scale;
+            o[ST_LOGE] = evalue_ss18(a, Lq, L, score, psts, K, mu, scale);
+        }
     }
 }
 

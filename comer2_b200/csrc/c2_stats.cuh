@@ -62,6 +62,7 @@ struct MapArgs {
     unsigned long long* pairk;  // [nmap] MAP DP maximum and end cell, packed for atomicMax
     int* status;
     int* counter;
+    unsigned spin;              // polls before a strip wait gives up (pipe_wait)
     float minpp;
     int modscores;
     // traceback outputs

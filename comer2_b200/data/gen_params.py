@@ -57,4 +57,7 @@ def main(root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("COMER2_REFERENCE", "")
+    if not root:
+        sys.exit("usage: gen_params.py <reference-root>  (or set COMER2_REFERENCE)")
+    main(root)

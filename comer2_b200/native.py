@@ -28,6 +28,7 @@ EXPORTS = [
     "c2_launch_count", "c2_run_stats", "c2_run_map", "c2_get_hits", "c2_search", "c2_get_search_space",
     "c2_run_phase1_static", "c2_set_score_mode", "c2_logz_fwd", "c2_logz_bwd", "c2_logz_cells",
     "c2_db2bin_info", "c2_db2bin_read", "c2_share_db", "c2_search_batch", "c2_format_report",
+    "c2_set_wait_limit", "c2_get_pair_scores", "c2_db2bin_descriptions",
 ]
 
 REPORT_PLAIN = 0
@@ -194,6 +195,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.c2_get_search_space.argtypes = [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]
     lib.c2_run_phase1_static.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     lib.c2_set_score_mode.argtypes = [C.c_void_p, C.c_int32]
+    lib.c2_set_wait_limit.argtypes = [C.c_void_p, C.c_uint32]
+    lib.c2_get_pair_scores.argtypes = [C.c_void_p, C.c_int32, _fp, _fp]
+    lib.c2_db2bin_descriptions.argtypes = [C.c_char_p, C.c_void_p, P(C.c_size_t), _i64p, C.c_char_p, C.c_size_t]
     lib.c2_logz_fwd.argtypes = [C.c_void_p, _i32p, C.c_int32, _fp, C.c_float, C.c_float, _fp]
     lib.c2_logz_bwd.argtypes = [C.c_void_p, _fp]
     lib.c2_logz_cells.argtypes = [C.c_void_p, C.c_int32, _fp, _fp]
@@ -366,6 +370,10 @@ class Handle:
         """SCORE_FP32 (CUDA cores) or SCORE_BF16_TC (split-BF16 tensor-core contractions)."""
         self._ck(self.lib.c2_set_score_mode(self._h, mode), "c2_set_score_mode")
 
+    def set_wait_limit(self, polls: int):
+        """Polls before a phase-2 strip wait gives up (0: the default; c2_set_wait_limit)."""
+        self._ck(self.lib.c2_set_wait_limit(self._h, int(polls)), "c2_set_wait_limit")
+
     def phase1(self):
         out = (c2_p1_result * self.nprof)()
         self._ck(self.lib.c2_get_phase1(self._h, out, self.nprof), "c2_get_phase1")
@@ -383,6 +391,15 @@ class Handle:
         dt = np.dtype([("score", np.float32), ("profile", np.int32), ("psts", np.int32),
                        ("beg", np.uint32), ("end", np.uint32), ("passed", np.int32)])
         return np.frombuffer(out, dtype=dt, count=n).copy()
+
+    def pair_scores(self, profile: int, L: int):
+        """(scores, modular scores), each [Lq][L] float32, of a finalised pair
+        of the current query as the device computed them (c2_get_pair_scores)."""
+        sm = np.zeros((self.Lq, L), np.float32)
+        mm = np.zeros((self.Lq, L), np.float32)
+        self._ck(self.lib.c2_get_pair_scores(self._h, int(profile), _ptr(sm, _fp), _ptr(mm, _fp)),
+                 "c2_get_pair_scores")
+        return sm, mm
 
     def run_stats(self) -> int:
         n = C.c_int32()
@@ -506,3 +523,25 @@ def read_db2bin(path: str):
         raise C2Error("c2_db2bin_read: %s" % err.value.decode())
     return ProfileSet(lengths, offsets, bkg, eno, trn, trg, cv, cvp, cvn, ss, sss, aa,
                       np.zeros((N + P, 7), np.int32), np.zeros((N, 20), np.int32))
+
+
+def read_db2bin_descriptions(path: str):
+    """Profile descriptions of a database written by the reference's db2bin
+    (c2_db2bin_descriptions), in the database's profile order."""
+    lib = load()
+    err = C.create_string_buffer(512)
+    n = C.c_size_t(0)
+    st = lib.c2_db2bin_descriptions(path.encode(), None, C.byref(n), None, err, 512)
+    if st != C2_OK:
+        raise C2Error("c2_db2bin_descriptions: %s" % err.value.decode())
+    P, N = C.c_int32(), C.c_int64()
+    st = lib.c2_db2bin_info(path.encode(), C.byref(P), C.byref(N), err, 512)
+    if st != C2_OK:
+        raise C2Error("c2_db2bin_info: %s" % err.value.decode())
+    buf = C.create_string_buffer(max(n.value, 1))
+    off = np.zeros(P.value, np.int64)
+    st = lib.c2_db2bin_descriptions(path.encode(), buf, C.byref(n), _ptr(off, _i64p), err, 512)
+    if st != C2_OK:
+        raise C2Error("c2_db2bin_descriptions: %s" % err.value.decode())
+    raw = buf.raw
+    return [raw[o:raw.index(b"\0", o)].decode() for o in off]

@@ -45,9 +45,9 @@ typedef struct {
     float ssswgt;          /* SSSWGT */
     float cvswgt;          /* CVSWGT */
     float minpp;           /* MINPP */
-    int32_t mapaln;        /* MAPALN */
+    int32_t mapaln;        /* MAPALN: must be 1 (MAP alignments); 0 is refused */
     int32_t x_uninf;       /* X_UNINF */
-    int32_t ssemodel;      /* SSEMODEL */
+    int32_t ssemodel;      /* SSEMODEL: 0 observed statistics, 1 and 2 the SS18 variants */
     const float* ssss;     /* SS score table, ssss_card x ssss_card, symmetric */
     int32_t ssss_card;
     const float* cvs2s_keys;    /* smoothed CV score map: keys, step 0.5 */
@@ -171,6 +171,16 @@ c2_status c2_run_finalize(c2_handle* h, int32_t* ncand);
 /* Copy finalisation records (in ascending profile order). */
 c2_status c2_get_finalize(c2_handle* h, c2_dp_result* out, int32_t n);
 
+/* The FP32 score and modular-score matrices (row-major [Lq][L], L the db
+ * profile's length) of one finalised pair of the current query, as the
+ * traceback sweep of c2_run_finalize computed them; either pointer may be
+ * NULL.  Valid until the next c2_run_finalize.  C2_ERR_ARG if the profile is
+ * not among the finalised pairs.  The reference keeps these matrices in its
+ * device heap (sections ddsBegOfOrgScores / ddsEndOfOrgScores,
+ * src/libmycu/cupro/CuBatchProcessing.cu:451-452) without an accessor; this
+ * one serves inspection and the parity tests. */
+c2_status c2_get_pair_scores(c2_handle* h, int32_t profile, float* scores, float* modscores);
+
 /* Compute the statistics and E-values of the finalised pairs whose score
  * exceeds the threshold; replaces CuBatchSS::CalculateAlnStatisticsDevice
  * (src/libmycu/cuss/CuBatchSS.cu:196-265).  *npassed receives their number. */
@@ -264,6 +274,16 @@ c2_status c2_set_stream(c2_handle* h, void* stream);
 /* Synchronize the handle's stream. */
 c2_status c2_sync(c2_handle* h);
 
+/* Bound of the waits between the strips of one pair in the phase-2 sweeps
+ * (traceback DP, MAP forward/backward, MAP DP): a strip polls its
+ * predecessor's progress at most `polls` times (0 restores the default,
+ * 2^22 polls with 128 ns sleeps, about a second), then gives up, the sweep
+ * finishes without faulting and c2_get_finalize / c2_run_stats /
+ * c2_get_hits return C2_ERR_DEVICE ("a strip wait ... timed out").  The
+ * next c2_set_query clears the error.  No counterpart in the reference,
+ * whose kernels neither wait on one another nor time out. */
+c2_status c2_set_wait_limit(c2_handle* h, uint32_t polls);
+
 /* Number of kernel launches issued by the handle since creation. */
 c2_status c2_launch_count(const c2_handle* h, uint64_t* n);
 
@@ -291,6 +311,14 @@ c2_status c2_db2bin_info(const char* path, int32_t* nprofiles, int64_t* npositio
 c2_status c2_db2bin_read(const char* path, int32_t* lengths, int64_t* offsets, float* bkg, float* eno, float* trn,
                          float* trg, float* cv, float* cvprior, float* cvnorm2, float* ss, uint8_t* ssstate,
                          uint8_t* aa, char* err, size_t errlen);
+/* Profile descriptions of the same database (the section after the
+ * description end addresses, PMProfileModel.cpp:1529-1533): buf == NULL gives
+ * the bytes needed in *bytes; otherwise buf receives the NUL-terminated
+ * descriptions back to back and offsets[k] (nprofiles entries) the start of
+ * profile k's.  The reference's reader keeps them for its result writers
+ * (CuDbReader / TdDataReader, cupro/TdDataReader.cpp:132-975). */
+c2_status c2_db2bin_descriptions(const char* path, char* buf, size_t* bytes, int64_t* offsets, char* err,
+                                 size_t errlen);
 
 /* Differentiable alignment (no counterpart in the reference, whose
  * forward-backward only feeds its MAP alignment).  Log-partition of the MAP
@@ -314,11 +342,13 @@ c2_status c2_logz_bwd(c2_handle* h, float* grad);
  * exp(F.MM + B.MM - logZ).  Either pointer may be NULL. */
 c2_status c2_logz_cells(c2_handle* h, int32_t pair, float* dlogz_ds, float* post);
 
-/* Phase 1 (as c2_run_phase1) that allocates nothing.  No counterpart in the
- * reference.  Its scratch (work counter, strip-boundary rows) lives in one
- * static 16 MiB device array per device, so the grid is limited to the 8-warp
- * blocks whose boundary rows fit; a database whose longest profile exceeds
- * 52,428 positions is rejected with C2_ERR_CAPACITY.  Results go to caller-owned
+/* Phase 1 (as c2_run_phase1 in the default C2_SCORE_FP32 mode) that allocates
+ * nothing.  No counterpart in the reference.  It always scores in FP32; a
+ * handle set to C2_SCORE_BF16_TC is refused with C2_ERR_STATE.  Its scratch
+ * (work counter, strip-boundary rows) lives in one static 16 MiB device array
+ * per device, so the grid is limited to the 8-warp blocks whose boundary rows
+ * fit; a database whose longest profile exceeds 52,416 positions is rejected
+ * with C2_ERR_CAPACITY.  Results go to caller-owned
  * device arrays of nprofiles entries (d_best: DP maxima, d_coords: packed
  * (column << 16 | row) of the maximum), in the layout c2_get_phase1 reports.
  * The array is shared by every call on the device: calls that overlap on the

@@ -5,9 +5,14 @@
 # are the reference oracle run on a B200 to pin this project's results; the
 # product never calls them.
 #
-# usage: oracle/build_ref.sh [reference-root]   (default /root/reference)
+# usage: oracle/build_ref.sh <reference-root>
+#        (or COMER2_REFERENCE=<reference-root> oracle/build_ref.sh)
 set -euo pipefail
-REF=${1:-/root/reference}
+REF=${1:-${COMER2_REFERENCE:-}}
+if [ -z "$REF" ] || [ ! -d "$REF/src" ]; then
+    echo "usage: $0 <reference-root> (the reference's source tree, with src/)" >&2
+    exit 2
+fi
 SRC="$REF/src"
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"

@@ -893,6 +893,15 @@ void orc_stats(const orc_stats_in* in, const real* S, const unsigned char* qaa, 
         out->logEpA = LOG((real)in->refK * l1l2) - (real)in->reflambda * (real)in->score;
     else
         out->logEpA = LOG(K * l1l2) - lambda * (real)in->score;
+    if (in->ssemodel == 0) {
+        /* observed-statistics model (CalcSignificanceObsDynPlmProfile,
+         * CuBatchSS_dynplm.cu:594-676; CalculateEvalueObs,
+         * CuBatchSS_SS18.cuh:372-384) */
+        out->mu = 0;
+        out->scale = 0;
+        out->logE = LOG((real)in->expgK * (real)in->searchspace) - (real)in->expglambda * (real)in->score;
+        return;
+    }
     real mu, scale;
     predict_evd(in, lambda, &mu, &scale);
     out->mu = mu;

@@ -18,7 +18,12 @@ BUILD = os.path.join(HERE, "_build")
 
 
 def build():
-    r = subprocess.run(["make", "-s", "-C", HERE], capture_output=True, text=True)
+    """Build the oracle; with COMER2_REFERENCE naming the reference's source
+    tree, also the helpers compiled from its own sources (oracle/_ref)."""
+    cmd = ["make", "-s", "-C", HERE]
+    if os.environ.get("COMER2_REFERENCE"):
+        cmd.append("REF=" + os.environ["COMER2_REFERENCE"])
+    r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
 

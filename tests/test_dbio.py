@@ -78,3 +78,48 @@ def test_db2bin_rejects_other_files(tmp_path):
     f.write_bytes(b"not a database" * 10)
     with pytest.raises(C2Error, match="not a COMER binary profile database"):
         read_db2bin(str(f))
+
+
+@needs_ref
+def test_db2bin_truncated_and_corrupt_files(tmp_path):
+    """A database cut short anywhere, or with a corrupt count, address or
+    profile length, is refused with an error message; nothing is read or
+    sized beyond the file."""
+    import struct
+    from comer2_b200.native import C2Error, read_db2bin
+    rng = np.random.default_rng(6)
+    ps = S.random_profiles(rng, [31, 12, 140, 64])
+    path, _ = _make_db(tmp_path, ps)
+    data = open(path, "rb").read()
+    hdr = len(b"COMER profile bin database v2.2")
+    bad = tmp_path / "bad.bin"
+    cuts = sorted({hdr - 3, hdr + 4, hdr + 16 + 8 * 40, len(data) // 3, len(data) // 2, len(data) - 300,
+                   len(data) - 1})
+    for cut in cuts:
+        bad.write_bytes(data[:cut])
+        with pytest.raises(C2Error, match="truncated|not a COMER"):
+            read_db2bin(str(bad))
+    # number of positions far beyond the file
+    b = bytearray(data)
+    b[hdr + 8:hdr + 16] = struct.pack("<Q", 1 << 60)
+    bad.write_bytes(bytes(b))
+    with pytest.raises(C2Error, match="number of positions"):
+        read_db2bin(str(bad))
+    # a section address past the end of the file
+    b = bytearray(data)
+    b[hdr + 16 + 8 * 30:hdr + 16 + 8 * 31] = struct.pack("<Q", len(data) + 4096)
+    bad.write_bytes(bytes(b))
+    with pytest.raises(C2Error, match="section address"):
+        read_db2bin(str(bad))
+    # a profile length that breaks the sum of lengths
+    b = bytearray(data)
+    a0 = struct.unpack("<Q", b[hdr + 16:hdr + 24])[0]
+    b[a0:a0 + 4] = struct.pack("<i", 5)
+    bad.write_bytes(bytes(b))
+    with pytest.raises(C2Error, match="sum of profile lengths"):
+        read_db2bin(str(bad))
+    # the intact file still reads, descriptions included (in the database's
+    # profile order, which makedb chooses)
+    from comer2_b200.native import read_db2bin_descriptions
+    assert read_db2bin(path).nprofiles == 4
+    assert sorted(read_db2bin_descriptions(path)) == ["p%04d" % k for k in range(4)]

@@ -131,3 +131,63 @@ def test_finalize_matches_oracle(params, orc32):
         assert rec["passed"] == int(rec["score"] > thld)
     assert agree >= 0.9 * n
     assert h.launch_count() >= 3
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_phase1_and_finalize_on_device_scores(params, orc32, mode):
+    """With an E-value threshold that makes every pair with a positive
+    maximum a candidate, the device's own FP32 score matrix of every pair is
+    available (c2_get_pair_scores).  On it the oracle's DP must reproduce the
+    phase-1 maximum (FP32 form: to 1e-6 relative with the same cell; BF16
+    form: within its 2e-3 relative candidate margin) and the finalisation
+    (score to 1e-5 relative, positive count, path ends); and the device's
+    scores must equal the oracle's cell by cell (5e-5 absolute: CUDA's fast
+    logarithm against the C library's), except
+    cells where the context-vector score crosses a table bin edge (one table
+    step, < 0.05), which must be rare."""
+    import copy
+    p = copy.deepcopy(params)
+    p.eval = 1e12
+    w = S.config(1, seed=3, scale=0.002)
+    h = _handle(p, mode)
+    h.upload_db(w.db)
+    h.set_query(w.queries[0])
+    thld, _ = h.thresholds()
+    assert thld == 0.0
+    h.run_phase1()
+    best, coords = h.phase1()
+    n = h.run_finalize()
+    fin = {int(r["profile"]): r for r in h.finalize(n)}
+    qo = orc32.profile(w.queries[0])
+    ncell = nedge = 0
+    for k in range(w.db.nprofiles):
+        if not best[k] > 0:
+            continue
+        assert k in fin
+        L = int(w.db.lengths[k])
+        do = orc32.profile(w.db, k)
+        sm, mm = h.pair_scores(k, L)
+        rs, rm = orc32.score_matrix(qo, do)
+        d = np.abs(sm - rs)
+        edge = d > 5e-5
+        assert (d[edge] < 0.05).all(), (k, float(d.max()))
+        assert np.abs(mm - rm)[~edge].max(initial=0.0) <= 5e-5
+        ncell += d.size
+        nedge += int(edge.sum())
+        ob, ox, oy, nt, bt = orc32.dp(qo, do, sm, with_btck=True)
+        if mode == 0:
+            assert float(best[k]) == pytest.approx(ob, rel=1e-6, abs=1e-6), k
+            if nt == 1:
+                assert (int(coords[k]) >> 16, int(coords[k]) & 0xFFFF) == (ox, oy), k
+        else:
+            assert abs(float(best[k]) - ob) <= 2e-3 * max(1.0, abs(ob)), k
+        sc, ps, bx, by = orc32.finalize(sm, bt, ob, ox, oy)
+        r = fin[k]
+        assert float(r["score"]) == pytest.approx(sc, rel=1e-5, abs=1e-5), k
+        if nt == 1:
+            assert int(r["psts"]) == ps, k
+            assert (int(r["beg"]) >> 16, int(r["beg"]) & 0xFFFF) == (bx, by), k
+            assert (int(r["end"]) >> 16, int(r["end"]) & 0xFFFF) == (ox, oy), k
+    assert ncell > 1_000_000
+    assert nedge <= 1e-4 * ncell, (nedge, ncell)
+    h.close()

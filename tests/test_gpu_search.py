@@ -37,6 +37,36 @@ def _oracle_search(orc, prm, w, searchspace, thld, logevthld):
     return out
 
 
+def _recheck_on_device_scores(h, orc, prm, w, x, searchspace, logevthld):
+    """Every stage after the score matrix, checked on the device's own FP32
+    score and modular-score matrices of the hit's pair (c2_get_pair_scores):
+    the oracle's DP, finalisation, statistics and MAP run on exactly the
+    scores the GPU used, so no rounding of the score terms can excuse a
+    difference.  DP scores within 1e-5 relative, log E within 1e-3, the
+    alignment (strings, counts, coordinates) identical."""
+    q = w.queries[0]
+    k = int(x["profile"])
+    off, nd = int(w.db.offsets[k]), int(w.db.lengths[k])
+    sm, mm = h.pair_scores(k, nd)
+    qo, do = orc.profile(q), orc.profile(w.db, k)
+    best, bx, by, nt, bt = orc.dp(qo, do, sm, with_btck=True)
+    score, psts, _, _ = orc.finalize(sm, bt, best, bx, by)
+    assert x["score"] == pytest.approx(score, rel=1e-5, abs=1e-5), k
+    st = orc.stats(sm, q.aa, w.db.aa[off:off + nd], score, psts, q.eno[0], w.db.eno[k], float(searchspace),
+                   prm.x_uninf)
+    assert (x["smin"], x["smax"]) == (st["min"], st["max"]), k
+    assert x["logE"] == pytest.approx(st["logE"], abs=1e-3), k
+    assert x["logEpA"] == pytest.approx(st["logEpA"], abs=1e-3), k
+    assert x["lambda_"] == pytest.approx(st["lambda_"], rel=1e-3, abs=1e-5), k
+    assert x["K"] == pytest.approx(st["K"], rel=1e-3, abs=1e-6), k
+    assert not (logevthld < st["logE"]), k
+    m = orc.map(qo, do, sm, mm, st["logEpA"], qss=q.ssstate, dss=w.db.ssstate[off:off + nd])
+    assert x["strings"] == m["strings"], k
+    assert (x["alnlen"], x["idts"], x["psts"], x["gaps"]) == (m["alnlen"], m["idts"], m["psts"], m["gaps"]), k
+    assert (x["beg"] >> 16, x["beg"] & 0xFFFF) == (m["begx"], m["begy"]), k
+    assert (x["end"] >> 16, x["end"] & 0xFFFF) == (m["endx"], m["endy"]), k
+
+
 def _run(params, w, mode=0):
     from comer2_b200.native import Handle
     h = Handle(params, 0)
@@ -65,8 +95,11 @@ def test_search_matches_oracle(params, orc32, seed, mode):
         k = int(x["profile"])
         r = ref[k]
         st, m = r["stats"], r["map"]
+        _recheck_on_device_scores(h, orc32, params, w, x, ss, logevthld)
         dscore = abs(x["score"] - r["score"])
         if dscore > 1e-4 * max(1.0, abs(r["score"])):
+            # a context-vector bin edge moved a cell by one table step: the
+            # hit was checked above on the device's scores
             flips += 1
             assert dscore < 0.1
             continue
@@ -99,6 +132,7 @@ def test_long_query_matches_oracle(params, orc32, mode):
     assert sorted(int(x["profile"]) for x in hits) == ref_hits
     for x in hits:
         r = ref[int(x["profile"])]
+        _recheck_on_device_scores(h, orc32, params, w, x, ss, logevthld)
         if abs(x["score"] - r["score"]) > 1e-4 * max(1.0, abs(r["score"])):
             continue
         assert x["logE"] == pytest.approx(r["stats"]["logE"], abs=1e-3)
@@ -127,6 +161,7 @@ def test_query_strip_edges_match_oracle(params, orc32, lq, mode):
     flips = 0
     for x in hits:
         r = ref[int(x["profile"])]
+        _recheck_on_device_scores(h, orc32, params, w, x, ss, logevthld)
         if abs(x["score"] - r["score"]) > 1e-4 * max(1.0, abs(r["score"])):
             flips += 1
             continue
@@ -208,3 +243,83 @@ def test_bf16_form_with_a_cv_table_off_its_index_range(params):
     assert np.allclose(r0["score"], r1["score"], rtol=1e-4, atol=1e-4)
     assert np.allclose(r0["logE"], r1["logE"], atol=1e-3)
     assert a0 == a1
+
+
+def test_observed_statistics_model_matches_oracle(params, orc32):
+    """SSEMODEL 0 (E-values from the expected gapped lambda and K over the
+    search space, the reference's CalcSignificanceObsDynPlmProfile): hit
+    list, log E-values and alignments equal the oracle's."""
+    import copy
+    p = copy.deepcopy(params)
+    p.ssemodel = 0
+    w = S.config(1, seed=9, scale=0.003)
+    h, hits, thld, logevthld, ss = _run(p, w, 1)
+    ref = _oracle_search(orc32, p, w, ss, thld, logevthld)
+    assert sorted(int(x["profile"]) for x in hits) == sorted(k for k, v in ref.items() if "map" in v)
+    assert len(hits) > 0
+    for x in hits:
+        _recheck_on_device_scores(h, orc32, p, w, x, ss, logevthld)
+        st = ref[int(x["profile"])]["stats"]
+        expect = np.log(np.float32(p.gapped_K) * np.float32(ss)) - np.float32(p.gapped_lambda) * x["score"]
+        assert x["logE"] == pytest.approx(float(expect), abs=1e-3)
+        assert x["logE"] == pytest.approx(st["logE"], abs=1e-3)
+    h.close()
+
+
+def test_config0_in_full_matches_oracle(params, orc32):
+    """The plain-method workload at full size (1 x 150 vs 2,000 profiles of
+    U[50,500]): the oracle's hit list, and every hit checked through all
+    stages on the device's own scores."""
+    w = S.config(0, seed=0, scale=1.0)
+    assert w.db.nprofiles == 2000
+    h, hits, thld, logevthld, ss = _run(params, w, 1)
+    ref = _oracle_search(orc32, params, w, ss, thld, logevthld)
+    assert sorted(int(x["profile"]) for x in hits) == sorted(k for k, v in ref.items() if "map" in v)
+    for x in hits:
+        _recheck_on_device_scores(h, orc32, params, w, x, ss, logevthld)
+    h.close()
+
+
+def test_config1_sample_with_all_homologs_matches_oracle(params, orc32):
+    """A 2,500-profile sample of the database-scan workload (1 x 400,
+    lognormal lengths) holding all its planted homologs, searched with the
+    full database's size for the thresholds and search space: the oracle's
+    hit list, and every hit checked on the device's own scores."""
+    w = S.config(1, seed=1, scale=0.025)
+    assert w.db.nprofiles == 2500 and len(w.homologs) >= 40
+    from comer2_b200.native import Handle
+    h = Handle(params, 0)
+    h.set_score_mode(1)
+    h.upload_db(w.db, total_positions=24_000_000, total_profiles=100_000)
+    hits = h.search(w.queries[0])
+    thld, logevthld = h.thresholds()
+    ss, _ = h.search_space()
+    ref = _oracle_search(orc32, params, w, ss, thld, logevthld)
+    assert sorted(int(x["profile"]) for x in hits) == sorted(k for k, v in ref.items() if "map" in v)
+    for k in w.homologs:
+        assert k in [int(x["profile"]) for x in hits]
+    for x in hits:
+        _recheck_on_device_scores(h, orc32, params, w, x, ss, logevthld)
+    h.close()
+
+
+def test_masked_residues_matches_oracle(params, orc32):
+    """'X' residues in the query and the database: with X_UNINF their cells
+    are left out of the score statistics (the reference's
+    CalcScoreProbsXuninfDynPlmProfile) and 'X' pairs count as identities in
+    the alignment middle line like any letter; hits, statistics and
+    alignments equal the oracle's."""
+    w = S.config(1, seed=2, scale=0.003)
+    rng = np.random.default_rng(123)
+    for ps in (w.queries[0], w.db):
+        idx = rng.choice(ps.npositions, size=max(1, ps.npositions // 15), replace=False)
+        ps.aa[idx] = ord("X")
+    assert params.x_uninf == 1
+    h, hits, thld, logevthld, ss = _run(params, w, 1)
+    ref = _oracle_search(orc32, params, w, ss, thld, logevthld)
+    assert sorted(int(x["profile"]) for x in hits) == sorted(k for k, v in ref.items() if "map" in v)
+    assert len(hits) > 0
+    assert any("X" in x["strings"][0] for x in hits)
+    for x in hits:
+        _recheck_on_device_scores(h, orc32, params, w, x, ss, logevthld)
+    h.close()

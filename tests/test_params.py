@@ -145,3 +145,16 @@ def test_cv_constants_match_reference(orc32):
     a, b, c = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
     orc32.lib.orc_cv_constants(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
     assert [np.float32(a.value), np.float32(b.value), np.float32(c.value)] == ref
+
+
+def test_create_refuses_unbuilt_options(params):
+    """MAPALN 0 (Viterbi alignments instead of MAP) and SSEMODEL outside
+    0..2 are refused by c2_create with C2_ERR_ARG before any device call,
+    rather than answered with results of another configuration."""
+    import copy
+    from comer2_b200.native import C2Error, Handle
+    for field, value in (("mapaln", 0), ("ssemodel", 3), ("ssemodel", -1)):
+        p = copy.deepcopy(params)
+        setattr(p, field, value)
+        with pytest.raises(C2Error, match="C2_ERR_ARG"):
+            Handle(p, 0)
