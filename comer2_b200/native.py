@@ -453,6 +453,7 @@ class Handle:
         s = make_profiles(q, k)
         n = C.c_int32()
         self._ck(self.lib.c2_search(self._h, C.byref(s), C.byref(n)), "c2_search")
+        self.Lq = int(q.lengths[0])
         return self.hits_arrays(n.value) if arrays else self.hits(n.value)
 
     def search_batch(self, queries: ProfileSet, nworkers: int = 1):

@@ -250,15 +250,17 @@ def test_observed_statistics_model_matches_oracle(params, orc32):
     search space, the reference's CalcSignificanceObsDynPlmProfile): hit
     list, log E-values and alignments equal the oracle's."""
     import copy
+    from oracle_py import Oracle
     p = copy.deepcopy(params)
     p.ssemodel = 0
+    orc = Oracle(p, 32)   # the oracle's statistics follow its own parameters
     w = S.config(1, seed=9, scale=0.003)
     h, hits, thld, logevthld, ss = _run(p, w, 1)
-    ref = _oracle_search(orc32, p, w, ss, thld, logevthld)
+    ref = _oracle_search(orc, p, w, ss, thld, logevthld)
     assert sorted(int(x["profile"]) for x in hits) == sorted(k for k, v in ref.items() if "map" in v)
     assert len(hits) > 0
     for x in hits:
-        _recheck_on_device_scores(h, orc32, p, w, x, ss, logevthld)
+        _recheck_on_device_scores(h, orc, p, w, x, ss, logevthld)
         st = ref[int(x["profile"])]["stats"]
         expect = np.log(np.float32(p.gapped_K) * np.float32(ss)) - np.float32(p.gapped_lambda) * x["score"]
         assert x["logE"] == pytest.approx(float(expect), abs=1e-3)
