@@ -43,22 +43,57 @@ cudaError_t launch_fin(const FinArgs& a, cudaStream_t st);
 
 using namespace c2;
 
+// Device memory budget of a handle (c2_set_device_memory_limit; the
+// reference's --dev-mem): bytes held by the handle's buffers, and the limit
+// (0: none).  Shared by the buffers that draw on it, which may outlive the
+// handle (a database store kept by another handle).
+struct Budget {
+    size_t limit = 0;
+    size_t used = 0;
+    std::mutex mu;
+};
+
 template <typename T>
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
+    std::shared_ptr<Budget> bud;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            cudaFree(p);
+            if (bud) {
+                std::lock_guard<std::mutex> lk(bud->mu);
+                bud->used -= n * sizeof(T);
+            }
+        }
         p = nullptr;
         n = 0;
+        bud.reset();
     }
-    cudaError_t ensure(size_t cnt) {
+    // at least cnt elements; a request beyond the budget fails as an
+    // allocation failure would, before cudaMalloc
+    cudaError_t ensure(size_t cnt, const std::shared_ptr<Budget>& b = nullptr) {
         if (cnt <= n && p) return cudaSuccess;
         release();
         if (cnt == 0) cnt = 1;
-        cudaError_t e = cudaMalloc((void**)&p, cnt * sizeof(T));
-        if (e == cudaSuccess) n = cnt;
+        const size_t bytes = cnt * sizeof(T);
+        if (b) {
+            std::lock_guard<std::mutex> lk(b->mu);
+            if (b->limit && b->used + bytes > b->limit) return cudaErrorMemoryAllocation;
+            b->used += bytes;
+        }
+        cudaError_t e = cudaMalloc((void**)&p, bytes);
+        if (e == cudaSuccess) {
+            n = cnt;
+            bud = b;
+        } else {
+            p = nullptr;
+            if (b) {
+                std::lock_guard<std::mutex> lk(b->mu);
+                b->used -= bytes;
+            }
+        }
         return e;
     }
 };
@@ -87,6 +122,7 @@ struct c2_handle {
     int nsm = 0;
     int grid = 0;
     int score_mode = C2_SCORE_FP32;   // phase-1 score arithmetic (c2_set_score_mode)
+    std::shared_ptr<Budget> budget = std::make_shared<Budget>();   // c2_set_device_memory_limit
     unsigned spin = PIPE_SPIN;        // polls before a phase-2 strip wait gives up (c2_set_wait_limit)
     // parameters
     c2_params prm{};
@@ -163,6 +199,12 @@ struct c2_handle {
     DevBuf<char> d_aln, d_alnpack;
     DevBuf<long long> d_alnoff;
     int alnstride = 0;
+    // hits of a search run in candidate groups (c2_search under a device
+    // memory budget), merged and sorted; c2_get_hits serves them when valid
+    bool acc_valid = false;
+    int ngroups = 1;
+    std::vector<c2_hit> acc_hits;
+    std::vector<char> acc_alns;
     // worker handles of c2_search_batch (sharing this handle's database)
     std::vector<c2_handle*> workers;
 };
@@ -338,13 +380,13 @@ extern "C" c2_status c2_create(int device, const c2_params* p, c2_handle** out)
         if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { st = C2_ERR_CUDA; break; }
         h->nsm = prop.multiProcessorCount;
         h->grid = h->nsm * p1_blocks_per_sm(sc.cvcard);
-        if (h->d_ssss.ensure(h->ssss.size()) || h->d_cvvals.ensure(h->cvvals.size()) ||
-            h->d_status.ensure(1) || h->d_counter.ensure(4)) { st = C2_ERR_NOMEM; break; }
+        if (h->d_ssss.ensure(h->ssss.size(), h->budget) || h->d_cvvals.ensure(h->cvvals.size(), h->budget) ||
+            h->d_status.ensure(1, h->budget) || h->d_counter.ensure(4, h->budget)) { st = C2_ERR_NOMEM; break; }
         if (cudaMemcpy(h->d_ssss.p, h->ssss.data(), h->ssss.size() * 4, cudaMemcpyHostToDevice) ||
             cudaMemcpy(h->d_cvvals.p, h->cvvals.data(), h->cvvals.size() * 4, cudaMemcpyHostToDevice) ||
             cudaMemset(h->d_status.p, 0, sizeof(int))) { st = C2_ERR_CUDA; break; }
         if (!h->nnw.empty()) {
-            if (h->d_nnw.ensure(h->nnw.size()) ||
+            if (h->d_nnw.ensure(h->nnw.size(), h->budget) ||
                 cudaMemcpy(h->d_nnw.p, h->nnw.data(), h->nnw.size() * 4, cudaMemcpyHostToDevice)) { st = C2_ERR_CUDA; break; }
         }
     } while (0);
@@ -615,8 +657,8 @@ extern "C" c2_status c2_upload_db(c2_handle* h, const c2_profiles* d, uint64_t t
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return d->lengths[a] > d->lengths[b]; });
     std::vector<long long> poff(d->offsets, d->offsets + P);
-    if (h->db->d_drec.ensure((size_t)N * DR_STRIDE) || h->db->d_pbkg.ensure(bkg.size()) || h->db->d_plen.ensure(P) ||
-        h->db->d_order.ensure(P) || h->db->d_poff.ensure(P) || h->d_best.ensure(P) || h->d_coords.ensure(P))
+    if (h->db->d_drec.ensure((size_t)N * DR_STRIDE, h->budget) || h->db->d_pbkg.ensure(bkg.size(), h->budget) || h->db->d_plen.ensure(P, h->budget) ||
+        h->db->d_order.ensure(P, h->budget) || h->db->d_poff.ensure(P, h->budget) || h->d_best.ensure(P, h->budget) || h->d_coords.ensure(P, h->budget))
         return fail(h, C2_ERR_NOMEM, "device allocation for %d profiles / %lld positions failed", P, (long long)N);
     if ((st = upload_records(h, d)) != C2_OK) return st;
     CK(cudaMemcpy(h->db->d_pbkg.p, bkg.data(), bkg.size() * 4, cudaMemcpyHostToDevice));
@@ -624,8 +666,8 @@ extern "C" c2_status c2_upload_db(c2_handle* h, const c2_profiles* d, uint64_t t
     CK(cudaMemcpy(h->db->d_order.p, order.data(), (size_t)P * 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->db->d_poff.p, poff.data(), (size_t)P * 8, cudaMemcpyHostToDevice));
     // raw transitions, residues, SS states and ENOs for the statistics and MAP stages
-    if (h->db->d_dtrn.ensure((size_t)(N + P) * 7) || h->db->d_daa.ensure((size_t)N) || h->db->d_dss.ensure((size_t)N) ||
-        h->db->d_peno.ensure((size_t)P))
+    if (h->db->d_dtrn.ensure((size_t)(N + P) * 7, h->budget) || h->db->d_daa.ensure((size_t)N, h->budget) || h->db->d_dss.ensure((size_t)N, h->budget) ||
+        h->db->d_peno.ensure((size_t)P, h->budget))
         return fail(h, C2_ERR_NOMEM, "device allocation of db side arrays failed");
     CK(cudaMemcpy(h->db->d_dtrn.p, d->trn, (size_t)(N + P) * 7 * 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->db->d_daa.p, d->aa, (size_t)N, cudaMemcpyHostToDevice));
@@ -636,7 +678,7 @@ extern "C" c2_status c2_upload_db(c2_handle* h, const c2_profiles* d, uint64_t t
     // strip-boundary scratch: per warp slot, two rows of 5 states
     const int lm = (h->Lmax + 31) & ~31;
     h->botstride = 10LL * lm;
-    if (h->d_bot.ensure((size_t)h->grid * P1_WARPS * h->botstride))
+    if (h->d_bot.ensure((size_t)h->grid * P1_WARPS * h->botstride, h->budget))
         return fail(h, C2_ERR_NOMEM, "strip-boundary scratch allocation failed");
     h->Lq = 0;
     h->db->tc_ready = false;
@@ -663,8 +705,8 @@ extern "C" c2_status c2_share_db(c2_handle* dst, const c2_handle* src)
     const int P = dst->nprof;
     const int lm = (dst->Lmax + 31) & ~31;
     dst->botstride = 10LL * lm;
-    if (dst->d_best.ensure(P) || dst->d_coords.ensure(P) ||
-        dst->d_bot.ensure((size_t)dst->grid * P1_WARPS * dst->botstride))
+    if (dst->d_best.ensure(P, dst->budget) || dst->d_coords.ensure(P, dst->budget) ||
+        dst->d_bot.ensure((size_t)dst->grid * P1_WARPS * dst->botstride, dst->budget))
         return fail(dst, C2_ERR_NOMEM, "share_db: per-handle buffers for %d profiles failed", P);
     dst->Lq = 0;
     return C2_OK;
@@ -682,6 +724,8 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
     h->h_cand.clear();
     h->h_cand_off.clear();
     h->ncand = h->npass = h->nmap = 0;
+    h->acc_valid = false;
+    h->ngroups = 1;
     const int Lq = q->lengths[0];
     h->Lq = Lq;
     h->qeno = q->eno ? q->eno[0] : 0.f;
@@ -713,7 +757,7 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
         rr[QR_C + 0] = cMI[r]; rr[QR_C + 1] = cIM[r]; rr[QR_C + 2] = cDN[r];
         if (r > 0) { rr[QR_CP + 0] = cMI[r - 1]; rr[QR_CP + 1] = cIM[r - 1]; rr[QR_CP + 2] = cDN[r - 1]; }
     }
-    if (h->d_qrec.ensure(h->h_qrec.size()) || h->d_qbkg.ensure(NAA))
+    if (h->d_qrec.ensure(h->h_qrec.size(), h->budget) || h->d_qbkg.ensure(NAA, h->budget))
         return fail(h, C2_ERR_NOMEM, "query allocation failed");
     // tensor-core query operands (layouts in c2_device.cuh): context vectors
     // (k = 19: 1, the 1/kappa0 column) and SS row tables
@@ -737,7 +781,7 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
             for (int r = 0; r < Lq; r++)
                 for (int c = 0; c < card; c++)
                     qU[((size_t)(r / 32) * MAX_SSSS_CARD + c) * 32 + (r % 32)] = U[(size_t)r * 32 + c];
-            if (h->d_qU.ensure(qU.size())) return fail(h, C2_ERR_NOMEM, "query SS table allocation failed");
+            if (h->d_qU.ensure(qU.size(), h->budget)) return fail(h, C2_ERR_NOMEM, "query SS table allocation failed");
             CK(cudaMemcpyAsync(h->d_qU.p, qU.data(), qU.size() * 4, cudaMemcpyHostToDevice, h->stream));
             CK(cudaStreamSynchronize(h->stream));
         }
@@ -774,7 +818,7 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
                                 (r < Lq && k < NAA) ? q->trg[(size_t)r * NAA + k] : 0.f;
                         }
                     }
-        if (h->d_qa.ensure(qa.size()) || h->d_qaaf.ensure(qaa.size()))
+        if (h->d_qa.ensure(qa.size(), h->budget) || h->d_qaaf.ensure(qaa.size(), h->budget))
             return fail(h, C2_ERR_NOMEM, "query operand allocation failed");
         CK(cudaMemcpyAsync(h->d_qa.p, qa.data(), qa.size() * 4, cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(h->d_qaaf.p, qaa.data(), qaa.size() * 4, cudaMemcpyHostToDevice, h->stream));
@@ -803,8 +847,8 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
             c[3] = pMI; c[4] = pIM; c[5] = pDN;
             pMI = mi; pIM = im; pDN = dn;
         }
-        if (h->d_qcf.ensure(qcf.size()) || h->d_qtrn.ensure((size_t)(Lq + 1) * 7) || h->d_qaa.ensure(Lq) ||
-            h->d_qss.ensure(Lq))
+        if (h->d_qcf.ensure(qcf.size(), h->budget) || h->d_qtrn.ensure((size_t)(Lq + 1) * 7, h->budget) || h->d_qaa.ensure(Lq, h->budget) ||
+            h->d_qss.ensure(Lq, h->budget))
             return fail(h, C2_ERR_NOMEM, "query side arrays allocation failed");
         CK(cudaMemcpyAsync(h->d_qcf.p, qcf.data(), qcf.size() * 4, cudaMemcpyHostToDevice, h->stream));
         // the same column -1 states with exact exp/log, for the log-partition model
@@ -828,7 +872,7 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
                 pMI = mi; pIM = im; pDN = dn;
             }
         }
-        if (h->d_qcfx.ensure(qx.size())) return fail(h, C2_ERR_NOMEM, "query side arrays allocation failed");
+        if (h->d_qcfx.ensure(qx.size(), h->budget)) return fail(h, C2_ERR_NOMEM, "query side arrays allocation failed");
         CK(cudaMemcpyAsync(h->d_qcfx.p, qx.data(), qx.size() * 4, cudaMemcpyHostToDevice, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         h->adj_fwd_done = false;
@@ -897,8 +941,8 @@ static c2_status tc_prepare_db(c2_handle* h)
         tt[k] = ntiles;
         ntiles += (long long)((h->h_plen[k] + 31) / 32) * 4;
     }
-    if (h->db->d_ttile.ensure(h->nprof) || h->db->d_tcdb.ensure((size_t)ntiles * TC_TILE_WORDS) ||
-        h->db->d_cold.ensure((size_t)h->npos * P1C_TRS))
+    if (h->db->d_ttile.ensure(h->nprof, h->budget) || h->db->d_tcdb.ensure((size_t)ntiles * TC_TILE_WORDS, h->budget) ||
+        h->db->d_cold.ensure((size_t)h->npos * P1C_TRS, h->budget))
         return fail(h, C2_ERR_NOMEM, "tensor-core db operands (%lld tiles) allocation failed", ntiles);
     CK(cudaMemcpyAsync(h->db->d_ttile.p, tt.data(), (size_t)h->nprof * 8, cudaMemcpyHostToDevice, h->stream));
     CK(launch_tc_pack(h->db->d_drec.p, h->db->d_poff.p, h->db->d_plen.p, h->db->d_ttile.p, h->nprof, h->db->d_tcdb.p, h->db->d_cold.p,
@@ -998,6 +1042,22 @@ extern "C" c2_status c2_set_stream(c2_handle* h, void* stream)
     return C2_OK;
 }
 
+extern "C" c2_status c2_set_device_memory_limit(c2_handle* h, uint64_t bytes)
+{
+    if (!h) return C2_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->budget->mu);
+    h->budget->limit = (size_t)bytes;
+    return C2_OK;
+}
+
+extern "C" c2_status c2_get_device_memory_use(const c2_handle* h, uint64_t* bytes)
+{
+    if (!h || !bytes) return C2_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->budget->mu);
+    *bytes = h->budget->used;
+    return C2_OK;
+}
+
 extern "C" c2_status c2_set_wait_limit(c2_handle* h, uint32_t polls)
 {
     if (!h) return C2_ERR_ARG;
@@ -1024,29 +1084,35 @@ extern "C" c2_status c2_get_phase1(c2_handle* h, c2_p1_result* out, int32_t n)
     return C2_OK;
 }
 
-extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
+// Pairs whose phase-1 maximum passes the candidate cut, ascending profile
+// order.  FinalizeDPPro: maxsc <= scorethld -> not passed.  With BF16 phase-1
+// scores the cut is lowered by a margin far above their error; the FP32
+// traceback sweep then applies the exact cut (fin_kernel).
+static c2_status select_candidates(c2_handle* h, std::vector<int>& cand)
 {
-    if (!h || !ncand) return C2_ERR_ARG;
-    if (h->nprof <= 0 || h->Lq <= 0) return fail(h, C2_ERR_STATE, "run_finalize needs a database and a query");
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->stream));
     std::vector<float> b(h->nprof);
     CK(cudaMemcpy(b.data(), h->d_best.p, (size_t)h->nprof * 4, cudaMemcpyDeviceToHost));
-    h->h_cand.clear();
-    h->h_cand_off.clear();
-    long long acc = 0;
-    // FinalizeDPPro: maxsc <= scorethld -> not passed.  With BF16 phase-1
-    // scores the candidate cut is lowered by a margin far above their error;
-    // the FP32 traceback sweep then applies the exact cut (fin_kernel).
     const float cut = (h->score_mode == C2_SCORE_FP32)
                           ? h->scorethld
                           : h->scorethld - C2_TC_MARGIN * std::max(1.0f, std::fabs(h->scorethld));
-    for (int k = 0; k < h->nprof; k++) {
-        if (b[k] > cut) {
-            h->h_cand.push_back(k);
-            h->h_cand_off.push_back(acc);
-            acc += (long long)h->Lq * h->h_plen[k];
-        }
+    cand.clear();
+    for (int k = 0; k < h->nprof; k++)
+        if (b[k] > cut) cand.push_back(k);
+    return C2_OK;
+}
+
+// Traceback sweep and finalisation of the candidate pairs `cand` (ascending
+// profile order).
+static c2_status finalize_set(c2_handle* h, const std::vector<int>& cand, int32_t* ncand)
+{
+    h->h_cand = cand;
+    h->h_cand_off.clear();
+    long long acc = 0;
+    for (int k : cand) {
+        h->h_cand_off.push_back(acc);
+        acc += (long long)h->Lq * h->h_plen[k];
     }
     h->ncand = (int)h->h_cand.size();
     *ncand = h->ncand;
@@ -1055,10 +1121,10 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     // strip-pipeline scratch: two halves, the second for the MAP backward sweep
     h->bnd_half = (size_t)(acc / h->Lq) * 10;
     h->prog_half = (size_t)nc * ((h->Lq + 31) / 32);
-    if (h->d_cand_prof.ensure(nc) || h->d_cand_off.ensure(nc) || h->d_btck.ensure((size_t)acc) ||
-        h->d_smat.ensure((size_t)acc) || h->d_mmat.ensure((size_t)acc) || h->d_fscore.ensure(nc) || h->d_fpsts.ensure(nc) ||
-        h->d_fpassed.ensure(nc) || h->d_fbeg.ensure(nc) || h->d_fend.ensure(nc) ||
-        h->d_bnd.ensure(2 * h->bnd_half) || h->d_tbkey.ensure(nc) || h->d_prog.ensure(2 * h->prog_half))
+    if (h->d_cand_prof.ensure(nc, h->budget) || h->d_cand_off.ensure(nc, h->budget) || h->d_btck.ensure((size_t)acc, h->budget) ||
+        h->d_smat.ensure((size_t)acc, h->budget) || h->d_mmat.ensure((size_t)acc, h->budget) || h->d_fscore.ensure(nc, h->budget) || h->d_fpsts.ensure(nc, h->budget) ||
+        h->d_fpassed.ensure(nc, h->budget) || h->d_fbeg.ensure(nc, h->budget) || h->d_fend.ensure(nc, h->budget) ||
+        h->d_bnd.ensure(2 * h->bnd_half, h->budget) || h->d_tbkey.ensure(nc, h->budget) || h->d_prog.ensure(2 * h->prog_half, h->budget))
         return fail(h, C2_ERR_NOMEM, "finalisation scratch for %d pairs (%lld cells) failed", nc, acc);
     CK(cudaMemcpyAsync(h->d_cand_prof.p, h->h_cand.data(), (size_t)nc * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_cand_off.p, h->h_cand_off.data(), (size_t)nc * 8, cudaMemcpyHostToDevice, h->stream));
@@ -1071,7 +1137,7 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
         std::vector<int> lens(nc), items;
         for (int i = 0; i < nc; i++) lens[i] = h->h_plen[h->h_cand[wo[i]]];
         strip_items(lens, (h->Lq + 31) / 32, h->nsm * P1TC_WARPS, items);
-        if (h->d_worder.ensure(nc) || h->d_tbitems.ensure(items.size()))
+        if (h->d_worder.ensure(nc, h->budget) || h->d_tbitems.ensure(items.size(), h->budget))
             return fail(h, C2_ERR_NOMEM, "candidate order allocation failed");
         CK(cudaMemcpyAsync(h->d_worder.p, wo.data(), (size_t)nc * 4, cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(h->d_tbitems.p, items.data(), items.size() * 4, cudaMemcpyHostToDevice, h->stream));
@@ -1121,6 +1187,17 @@ extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
     CK(launch_fin(f, h->stream));
     h->launches++;
     return C2_OK;
+}
+
+extern "C" c2_status c2_run_finalize(c2_handle* h, int32_t* ncand)
+{
+    if (!h || !ncand) return C2_ERR_ARG;
+    if (h->nprof <= 0 || h->Lq <= 0) return fail(h, C2_ERR_STATE, "run_finalize needs a database and a query");
+    h->acc_valid = false;
+    std::vector<int> cand;
+    c2_status st = select_candidates(h, cand);
+    if (st != C2_OK) return st;
+    return finalize_set(h, cand, ncand);
 }
 
 extern "C" c2_status c2_get_finalize(c2_handle* h, c2_dp_result* out, int32_t n)
@@ -1212,7 +1289,7 @@ extern "C" c2_status c2_run_stats(c2_handle* h, int32_t* npassed)
     h->npass = (int)h->h_p2.size();
     *npassed = h->npass;
     if (h->npass == 0) return C2_OK;
-    if (h->d_p2.ensure(h->npass) || h->d_stats.ensure((size_t)h->npass * STATS_NOUT))
+    if (h->d_p2.ensure(h->npass, h->budget) || h->d_stats.ensure((size_t)h->npass * STATS_NOUT, h->budget))
         return fail(h, C2_ERR_NOMEM, "statistics buffers for %d pairs failed", h->npass);
     CK(cudaMemcpyAsync(h->d_p2.p, h->h_p2.data(), (size_t)h->npass * 4, cudaMemcpyHostToDevice, h->stream));
     StatsArgs a;
@@ -1286,16 +1363,16 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
     long long skl = 0;
     for (int c = 0; c < h->ncand; c++) skl += (long long)h->h_plen[h->h_cand[c]] + 31;
     const size_t fbn = (size_t)32 * ((h->Lq + 31) / 32) * (size_t)skl;
-    if (h->d_mapcand.ensure(nm) || h->d_mappass.ensure(nm) || h->d_fb.ensure(fbn) || h->d_bb.ensure(fbn) ||
-        h->d_pairf.ensure((size_t)nm * 4) ||
-        h->d_pairc.ensure(nm) || h->d_alninfo.ensure((size_t)nm * 8) || h->d_aln.ensure((size_t)nm * 5 * h->alnstride) ||
-        h->d_pairk.ensure(nm))
+    if (h->d_mapcand.ensure(nm, h->budget) || h->d_mappass.ensure(nm, h->budget) || h->d_fb.ensure(fbn, h->budget) || h->d_bb.ensure(fbn, h->budget) ||
+        h->d_pairf.ensure((size_t)nm * 4, h->budget) ||
+        h->d_pairc.ensure(nm, h->budget) || h->d_alninfo.ensure((size_t)nm * 8, h->budget) || h->d_aln.ensure((size_t)nm * 5 * h->alnstride, h->budget) ||
+        h->d_pairk.ensure(nm, h->budget))
         return fail(h, C2_ERR_NOMEM, "MAP buffers for %d pairs failed", nm);
     {
         std::vector<int> lens(nm), items;
         for (int i = 0; i < nm; i++) lens[i] = h->h_plen[h->h_cand[h->h_mapcand[i]]];
         strip_items(lens, (h->Lq + 31) / 32, h->grid * P1_WARPS, items);
-        if (h->d_mapitems.ensure(items.size())) return fail(h, C2_ERR_NOMEM, "MAP work table allocation failed");
+        if (h->d_mapitems.ensure(items.size(), h->budget)) return fail(h, C2_ERR_NOMEM, "MAP work table allocation failed");
         CK(cudaMemcpyAsync(h->d_mapitems.p, items.data(), items.size() * 4, cudaMemcpyHostToDevice, h->stream));
         CK(cudaStreamSynchronize(h->stream));
     }
@@ -1343,9 +1420,8 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
     return C2_OK;
 }
 
-extern "C" c2_status c2_get_hits(c2_handle* h, c2_hit* hits, int32_t n, char* alns, size_t* aln_bytes)
+static c2_status hits_direct(c2_handle* h, c2_hit* hits, int32_t n, char* alns, size_t* aln_bytes)
 {
-    if (!h || !aln_bytes) return C2_ERR_ARG;
     CK(cudaStreamSynchronize(h->stream));
     int stw = 0;
     CK(cudaMemcpy(&stw, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
@@ -1381,7 +1457,7 @@ extern "C" c2_status c2_get_hits(c2_handle* h, c2_hit* hits, int32_t n, char* al
         }
     }
     if (nm > 0) {
-        if (h->d_alnoff.ensure((size_t)nm) || h->d_alnpack.ensure(need))
+        if (h->d_alnoff.ensure((size_t)nm, h->budget) || h->d_alnpack.ensure(need, h->budget))
             return fail(h, C2_ERR_NOMEM, "alignment packing buffers failed");
         CK(cudaMemcpyAsync(h->d_alnoff.p, off.data(), (size_t)nm * 8, cudaMemcpyHostToDevice, h->stream));
         CK(launch_aln_pack(h->d_aln.p, h->alnstride, h->d_alninfo.p, h->d_alnoff.p, nm, h->d_alnpack.p, h->stream));
@@ -1419,6 +1495,92 @@ extern "C" c2_status c2_get_hits(c2_handle* h, c2_hit* hits, int32_t n, char* al
     return C2_OK;
 }
 
+extern "C" c2_status c2_get_hits(c2_handle* h, c2_hit* hits, int32_t n, char* alns, size_t* aln_bytes)
+{
+    if (!h || !aln_bytes) return C2_ERR_ARG;
+    if (!h->acc_valid) return hits_direct(h, hits, n, alns, aln_bytes);
+    const int nm = (int)h->acc_hits.size();
+    if (!alns || !hits) {
+        *aln_bytes = h->acc_alns.size();
+        return (hits || alns) ? C2_ERR_ARG : C2_OK;
+    }
+    if (n < nm || *aln_bytes < h->acc_alns.size())
+        return fail(h, C2_ERR_ARG, "output buffers too small (%d hits, %zu bytes)", nm, h->acc_alns.size());
+    std::copy(h->acc_hits.begin(), h->acc_hits.end(), hits);
+    std::copy(h->acc_alns.begin(), h->acc_alns.end(), alns);
+    return C2_OK;
+}
+
+// Phase-2 buffers sized by the candidate pairs (released between groups)
+static void release_phase2(c2_handle* h)
+{
+    h->d_cand_prof.release(); h->d_cand_off.release(); h->d_btck.release(); h->d_smat.release();
+    h->d_mmat.release(); h->d_fscore.release(); h->d_fpsts.release(); h->d_fpassed.release();
+    h->d_fbeg.release(); h->d_fend.release(); h->d_bnd.release(); h->d_tbkey.release(); h->d_prog.release();
+    h->d_worder.release(); h->d_tbitems.release(); h->d_mapitems.release(); h->d_p2.release(); h->d_stats.release();
+    h->d_mapcand.release(); h->d_mappass.release(); h->d_alninfo.release(); h->d_fb.release(); h->d_bb.release();
+    h->d_pairf.release(); h->d_pairc.release(); h->d_pairk.release(); h->d_aln.release(); h->d_alnpack.release();
+    h->d_alnoff.release();
+}
+
+// Device bytes phase 2 takes for one candidate pair of db length L: score,
+// modular-score and traceback matrices, strip-boundary rows and progress
+// words, the MAP sweeps' F and B in wavefront order, the alignment rows, and
+// the per-pair records (an upper estimate of the buffers finalize_set,
+// c2_run_stats, c2_run_map and c2_get_hits size by the pairs).
+static size_t pair_scratch_bytes(const c2_handle* h, int L)
+{
+    const size_t Lq = (size_t)h->Lq, ns = (Lq + 31) / 32;
+    return 9 * Lq * (size_t)L + 2 * 10 * 4 * (size_t)L + 2 * 4 * ns + 4 * ns * 2 + 2 * 4 * 32 * ns * ((size_t)L + 31) +
+           2 * 5 * (Lq + (size_t)h->Lmax + 1) + 512;
+}
+
+// Candidate groups whose phase-2 scratch fits the handle's device memory
+// budget (one group without a budget).  The phase-2 buffers of an earlier
+// search are released first, so the budget's use is the fixed part.
+static c2_status plan_groups(c2_handle* h, const std::vector<int>& cand, std::vector<std::vector<int>>& groups)
+{
+    groups.clear();
+    size_t limit, used;
+    {
+        std::lock_guard<std::mutex> lk(h->budget->mu);
+        limit = h->budget->limit;
+    }
+    if (limit == 0 || cand.empty()) {
+        groups.push_back(cand);
+        return C2_OK;
+    }
+    release_phase2(h);
+    {
+        std::lock_guard<std::mutex> lk(h->budget->mu);
+        used = h->budget->used;
+    }
+    const size_t margin = size_t(1) << 20;
+    if (used + margin >= limit)
+        return fail(h, C2_ERR_NOMEM, "device memory budget of %zu bytes leaves nothing for phase 2 (%zu in use)", limit,
+                    used);
+    const size_t avail = (limit - used - margin) / 10 * 9;
+    std::vector<int> g;
+    size_t gb = 0;
+    for (int k : cand) {
+        const size_t b = pair_scratch_bytes(h, h->h_plen[k]);
+        if (b > avail)
+            return fail(h, C2_ERR_NOMEM,
+                        "device memory budget: the phase-2 scratch of one pair (profile %d, %d x %d cells, %zu bytes) "
+                        "exceeds the %zu bytes left",
+                        k, h->Lq, h->h_plen[k], b, avail);
+        if (gb + b > avail && !g.empty()) {
+            groups.push_back(g);
+            g.clear();
+            gb = 0;
+        }
+        g.push_back(k);
+        gb += b;
+    }
+    if (!g.empty()) groups.push_back(g);
+    return C2_OK;
+}
+
 extern "C" c2_status c2_search(c2_handle* h, const c2_profiles* q, int32_t* nhits)
 {
     if (!h || !q || !nhits) return C2_ERR_ARG;
@@ -1426,9 +1588,63 @@ extern "C" c2_status c2_search(c2_handle* h, const c2_profiles* q, int32_t* nhit
     int32_t n = 0;
     if ((st = c2_set_query(h, q)) != C2_OK) return st;
     if ((st = c2_run_phase1(h)) != C2_OK) return st;
-    if ((st = c2_run_finalize(h, &n)) != C2_OK) return st;
-    if ((st = c2_run_stats(h, &n)) != C2_OK) return st;
-    if ((st = c2_run_map(h, nhits)) != C2_OK) return st;
+    std::vector<int> cand;
+    if ((st = select_candidates(h, cand)) != C2_OK) return st;
+    std::vector<std::vector<int>> groups;
+    if ((st = plan_groups(h, cand, groups)) != C2_OK) return st;
+    h->ngroups = (int)groups.size();
+    if (groups.size() <= 1) {
+        if ((st = finalize_set(h, cand, &n)) != C2_OK) return st;
+        if ((st = c2_run_stats(h, &n)) != C2_OK) return st;
+        return c2_run_map(h, nhits);
+    }
+    // candidate groups in turn: finalisation, statistics, MAP and the hits
+    // of each group to the host, then one list sorted by log E (then profile)
+    std::vector<c2_hit> all;
+    std::vector<char> aln;
+    for (const auto& g : groups) {
+        release_phase2(h);
+        if ((st = finalize_set(h, g, &n)) != C2_OK) return st;
+        if ((st = c2_run_stats(h, &n)) != C2_OK) return st;
+        int32_t nm = 0;
+        if ((st = c2_run_map(h, &nm)) != C2_OK) return st;
+        size_t bytes = 0;
+        if ((st = hits_direct(h, nullptr, 0, nullptr, &bytes)) != C2_OK) return st;
+        std::vector<c2_hit> hs((size_t)std::max(nm, 1));
+        std::vector<char> as(bytes + 1);
+        if ((st = hits_direct(h, hs.data(), nm, as.data(), &bytes)) != C2_OK) return st;
+        const int64_t base = (int64_t)aln.size();
+        for (int i = 0; i < nm; i++) {
+            hs[i].aln_offset += base;
+            all.push_back(hs[i]);
+        }
+        aln.insert(aln.end(), as.begin(), as.begin() + (long)bytes);
+    }
+    release_phase2(h);
+    std::vector<int> order(all.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        if (all[x].logE != all[y].logE) return all[x].logE < all[y].logE;
+        return all[x].profile < all[y].profile;
+    });
+    h->acc_hits.clear();
+    h->acc_alns.clear();
+    for (int i : order) {
+        c2_hit r = all[i];
+        const size_t len = (size_t)5 * (r.alnlen + 1);
+        r.aln_offset = (int64_t)h->acc_alns.size();
+        h->acc_alns.insert(h->acc_alns.end(), aln.begin() + all[i].aln_offset, aln.begin() + all[i].aln_offset + (long)len);
+        h->acc_hits.push_back(r);
+    }
+    h->acc_valid = true;
+    *nhits = (int32_t)h->acc_hits.size();
+    return C2_OK;
+}
+
+extern "C" c2_status c2_get_search_groups(const c2_handle* h, int32_t* ngroups)
+{
+    if (!h || !ngroups) return C2_ERR_ARG;
+    *ngroups = h->ngroups;
     return C2_OK;
 }
 
@@ -1565,8 +1781,8 @@ extern "C" c2_status c2_logz_fwd(c2_handle* h, const int32_t* profiles, int32_t 
     for (int k = 0; k < 7; k++) h->adj_theta[k] = theta ? theta[k] : 0.f;
     h->adj_wss = wss;
     h->adj_wcv = wcv;
-    if (h->d_adjprof.ensure(npairs) || h->d_adjoff.ensure(npairs) || h->d_adjbuf.ensure((size_t)acc * 15) ||
-        h->d_adjlogz.ensure(npairs) || h->d_adjgrad.ensure((size_t)npairs * 9))
+    if (h->d_adjprof.ensure(npairs, h->budget) || h->d_adjoff.ensure(npairs, h->budget) || h->d_adjbuf.ensure((size_t)acc * 15, h->budget) ||
+        h->d_adjlogz.ensure(npairs, h->budget) || h->d_adjgrad.ensure((size_t)npairs * 9, h->budget))
         return fail(h, C2_ERR_NOMEM, "logz_fwd: scratch for %d pairs (%lld cells) failed", npairs, acc);
     CK(cudaMemcpyAsync(h->d_adjprof.p, profiles, (size_t)npairs * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_adjoff.p, h->adj_off.data(), (size_t)npairs * 8, cudaMemcpyHostToDevice, h->stream));
@@ -1663,6 +1879,7 @@ static c2_status batch_workers(c2_handle* h, int nw)
         c2_handle* w = nullptr;
         c2_status st = c2_create(h->device, &p, &w);
         if (st != C2_OK) return fail(h, st, "batch: creating a worker handle failed");
+        w->budget = h->budget;   // the workers draw on the handle's device memory budget
         if ((st = c2_share_db(w, h)) != C2_OK) {
             std::string e = w->err;
             c2_destroy(w);
@@ -1670,7 +1887,10 @@ static c2_status batch_workers(c2_handle* h, int nw)
         }
         h->workers.push_back(w);
     }
-    for (c2_handle* w : h->workers) w->score_mode = h->score_mode;
+    for (c2_handle* w : h->workers) {
+        w->score_mode = h->score_mode;
+        w->spin = h->spin;
+    }
     return C2_OK;
 }
 

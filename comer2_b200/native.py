@@ -28,7 +28,8 @@ EXPORTS = [
     "c2_launch_count", "c2_run_stats", "c2_run_map", "c2_get_hits", "c2_search", "c2_get_search_space",
     "c2_run_phase1_static", "c2_set_score_mode", "c2_logz_fwd", "c2_logz_bwd", "c2_logz_cells",
     "c2_db2bin_info", "c2_db2bin_read", "c2_share_db", "c2_search_batch", "c2_format_report",
-    "c2_set_wait_limit", "c2_get_pair_scores", "c2_db2bin_descriptions",
+    "c2_set_wait_limit", "c2_get_pair_scores", "c2_db2bin_descriptions", "c2_set_device_memory_limit",
+    "c2_get_device_memory_use", "c2_get_search_groups",
 ]
 
 REPORT_PLAIN = 0
@@ -196,6 +197,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.c2_run_phase1_static.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     lib.c2_set_score_mode.argtypes = [C.c_void_p, C.c_int32]
     lib.c2_set_wait_limit.argtypes = [C.c_void_p, C.c_uint32]
+    lib.c2_set_device_memory_limit.argtypes = [C.c_void_p, C.c_uint64]
+    lib.c2_get_device_memory_use.argtypes = [C.c_void_p, P(C.c_uint64)]
+    lib.c2_get_search_groups.argtypes = [C.c_void_p, P(C.c_int32)]
     lib.c2_get_pair_scores.argtypes = [C.c_void_p, C.c_int32, _fp, _fp]
     lib.c2_db2bin_descriptions.argtypes = [C.c_char_p, C.c_void_p, P(C.c_size_t), _i64p, C.c_char_p, C.c_size_t]
     lib.c2_logz_fwd.argtypes = [C.c_void_p, _i32p, C.c_int32, _fp, C.c_float, C.c_float, _fp]
@@ -369,6 +373,21 @@ class Handle:
     def set_score_mode(self, mode: int):
         """SCORE_FP32 (CUDA cores) or SCORE_BF16_TC (split-BF16 tensor-core contractions)."""
         self._ck(self.lib.c2_set_score_mode(self._h, mode), "c2_set_score_mode")
+
+    def set_memory_limit(self, nbytes: int):
+        """Device memory budget of the handle in bytes, 0 for none (c2_set_device_memory_limit)."""
+        self._ck(self.lib.c2_set_device_memory_limit(self._h, int(nbytes)), "c2_set_device_memory_limit")
+
+    def memory_use(self) -> int:
+        n = C.c_uint64()
+        self._ck(self.lib.c2_get_device_memory_use(self._h, C.byref(n)), "c2_get_device_memory_use")
+        return n.value
+
+    def search_groups(self) -> int:
+        """Candidate groups the last search ran its phase 2 in (c2_get_search_groups)."""
+        n = C.c_int32()
+        self._ck(self.lib.c2_get_search_groups(self._h, C.byref(n)), "c2_get_search_groups")
+        return n.value
 
     def set_wait_limit(self, polls: int):
         """Polls before a phase-2 strip wait gives up (0: the default; c2_set_wait_limit)."""

@@ -274,6 +274,23 @@ c2_status c2_set_stream(c2_handle* h, void* stream);
 /* Synchronize the handle's stream. */
 c2_status c2_sync(c2_handle* h);
 
+/* Device memory budget of the handle, in bytes (0: none): a buffer that
+ * would take the handle's device memory beyond it is refused with
+ * C2_ERR_NOMEM before cudaMalloc; c2_search then processes its candidate
+ * pairs in groups whose phase-2 scratch fits.  Replaces the reference's
+ * --dev-mem limit on its device heap (CuDeviceMemory, src/comer/comer.h
+ * usage: "Maximum amount of GPU memory (MB) that can be used").  Worker
+ * handles of c2_search_batch draw on the same budget. */
+c2_status c2_set_device_memory_limit(c2_handle* h, uint64_t bytes);
+
+/* Device memory the handle's buffers hold now, in bytes. */
+c2_status c2_get_device_memory_use(const c2_handle* h, uint64_t* bytes);
+
+/* Number of candidate groups the last c2_search processed its phase 2 in
+ * (1 unless a device memory budget split it).  After a search of several
+ * groups, c2_get_pair_scores holds only the last group's pairs. */
+c2_status c2_get_search_groups(const c2_handle* h, int32_t* ngroups);
+
 /* Bound of the waits between the strips of one pair in the phase-2 sweeps
  * (traceback DP, MAP forward/backward, MAP DP): a strip polls its
  * predecessor's progress at most `polls` times (0 restores the default,
