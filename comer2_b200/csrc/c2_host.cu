@@ -339,7 +339,9 @@ extern "C" c2_status c2_create(int device, const c2_params* p, c2_handle** out)
         !p->cvs2s_values || p->cvs2s_card <= 1 || p->cvs2s_card > std::min(MAX_CVCARD, P1TC_MAX_CVCARD) ||
         p->cvs2s_shift < 0)
         return C2_ERR_ARG;
-    if (p->ssswgt <= 0.f || p->cvswgt <= 0.f) return C2_ERR_ARG;  // SS and CV terms both in use
+    // SS and CV term weights: 0 leaves a term out, as the reference's score
+    // kernels are then not launched (cusco/CuBatchScoreMatrix.cu:273-352)
+    if (!(p->ssswgt >= 0.f) || !(p->cvswgt >= 0.f)) return C2_ERR_ARG;
     // SSEMODEL 0 (observed statistics), 1 and 2 (SS18 variants) are built;
     // MAPALN 0 (Viterbi alignments drawn by FinalizeDP_ALN instead of MAP,
     // cupro/CuBatchProcessing.cu:477-510) is not, and is refused rather than

@@ -42,8 +42,8 @@ typedef struct {
     float gapped_lambda, gapped_K, gapped_H;             /* [GAPPED_A_1] */
     float gapped_alpha, gapped_beta;
     float eval;            /* EVAL */
-    float ssswgt;          /* SSSWGT */
-    float cvswgt;          /* CVSWGT */
+    float ssswgt;          /* SSSWGT (>= 0; 0 leaves the SS term out) */
+    float cvswgt;          /* CVSWGT (>= 0; 0 leaves the context-vector term out) */
     float minpp;           /* MINPP */
     int32_t mapaln;        /* MAPALN: must be 1 (MAP alignments); 0 is refused */
     int32_t x_uninf;       /* X_UNINF */

@@ -749,6 +749,8 @@ typedef struct {
     real mu, scale;                           /* SS18 EVD parameters */
 } orc_stats_out;
 
+void orc_significance(const orc_stats_in* in, real lambda, real K, orc_stats_out* out);
+
 static void predict_evd(const orc_stats_in* in, real lambda, real* mu, real* scale)
 {
     const float* w = in->nnw;
@@ -885,6 +887,19 @@ void orc_stats(const orc_stats_in* in, const real* S, const unsigned char* qaa, 
         }
     real K = calc_K(&c, minu, maxu, E, lambda, H);
     out->min = minu; out->max = maxu; out->E = E; out->H = H; out->lambda = lambda; out->K = K;
+    orc_significance(in, lambda, K, out);
+}
+
+/*
+ * The significance part of the statistics on given lambda and K (the pair's
+ * computed ungapped parameters; <= 0 for a failed computation): derived
+ * gapped lambda and K, the pair's own log E-value, and the SS18 (or observed
+ * statistics) log E-value (CuBatchSS_dynplm.cu:447-676).  Filling only
+ * lambda_est, K_est, logEpA, mu, scale and logE of out.
+ */
+void orc_significance(const orc_stats_in* in, real lambda, real K, orc_stats_out* out)
+{
+    const int nq = in->nq, nd = in->nd;
     /* SS18 significance (CuBatchSS_dynplm.cu:447-580) */
     out->lambda_est = 0 < lambda ? lambda * ((real)in->expglambda / (real)in->reflambda) : (real)-1.0f;
     out->K_est = 0 < K ? K * ((real)in->expgK / (real)in->refK) : (real)-1.0f;

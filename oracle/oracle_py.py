@@ -98,6 +98,7 @@ class Oracle:
         self.StatsOut = _stats_out(self.crt)
         self.MapOut = _map_out(self.crt)
         L.orc_stats.argtypes = [C.POINTER(orc_stats_in), rp, _u8p, _u8p, C.c_int, C.POINTER(self.StatsOut)]
+        L.orc_significance.argtypes = [C.POINTER(orc_stats_in), self.crt, self.crt, C.POINTER(self.StatsOut)]
         L.orc_map.argtypes = [C.POINTER(orc_profile), C.POINTER(orc_profile), rp, rp, self.crt, self.crt,
                               C.c_int, _u8p, _u8p, rp, C.c_char_p, C.POINTER(self.MapOut)]
         L.orc_set_map_exact.argtypes = [C.c_int]
@@ -224,6 +225,17 @@ class Oracle:
         self.lib.orc_stats(C.byref(si), S.ctypes.data_as(C.POINTER(self.crt)), qa.ctypes.data_as(_u8p),
                            da.ctypes.data_as(_u8p), xuninf, C.byref(o))
         return {k: getattr(o, k) for k, _ in o._fields_}
+
+    def significance(self, nq, nd, score, psts, qeno, deno, searchspace, lambda_, K):
+        """log E-values of one pair from given computed ungapped lambda and K
+        (<= 0: failed): dict with lambda_est, K_est, logEpA, mu, scale, logE."""
+        p = self.params
+        si = orc_stats_in(int(p.ssemodel), int(nq), int(nd), float(qeno), float(deno), float(searchspace),
+                          float(p.ungapped_lambda), float(p.ungapped_K), float(p.gapped_lambda),
+                          float(p.gapped_K), self._f32(p.sse_nn_weights), float(score), float(psts))
+        o = self.StatsOut()
+        self.lib.orc_significance(C.byref(si), lambda_, K, C.byref(o))
+        return {k: getattr(o, k) for k in ("lambda_est", "K_est", "logEpA", "mu", "scale", "logE")}
 
     def map(self, q, d, S, MOD, logepa, qss=None, dss=None, exact=False, with_post=False):
         """MAP alignment of one pair: dict with logZ, coordinates, counts and strings."""

@@ -1,0 +1,79 @@
+"""The comer2 program end to end on the GPU: a query file of two stacked
+text profiles against a database made by the reference's makedb + db2bin,
+result files in both formats.  Its hits equal the C ABI search of the same
+profiles (as the library's readers read them), in the order and with the
+scores, E-values and alignments the JSON file reports."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from comer2_b200 import synth as S
+from comer2_b200 import textfmt
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.path.join(ROOT, "oracle", "_ref")
+needs_ref = pytest.mark.skipif(not os.path.exists(os.path.join(REF, "db2bin")),
+                               reason="reference tools not built (oracle/build_ref.sh)")
+
+
+@needs_ref
+def test_program_matches_the_library(tmp_path, params):
+    from comer2_b200 import build as B
+    from comer2_b200.native import Handle, read_db2bin, read_db2bin_descriptions
+    rng = np.random.default_rng(31)
+    w = S.config(1, seed=6, scale=0.0015)   # 150 profiles, 3 planted homologs of query 0
+    q2 = S.random_profiles(rng, [120])
+    pro = tmp_path / "pro"
+    pro.mkdir()
+    for k in range(w.db.nprofiles):
+        with open(pro / ("p%04d.pro" % k), "w") as fh:
+            textfmt.write_profile(fh, w.db, k, "p%04d" % k, "profile %d of the test database" % k)
+    opts = os.path.join(REF, "var", "options.txt")
+    subprocess.run([os.path.join(REF, "makedb"), "-o", str(tmp_path / "tdb"), "-p", opts, "-d", str(pro)],
+                   check=True, capture_output=True)
+    subprocess.run([os.path.join(REF, "db2bin"), "-d", str(tmp_path / "tdb"), "-p", opts], check=True,
+                   capture_output=True)
+    qf = tmp_path / "two.pro"
+    with open(qf, "w") as fh:
+        textfmt.write_profile(fh, w.queries[0], 0, "q0", "first query")
+        textfmt.write_profile(fh, q2, 0, "q1", "second query")
+    out = tmp_path / "out"
+    for fmt in ("1", "0"):
+        r = subprocess.run([B.PROG, "-i", str(qf), "-d", str(tmp_path / "tdb"), "-o", str(out), "-f", fmt, "-v"],
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+    assert sorted(os.listdir(out)) == ["two__0.json", "two__0.out", "two__1.json", "two__1.out"]
+    # the same search through the library
+    D = read_db2bin(str(tmp_path / "tdb.bin"))
+    desc = read_db2bin_descriptions(str(tmp_path / "tdb.bin"))
+    Q = textfmt.read_profiles(qf.read_text())
+    h = Handle(params, 0)
+    h.upload_db(D)
+    for qn in range(2):
+        hits = h.search(_one(Q, qn))
+        doc = json.loads(open(out / ("two__%d.json" % qn)).read())["comer_search"]
+        assert doc["query"]["description"] == ("first query", "second query")[qn]
+        recs = [x["hit_record"] for x in doc["search_hits"]]
+        assert [x["target_description"] for x in recs] == [desc[x["profile"]] for x in hits]
+        for x, r in zip(hits, recs):
+            a = r["alignment"]
+            assert a["score"] == pytest.approx(x["score"], abs=0.01)
+            assert a["evalue"] == pytest.approx(float(np.exp(np.float64(x["logE"]))), rel=0.06, abs=1e-300)
+        plain = open(out / ("two__%d.out" % qn)).read()
+        for x in hits[:5]:
+            assert desc[x["profile"]] in plain
+    assert len(json.loads(open(out / "two__0.json").read())["comer_search"]["search_hits"]) >= 3
+    h.close()
+
+
+def _one(P, k):
+    L, o = int(P.lengths[k]), int(P.offsets[k])
+    return S.ProfileSet(np.array([L], np.int32), np.zeros(1, np.int64), P.bkg[k:k + 1], P.eno[k:k + 1],
+                        P.trn[o + k:o + k + L + 1], P.trg[o:o + L], P.cv[o:o + L], P.cvprior[o:o + L],
+                        P.cvnorm2[o:o + L], P.ss[o:o + L], P.ssstate[o:o + L], P.aa[o:o + L],
+                        P.trn_int[o + k:o + k + L + 1], P.trg_int[o:o + L])

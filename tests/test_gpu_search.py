@@ -325,3 +325,37 @@ def test_masked_residues_matches_oracle(params, orc32):
     for x in hits:
         _recheck_on_device_scores(h, orc32, params, w, x, ss, logevthld)
     h.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("case", ["c1_s2", "c1_s9", "c0_s4"])
+def test_matches_the_reference_run(params, case, mode):
+    """The CUDA path against the reference's own results on a B200 (the
+    fixtures of tests/test_ref_golden.py; SS and CV weights 0, the only
+    setting in which that build's results are valid): for every hit the
+    reference reported, the DP score within the printed 0.006, and the
+    expected score and score range of the pair's score distribution to the
+    printed digits.  The E-value threshold is raised so that every pair gets
+    its statistics; the E-values and MAP alignments follow the statistics,
+    which are checked against the oracle elsewhere (the reference's own
+    lambda and K are not valid on this build)."""
+    import copy
+    from test_ref_golden import fixture_params, fixture_workload, load_fixture
+    from comer2_b200.native import Handle
+    fx = load_fixture(case)
+    p = fixture_params(params, fx)
+    p = copy.deepcopy(p)
+    p.eval = 1e12
+    w = fixture_workload(fx)
+    h = Handle(p, 0)
+    h.set_score_mode(mode)
+    h.upload_db(w.db)
+    got = {int(x["profile"]): x for x in h.search(w.queries[0])}
+    for r in fx["hits"]:
+        k = r["profile"]
+        assert k in got, k
+        x = got[k]
+        assert abs(x["score"] - r["score"]) <= 0.006, (k, x["score"], r["score"])
+        assert abs(x["E"] - r["expected_score"]) <= 6e-5, (k, x["E"], r["expected_score"])
+        assert (x["smin"], x["smax"]) == (r["min_score"], r["max_score"]), k
+    h.close()
