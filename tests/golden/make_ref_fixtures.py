@@ -266,6 +266,8 @@ def collect_plain(outroot, variant="w00"):
               "format": "plain", "n_hits": len(hits), "hits": hits}
         with open(os.path.join(HERE, "ref_%s_%s_plain.json" % (case, variant)), "w") as fh:
             json.dump(fx, fh, indent=0)
+        # the file itself, for the writers' byte-for-byte comparison
+        shutil.copyfile(files[0], os.path.join(HERE, "ref_%s_%s.out" % (case, variant)))
         summary[case] = len(hits)
     print(json.dumps(summary))
 

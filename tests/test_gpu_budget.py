@@ -13,6 +13,14 @@ from comer2_b200 import synth as S
 pytestmark = pytest.mark.gpu
 
 
+def _pair_scratch_bytes(Lq, L, Lmax):
+    """The library's estimate of one candidate pair's phase-2 device bytes
+    (pair_scratch_bytes in c2_host.cu)."""
+    ns = (Lq + 31) // 32
+    return (9 * Lq * L + 2 * 10 * 4 * L + 2 * 4 * ns + 4 * ns * 2 + 2 * 4 * 32 * ns * (L + 31)
+            + 2 * 5 * (Lq + Lmax + 1) + 512)
+
+
 def _key(rec, buf):
     raw = bytes(buf)
     out = []
@@ -37,9 +45,14 @@ def test_budget_groups_give_the_same_hits(params, mode):
     h.set_score_mode(mode)
     h.upload_db(w.db, total_positions=18_000_000, total_profiles=50_000)
     h.set_query(w.queries[0])
+    h.run_phase1()
+    h.sync()
     base = h.memory_use()
-    # room for about one long candidate's phase-2 scratch at a time
-    limit = base + 64 * 2**20
+    # room for the phase-2 scratch of the longest hit's pair and a little
+    # more, so that the candidates go in several groups
+    Lq = int(w.queries[0].lengths[0])
+    longest = max(int(w.db.lengths[x[0]]) for x in ref)
+    limit = base + (2 << 20) + int(1.3 * _pair_scratch_bytes(Lq, longest, int(w.db.lengths.max())) / 0.9)
     h.set_memory_limit(limit)
     got = _key(*h.search(w.queries[0], arrays=True))
     assert h.search_groups() >= 2

@@ -136,3 +136,118 @@ def test_oracle_statistics_are_valid_where_the_reference_failed(params, case):
         st = orc.stats(x["S"], q.aa, w.db.aa[off:off + nd], x["score"], x["psts"], q.eno[0], w.db.eno[k], float(ss),
                        prm.x_uninf)
         assert 0.9 < st["lambda_"] < 1.1 and 0.3 < st["K"] < 0.6 and 1.5 < st["H"] < 2.1, (k, st)
+
+
+def _sig_interval(x, digits):
+    """[lo, hi) of the values that %.<digits>g prints as the string x (which
+    drops trailing zeros, so x alone does not give the precision)."""
+    ex = int(("%e" % float(x)).split("e")[1])
+    half = 0.5 * 10 ** (ex - (digits - 1))
+    return float(x) - half, float(x) + half
+
+
+def _interval_logE(r, searchspace, summary_e):
+    """A log E-value consistent with every printed value the reference derived
+    from it: the bit score (%.1f), the E-value (%.2g), the P-value (%.2g) and
+    the summary list's E-value (%.1g)."""
+    ln2 = math.log(2.0)
+    lss = math.log(np.float32(searchspace))
+    los = [lss - (r["bit_score"] + 0.05) * ln2]
+    his = [lss - (r["bit_score"] - 0.05) * ln2]
+    for s_, dg in (("%.2g" % r["evalue"], 2), (summary_e, 1)):
+        lo, hi = _sig_interval(s_, dg)
+        los.append(math.log(lo))
+        his.append(math.log(hi))
+    if r["evalue"] >= 0.01:
+        lo, hi = _sig_interval("%.2g" % r["pvalue"], 2)
+        los.append(math.log(-math.log1p(-lo)))
+        if hi < 1.0:
+            his.append(math.log(-math.log1p(-hi)))
+    lo, hi = max(los), min(his)
+    assert lo < hi, (r["profile"], los, his)
+    return 0.5 * (lo + hi)
+
+
+def _summary_evalues(text):
+    """profile -> E-value string of the reference file's summary list."""
+    out = {}
+    for ln in text.splitlines():
+        t = ln.split()
+        if len(t) == 3 and t[0].startswith("p0") and ln.startswith("p0"):
+            out[int(t[0][1:])] = t[2]
+    return out
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_plain_writer_reproduces_the_reference_file(params, case):
+    """c2_format_report against the reference's own Plain result file, byte
+    for byte: the hit records are rebuilt from the oracle (scores, MAP
+    alignments on the reference's lambda and K) and the printed statistics
+    of the reference's run (its lambda, K and entropy values as printed, and
+    a log E-value consistent with its printed E-value and bit score)."""
+    from oracle_py import Oracle
+    from comer2_b200 import native as N
+    fx = load_fixture(case)
+    prm = fixture_params(params, fx)
+    w = fixture_workload(fx)
+    orc = Oracle(prm, 32)
+    q = w.queries[0]
+    qo = orc.profile(q)
+    Lq = int(q.lengths[0])
+    ss, dl = orc.length_adjustment(prm.gapped_lambda, prm.gapped_K, prm.gapped_alpha, prm.gapped_beta, Lq,
+                                   int(w.db.lengths.sum()), int(w.db.nprofiles))
+    with open(os.path.join(HERE, "golden", "ref_%s_w00.out" % case)) as fh:
+        ref = fh.read()
+    summ = _summary_evalues(ref)
+    hits = np.zeros(len(fx["hits"]), N.HIT_DTYPE)
+    alns = []
+    pos = 0
+
+    def printed(v, tiny):
+        # the writer prints K / lambda values > 0 with 4 decimals and "n/a" otherwise
+        return -1.0 if v == "n/a" else (float(v) if float(v) > 0 else tiny)
+
+    for i, r in enumerate(fx["hits"]):
+        k = r["profile"]
+        off, nd = int(w.db.offsets[k]), int(w.db.lengths[k])
+        do = orc.profile(w.db, k)
+        x = orc.pair(qo, do)
+        lam, K = ref_lambda_K(r)
+        sg = orc.significance(Lq, nd, x["score"], x["psts"], q.eno[0], w.db.eno[k], ss, lam, K)
+        m = orc.map(qo, do, x["S"], x["MOD"], sg["logEpA"], qss=q.ssstate, dss=w.db.ssstate[off:off + nd])
+        h = hits[i]
+        h["profile"], h["score"], h["logE"] = k, x["score"], _interval_logE(r, ss, summ[k])
+        h["lambda_"], h["K"] = printed(r["computed_lambda_ungapped"], 1e-6), printed(r["computed_K_ungapped"], 1e-6)
+        h["lambda_est"] = printed(r["estimated_lambda_gapped"], 1e-6)
+        h["K_est"] = printed(r["estimated_K_gapped"], 1e-6)
+        h["E"], h["H"] = r["expected_score"], r["entropy"]
+        h["smin"], h["smax"] = r["min_score"], r["max_score"]
+        h["alnlen"], h["idts"], h["psts"], h["gaps"] = m["alnlen"], m["idts"], m["psts"], m["gaps"]
+        h["beg"] = (m["begx"] << 16) | m["begy"]
+        h["end"] = (m["endx"] << 16) | m["endy"]
+        h["aln_offset"] = pos
+        for sgl in m["strings"]:
+            alns.append(sgl.encode() + b"\0")
+            pos += len(sgl) + 1
+    text = N.format_report(
+        N.REPORT_PLAIN, hits, np.frombuffer(b"".join(alns), np.uint8), query_length=Lq,
+        query_eno=float(q.eno[0]), query_desc="query", query_has_ss=True,
+        db_lengths=w.db.lengths, db_eno=w.db.eno, db_desc=["p%06d" % k for k in range(w.db.nprofiles)],
+        db_names=["db"], db_positions=int(w.db.lengths.sum()), db_profiles=int(w.db.nprofiles),
+        logevthld=math.log(prm.eval), searchspace=float(ss), deltalen=int(dl), ref_lambda=prm.ungapped_lambda,
+        ref_K=prm.ungapped_K, gapped_lambda=prm.gapped_lambda, gapped_K=prm.gapped_K, print_ss=False,
+        dsclen=1024, dscwidth=80, alnwidth=60, show=1, nhits=700, nalns=700, progname="comer",
+        progversion="2.03.03", references=REFERENCES)
+    if text != ref:
+        import difflib
+        diff = "".join(list(difflib.unified_diff(ref.splitlines(True), text.splitlines(True), "reference",
+                                                 "c2_format_report"))[:60])
+        pytest.fail("Plain file differs from the reference's:\n" + diff)
+
+
+REFERENCES = [
+    "Margelevicius, M. (2020). COMER2: GPU-accelerated sensitive and specific homology searches. "
+    "Bioinformatics 36, 3570-3572.",
+    "Margelevicius, M. (2016). Bayesian nonparametrics in protein remote homology search. "
+    "Bioinformatics 32, 2744-2752.",
+]
