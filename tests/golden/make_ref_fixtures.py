@@ -113,7 +113,9 @@ def collect(outroot):
 
 
 # option variants of the reference runs: name -> (SSSWGT, CVSWGT)
-VARIANTS = {"w00": (0.0, 0.0), "w0cv": (0.0, 0.15), "wss0": (0.12, 0.0)}
+VARIANTS = {"w00": (0.0, 0.0), "w0cv": (0.0, 0.15), "wss0": (0.12, 0.0), "w00aln0": (0.0, 0.0)}
+# options besides the weights: MAPALN 0 (Viterbi alignments) for the aln0 runs
+VARIANT_MAPALN = {"w00aln0": 0}
 HIT_FIELDS = ("score", "bit_score", "evalue", "pvalue", "n_identities", "n_positives", "n_gaps", "aln_length",
               "query_from", "query_to", "target_from", "target_to", "query_secstr", "target_secstr", "query_aln",
               "target_aln", "middle", "computed_K_ungapped", "computed_lambda_ungapped", "estimated_K_gapped",
@@ -263,7 +265,7 @@ def collect_plain(outroot, variant="w00"):
         hits = _load_ref_plain(files[0])
         wss, wcv = VARIANTS[variant]
         fx = {"case": case, "config": CASES[case], "variant": variant, "ssswgt": wss, "cvswgt": wcv,
-              "format": "plain", "n_hits": len(hits), "hits": hits}
+              "mapaln": VARIANT_MAPALN.get(variant, 1), "format": "plain", "n_hits": len(hits), "hits": hits}
         with open(os.path.join(HERE, "ref_%s_%s_plain.json" % (case, variant)), "w") as fh:
             json.dump(fx, fh, indent=0)
         # the file itself, for the writers' byte-for-byte comparison
@@ -319,6 +321,6 @@ if __name__ == "__main__":
     elif cmd == "collect_variants":
         collect_variants(sys.argv[2])
     elif cmd == "collect_plain":
-        collect_plain(sys.argv[2])
+        collect_plain(sys.argv[2], sys.argv[3] if len(sys.argv) > 3 else "w00")
     elif cmd == "summarize":
         summarize(sys.argv[2:])

@@ -328,11 +328,13 @@ def test_masked_residues_matches_oracle(params, orc32):
 
 
 @pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("variant", ["w00", "w00aln0"])
 @pytest.mark.parametrize("case", ["c1_s2", "c1_s9", "c0_s4"])
-def test_matches_the_reference_run(params, case, mode):
+def test_matches_the_reference_run(params, case, variant, mode):
     """The CUDA path against the reference's own results on a B200 (the
     fixtures of tests/test_ref_golden.py; SS and CV weights 0, the only
-    setting in which that build's results are valid): for every hit the
+    setting in which that build's results are valid; MAP or, with MAPALN 0,
+    Viterbi alignments and that setting's score shift): for every hit the
     reference reported, the DP score within the printed 0.006, and the
     expected score and score range of the pair's score distribution to the
     printed digits.  The E-value threshold is raised so that every pair gets
@@ -342,7 +344,7 @@ def test_matches_the_reference_run(params, case, mode):
     import copy
     from test_ref_golden import fixture_params, fixture_workload, load_fixture
     from comer2_b200.native import Handle
-    fx = load_fixture(case)
+    fx = load_fixture(case, variant)
     p = fixture_params(params, fx)
     p = copy.deepcopy(p)
     p.eval = 1e12
@@ -361,46 +363,6 @@ def test_matches_the_reference_run(params, case, mode):
     h.close()
 
 
-def viterbi_alignment(bt, S, qaa, daa, qss, dss, x, y):
-    """The Viterbi DP's own alignment (MAPALN 0): the walk from the DP
-    maximum (x, y) through the traceback codes, as FinalizeDP_ALN draws it
-    (src/libmycu/cudp/CuBatchDP_aln_final.cu:240-360): query, middle and
-    target rows and the SS rows, identities, non-identical positives, gaps,
-    0-based first cell and the end cell.  bt, S: [Lq][L]."""
-    STOP, LEFT, UP = 0, 1, 2
-    end = (x, y)
-    q, m, t, sq, st = [], [], [], [], []
-    idts = psts = gaps = 0
-    while x >= 0 and y >= 0:
-        b = int(bt[y, x])
-        if b == STOP:
-            break
-        if b == UP:
-            gaps += 1
-            q.append(chr(qaa[y])); t.append("-"); m.append(" "); sq.append(chr(qss[y])); st.append(" ")
-            y -= 1
-            continue
-        if b == LEFT:
-            gaps += 1
-            q.append("-"); t.append(chr(daa[x])); m.append(" "); sq.append(" "); st.append(chr(dss[x]))
-            x -= 1
-            continue
-        cq, cd = chr(qaa[y]), chr(daa[x])
-        q.append(cq); t.append(cd); sq.append(chr(qss[y])); st.append(chr(dss[x]))
-        if cq == cd:
-            m.append(cq)
-            idts += 1
-        elif S[y, x] > 0:
-            m.append("+")
-            psts += 1
-        else:
-            m.append(" ")
-        x -= 1
-        y -= 1
-    rows = ["".join(reversed(r)) for r in (q, m, t, sq, st)]
-    return rows, len(q), idts, psts, gaps, (x + 1, y + 1), end
-
-
 @pytest.mark.parametrize("mode", [0, 1])
 def test_viterbi_alignments_match_oracle(params, mode):
     """MAPALN 0: the hits carry the Viterbi DP's own alignments (the
@@ -410,6 +372,7 @@ def test_viterbi_alignments_match_oracle(params, mode):
     oracle's (which applies the same MAPALN-0 score terms)."""
     import copy
     from oracle_py import Oracle
+    from test_ref_golden import viterbi_alignment
     p = copy.deepcopy(params)
     p.mapaln = 0
     orc = Oracle(p, 32)

@@ -38,8 +38,11 @@ CASES = ("c1_s2", "c1_s9", "c0_s4")
 LAMBDA_FAIL, K_FAIL = -32.0, -1.0   # a failed computation: -1 in scaled units, times the scale 32; K -1
 
 
-def load_fixture(case):
-    with open(os.path.join(HERE, "golden", "ref_%s_w00_plain.json" % case)) as fh:
+VARIANTS = ("w00", "w00aln0")   # SS and CV weights 0; MAP alignments / MAPALN 0 (Viterbi alignments)
+
+
+def load_fixture(case, variant="w00"):
+    with open(os.path.join(HERE, "golden", "ref_%s_%s_plain.json" % (case, variant))) as fh:
         return json.load(fh)
 
 
@@ -47,6 +50,7 @@ def fixture_params(params, fx):
     p = copy.deepcopy(params)
     p.ssswgt = np.float32(fx["ssswgt"])
     p.cvswgt = np.float32(fx["cvswgt"])
+    p.mapaln = int(fx.get("mapaln", 1))
     return p
 
 
@@ -67,6 +71,46 @@ def search_space(orc, prm, w):
                                  int(q.lengths[0]), int(w.db.lengths.sum()), int(w.db.nprofiles))[0]
 
 
+def viterbi_alignment(bt, S, qaa, daa, qss, dss, x, y):
+    """The Viterbi DP's own alignment (MAPALN 0): the walk from the DP
+    maximum (x, y) through the traceback codes, as FinalizeDP_ALN draws it
+    (src/libmycu/cudp/CuBatchDP_aln_final.cu:240-360): query, middle and
+    target rows and the SS rows, identities, non-identical positives, gaps,
+    0-based first cell and the end cell.  bt, S: [Lq][L]."""
+    STOP, LEFT, UP = 0, 1, 2
+    end = (x, y)
+    q, m, t, sq, st = [], [], [], [], []
+    idts = psts = gaps = 0
+    while x >= 0 and y >= 0:
+        b = int(bt[y, x])
+        if b == STOP:
+            break
+        if b == UP:
+            gaps += 1
+            q.append(chr(qaa[y])); t.append("-"); m.append(" "); sq.append(chr(qss[y])); st.append(" ")
+            y -= 1
+            continue
+        if b == LEFT:
+            gaps += 1
+            q.append("-"); t.append(chr(daa[x])); m.append(" "); sq.append(" "); st.append(chr(dss[x]))
+            x -= 1
+            continue
+        cq, cd = chr(qaa[y]), chr(daa[x])
+        q.append(cq); t.append(cd); sq.append(chr(qss[y])); st.append(chr(dss[x]))
+        if cq == cd:
+            m.append(cq)
+            idts += 1
+        elif S[y, x] > 0:
+            m.append("+")
+            psts += 1
+        else:
+            m.append(" ")
+        x -= 1
+        y -= 1
+    rows = ["".join(reversed(r)) for r in (q, m, t, sq, st)]
+    return rows, len(q), idts, psts, gaps, (x + 1, y + 1), end
+
+
 def check_alignment(r, strings, alnlen, idts, psts, gaps, beg, end):
     """One hit's MAP alignment against the fixture record (beg/end: (x, y)
     of the first and last aligned cells, 0-based; the Plain file prints
@@ -85,10 +129,21 @@ def check_evalue(r, logE, searchspace):
     assert abs(bits - r["bit_score"]) <= 0.051, (k, bits, r["bit_score"])
 
 
+def oracle_alignment(orc, prm, qo, do, x, q, w, off, nd, logepa):
+    """The hit's alignment as the reference's configuration draws it: MAP
+    (MAPALN 1) or the Viterbi DP's own (MAPALN 0)."""
+    if prm.mapaln:
+        m = orc.map(qo, do, x["S"], x["MOD"], logepa, qss=q.ssstate, dss=w.db.ssstate[off:off + nd])
+        return m["strings"], m["alnlen"], m["idts"], m["psts"], m["gaps"], (m["begx"], m["begy"]), (m["endx"], m["endy"])
+    return viterbi_alignment(x["btck"], x["S"], q.aa, w.db.aa[off:off + nd], q.ssstate, w.db.ssstate[off:off + nd],
+                             x["x"], x["y"])
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("case", CASES)
-def test_oracle_matches_the_reference_run(params, case):
+def test_oracle_matches_the_reference_run(params, case, variant):
     from oracle_py import Oracle
-    fx = load_fixture(case)
+    fx = load_fixture(case, variant)
     assert fx["n_hits"] == len(fx["hits"]) > 0
     prm = fixture_params(params, fx)
     w = fixture_workload(fx)
@@ -111,9 +166,7 @@ def test_oracle_matches_the_reference_run(params, case):
         lam, K = ref_lambda_K(r)
         sg = orc.significance(Lq, nd, x["score"], x["psts"], q.eno[0], w.db.eno[k], ss, lam, K)
         check_evalue(r, sg["logE"], ss)
-        m = orc.map(qo, do, x["S"], x["MOD"], sg["logEpA"], qss=q.ssstate, dss=w.db.ssstate[off:off + nd])
-        check_alignment(r, m["strings"], m["alnlen"], m["idts"], m["psts"], m["gaps"], (m["begx"], m["begy"]),
-                        (m["endx"], m["endy"]))
+        check_alignment(r, *oracle_alignment(orc, prm, qo, do, x, q, w, off, nd, sg["logEpA"]))
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -178,8 +231,9 @@ def _summary_evalues(text):
     return out
 
 
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("case", CASES)
-def test_plain_writer_reproduces_the_reference_file(params, case):
+def test_plain_writer_reproduces_the_reference_file(params, case, variant):
     """c2_format_report against the reference's own Plain result file, byte
     for byte: the hit records are rebuilt from the oracle (scores, MAP
     alignments on the reference's lambda and K) and the printed statistics
@@ -187,7 +241,7 @@ def test_plain_writer_reproduces_the_reference_file(params, case):
     a log E-value consistent with its printed E-value and bit score)."""
     from oracle_py import Oracle
     from comer2_b200 import native as N
-    fx = load_fixture(case)
+    fx = load_fixture(case, variant)
     prm = fixture_params(params, fx)
     w = fixture_workload(fx)
     orc = Oracle(prm, 32)
@@ -196,7 +250,7 @@ def test_plain_writer_reproduces_the_reference_file(params, case):
     Lq = int(q.lengths[0])
     ss, dl = orc.length_adjustment(prm.gapped_lambda, prm.gapped_K, prm.gapped_alpha, prm.gapped_beta, Lq,
                                    int(w.db.lengths.sum()), int(w.db.nprofiles))
-    with open(os.path.join(HERE, "golden", "ref_%s_w00.out" % case)) as fh:
+    with open(os.path.join(HERE, "golden", "ref_%s_%s.out" % (case, variant))) as fh:
         ref = fh.read()
     summ = _summary_evalues(ref)
     hits = np.zeros(len(fx["hits"]), N.HIT_DTYPE)
@@ -214,7 +268,8 @@ def test_plain_writer_reproduces_the_reference_file(params, case):
         x = orc.pair(qo, do)
         lam, K = ref_lambda_K(r)
         sg = orc.significance(Lq, nd, x["score"], x["psts"], q.eno[0], w.db.eno[k], ss, lam, K)
-        m = orc.map(qo, do, x["S"], x["MOD"], sg["logEpA"], qss=q.ssstate, dss=w.db.ssstate[off:off + nd])
+        strings, alnlen, idts, psts, gaps, beg, end = oracle_alignment(orc, prm, qo, do, x, q, w, off, nd,
+                                                                         sg["logEpA"])
         h = hits[i]
         h["profile"], h["score"], h["logE"] = k, x["score"], _interval_logE(r, ss, summ[k])
         h["lambda_"], h["K"] = printed(r["computed_lambda_ungapped"], 1e-6), printed(r["computed_K_ungapped"], 1e-6)
@@ -222,11 +277,11 @@ def test_plain_writer_reproduces_the_reference_file(params, case):
         h["K_est"] = printed(r["estimated_K_gapped"], 1e-6)
         h["E"], h["H"] = r["expected_score"], r["entropy"]
         h["smin"], h["smax"] = r["min_score"], r["max_score"]
-        h["alnlen"], h["idts"], h["psts"], h["gaps"] = m["alnlen"], m["idts"], m["psts"], m["gaps"]
-        h["beg"] = (m["begx"] << 16) | m["begy"]
-        h["end"] = (m["endx"] << 16) | m["endy"]
+        h["alnlen"], h["idts"], h["psts"], h["gaps"] = alnlen, idts, psts, gaps
+        h["beg"] = (beg[0] << 16) | beg[1]
+        h["end"] = (end[0] << 16) | end[1]
         h["aln_offset"] = pos
-        for sgl in m["strings"]:
+        for sgl in strings:
             alns.append(sgl.encode() + b"\0")
             pos += len(sgl) + 1
     text = N.format_report(
