@@ -40,6 +40,7 @@ WORKLOADS = {
     0: "1 query L=150 vs 2000 db profiles U[50,500]",
     1: WORKLOAD,
     2: "64 queries LN(250,0.6)[50,1500] vs 20000 db profiles LN(200,0.6)[30,2000], 2% homologs of query 0",
+    3: "differentiable alignment: log-partition forward + adjoint, 256 pairs of 1 query vs 256 profiles U[100,600]",
     4: "1 query L=3000 (6 domains) vs 50000 db profiles LN(300,0.6)[30,2000], 5% planted homologs",
 }
 
@@ -265,6 +266,50 @@ def batch_workload(args):
     h.close()
 
 
+def adjoint_workload(args):
+    """Configuration 3: the log-partition of the MAP forward model and its
+    hand-written adjoint (c2_logz_fwd + c2_logz_bwd: dlogZ/dtheta, dlogZ/dwss,
+    dlogZ/dwcv per pair) for one query of length U[100,600] against 256 db
+    profiles of lengths U[100,600]; cells = forward cells of the 256 pairs,
+    device-timed per forward + backward step (CUDA events)."""
+    import torch
+    from comer2_b200 import params as P, synth as S
+    from comer2_b200.native import Handle
+    prm = P.load_default()
+    w = S.config(3, seed=0, scale=args.scale)
+    q = w.queries[0]
+    cells = float(q.lengths[0]) * float(w.db.lengths.sum())
+    h = Handle(prm, 0)
+    st = torch.cuda.Stream()
+    h.set_stream(st.cuda_stream)
+    h.upload_db(w.db)
+    h.set_query(q)
+    pairs = np.arange(w.db.nprofiles, dtype=np.int32)
+    theta = np.zeros(7, np.float32)
+    for _ in range(max(3, args.warmup)):
+        h.logz_fwd(pairs, theta, 0.12, 0.15)
+        h.logz_bwd()
+    ts = []
+    for _ in range(max(1, args.steps)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        z = h.logz_fwd(pairs, theta, 0.12, 0.15)
+        g = h.logz_bwd()
+        e1.record(st)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    ms = float(np.mean(ts))
+    line = {"metric": "GCUPS (log-partition forward + adjoint)", "value": cells / (ms * 1e-3) / 1e9, "unit": UNIT,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOADS[3], "pairs": int(w.db.nprofiles), "cells": cells,
+                       "timing": "device (CUDA events); logZ and the 9 gradients per pair copied to the host each step"},
+            "finite": bool(np.isfinite(z).all() and np.isfinite(g).all())}
+    print(json.dumps(line))
+    h.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -281,6 +326,8 @@ def main():
     args = ap.parse_args()
     if args.workload == 2:
         return batch_workload(args)
+    if args.workload == 3:
+        return adjoint_workload(args)
     if args.workload != 1:
         global WORKLOAD
         WORKLOAD = WORKLOADS[args.workload]
