@@ -121,9 +121,9 @@ extern "C" c2_status c2_db2bin_info(const char* path, int32_t* nprofiles, int64_
 }
 
 namespace {
-c2_status read_sections(FILE* f, const Header& h, int32_t* lengths, int64_t* offsets, float* bkg, float* eno,
-                        float* trn, float* trg, float* cv, float* cvprior, float* cvnorm2, float* ss,
-                        uint8_t* ssstate, uint8_t* aa, char* err, size_t errlen);
+c2_status read_sections(FILE* f, const Header& h, uint64_t k0, uint64_t k1, int32_t* lengths, int64_t* offsets,
+                        float* bkg, float* eno, float* trn, float* trg, float* cv, float* cvprior, float* cvnorm2,
+                        float* ss, uint8_t* ssstate, uint8_t* aa, char* err, size_t errlen);
 }  // namespace
 
 extern "C" c2_status c2_db2bin_read(const char* path, int32_t* lengths, int64_t* offsets, float* bkg, float* eno,
@@ -143,8 +143,69 @@ extern "C" c2_status c2_db2bin_read(const char* path, int32_t* lengths, int64_t*
     c2_status st = read_header(F.f, h, err, errlen);
     if (st != C2_OK) return st;
     try {
-        return read_sections(F.f, h, lengths, offsets, bkg, eno, trn, trg, cv, cvprior, cvnorm2, ss, ssstate, aa,
-                             err, errlen);
+        return read_sections(F.f, h, 0, h.nprof, lengths, offsets, bkg, eno, trn, trg, cv, cvprior, cvnorm2, ss,
+                             ssstate, aa, err, errlen);
+    } catch (...) {
+        set_err(err, errlen, "out of host memory reading the binary database");
+        return C2_ERR_NOMEM;
+    }
+}
+
+extern "C" c2_status c2_db2bin_lengths(const char* path, int32_t* lengths, char* err, size_t errlen)
+{
+    if (!path || !lengths) return C2_ERR_ARG;
+    File F;
+    F.f = fopen(path, "rb");
+    if (!F.f) {
+        set_err(err, errlen, std::string("cannot open ") + path);
+        return C2_ERR_ARG;
+    }
+    Header h;
+    c2_status st = read_header(F.f, h, err, errlen);
+    if (st != C2_OK) return st;
+    if (!read_at(F.f, h.addr[0], lengths, h.nprof * sizeof(int32_t))) {
+        set_err(err, errlen, "truncated or inconsistent binary database: lengths");
+        return C2_ERR_ARG;
+    }
+    uint64_t acc = 0;
+    for (uint64_t k = 0; k < h.nprof; k++) {
+        if (lengths[k] < 1) {
+            set_err(err, errlen, "truncated or inconsistent binary database: profile length");
+            return C2_ERR_ARG;
+        }
+        acc += (uint64_t)lengths[k];
+    }
+    if (acc != h.npos) {
+        set_err(err, errlen, "truncated or inconsistent binary database: sum of profile lengths");
+        return C2_ERR_ARG;
+    }
+    return C2_OK;
+}
+
+extern "C" c2_status c2_db2bin_read_range(const char* path, int32_t k0, int32_t k1, int32_t* lengths,
+                                          int64_t* offsets, float* bkg, float* eno, float* trn, float* trg, float* cv,
+                                          float* cvprior, float* cvnorm2, float* ss, uint8_t* ssstate, uint8_t* aa,
+                                          char* err, size_t errlen)
+{
+    if (!path || !lengths || !offsets || !bkg || !eno || !trn || !trg || !cv || !cvprior || !cvnorm2 || !ss ||
+        !ssstate || !aa || k0 < 0 || k1 <= k0)
+        return C2_ERR_ARG;
+    File F;
+    F.f = fopen(path, "rb");
+    if (!F.f) {
+        set_err(err, errlen, std::string("cannot open ") + path);
+        return C2_ERR_ARG;
+    }
+    Header h;
+    c2_status st = read_header(F.f, h, err, errlen);
+    if (st != C2_OK) return st;
+    if ((uint64_t)k1 > h.nprof) {
+        set_err(err, errlen, "profile range beyond the end of the database");
+        return C2_ERR_ARG;
+    }
+    try {
+        return read_sections(F.f, h, (uint64_t)k0, (uint64_t)k1, lengths, offsets, bkg, eno, trn, trg, cv, cvprior,
+                             cvnorm2, ss, ssstate, aa, err, errlen);
     } catch (...) {
         set_err(err, errlen, "out of host memory reading the binary database");
         return C2_ERR_NOMEM;
@@ -152,9 +213,9 @@ extern "C" c2_status c2_db2bin_read(const char* path, int32_t* lengths, int64_t*
 }
 
 namespace {
-c2_status read_sections(FILE* f, const Header& h, int32_t* lengths, int64_t* offsets, float* bkg, float* eno,
-                        float* trn, float* trg, float* cv, float* cvprior, float* cvnorm2, float* ss,
-                        uint8_t* ssstate, uint8_t* aa, char* err, size_t errlen)
+c2_status read_sections(FILE* f, const Header& h, uint64_t k0, uint64_t k1, int32_t* lengths, int64_t* offsets,
+                        float* bkg, float* eno, float* trn, float* trg, float* cv, float* cvprior, float* cvnorm2,
+                        float* ss, uint8_t* ssstate, uint8_t* aa, char* err, size_t errlen)
 {
     const uint64_t P = h.nprof, N = h.npos;
     int a = 0;
@@ -162,48 +223,60 @@ c2_status read_sections(FILE* f, const Header& h, int32_t* lengths, int64_t* off
         set_err(err, errlen, std::string("truncated or inconsistent binary database: ") + what);
         return C2_ERR_ARG;
     };
-    // lengths, ENOs, backgrounds
-    if (!read_at(f, h.addr[a++], lengths, P * sizeof(int32_t))) return fail("lengths");
-    uint64_t acc = 0;
+    // every profile's length (the positions before k0 and the total are
+    // needed); profiles [k0, k1) hold Pr profiles and Nr positions from p0 on
+    std::vector<int32_t> all(P);
+    if (!read_at(f, h.addr[a++], all.data(), P * sizeof(int32_t))) return fail("lengths");
+    uint64_t acc = 0, p0 = 0, Nr = 0;
     for (uint64_t k = 0; k < P; k++) {
-        if (lengths[k] < 1) return fail("profile length");
-        offsets[k] = (int64_t)acc;
-        acc += (uint64_t)lengths[k];
+        if (all[k] < 1) return fail("profile length");
+        if (k == k0) p0 = acc;
+        if (k0 <= k && k < k1) {
+            lengths[k - k0] = all[k];
+            offsets[k - k0] = (int64_t)Nr;
+            Nr += (uint64_t)all[k];
+        }
+        acc += (uint64_t)all[k];
     }
     if (acc != N) return fail("sum of profile lengths");
-    if (!read_at(f, h.addr[a++], eno, P * sizeof(float))) return fail("ENOs");
-    std::vector<float> col(std::max<uint64_t>(N + P, P));
+    const uint64_t Pr = k1 - k0;
+    if (!read_at(f, h.addr[a++] + k0 * sizeof(float), eno, Pr * sizeof(float))) return fail("ENOs");
+    std::vector<float> col(Nr + Pr);
     for (int r = 0; r < kNAA; r++) {
-        if (!read_at(f, h.addr[a++], col.data(), P * sizeof(float))) return fail("backgrounds");
-        for (uint64_t k = 0; k < P; k++) bkg[k * kNAA + r] = col[k];
+        if (!read_at(f, h.addr[a++] + k0 * sizeof(float), col.data(), Pr * sizeof(float))) return fail("backgrounds");
+        for (uint64_t k = 0; k < Pr; k++) bkg[k * kNAA + r] = col[k];
     }
+    // transitions: one row per position plus one per profile (its beginning
+    // state), so profile k0's rows start at row p0 + k0
     for (int t = 0; t < kNTRN; t++) {
-        if (!read_at(f, h.addr[a++], col.data(), (N + P) * sizeof(float))) return fail("transitions");
-        for (uint64_t i = 0; i < N + P; i++) trn[i * kNTRN + t] = col[i];
+        if (!read_at(f, h.addr[a++] + (p0 + k0) * sizeof(float), col.data(), (Nr + Pr) * sizeof(float)))
+            return fail("transitions");
+        for (uint64_t i = 0; i < Nr + Pr; i++) trn[i * kNTRN + t] = col[i];
     }
     for (int r = 0; r < kNAA; r++) {
-        if (!read_at(f, h.addr[a++], col.data(), N * sizeof(float))) return fail("target probabilities");
-        for (uint64_t i = 0; i < N; i++) trg[i * kNAA + r] = col[i];
+        if (!read_at(f, h.addr[a++] + p0 * sizeof(float), col.data(), Nr * sizeof(float)))
+            return fail("target probabilities");
+        for (uint64_t i = 0; i < Nr; i++) trg[i * kNAA + r] = col[i];
     }
     for (int r = 0; r < kNCV; r++) {
-        if (!read_at(f, h.addr[a++], col.data(), N * sizeof(float))) return fail("context vectors");
-        for (uint64_t i = 0; i < N; i++) cv[i * kNCV + r] = col[i];
+        if (!read_at(f, h.addr[a++] + p0 * sizeof(float), col.data(), Nr * sizeof(float))) return fail("context vectors");
+        for (uint64_t i = 0; i < Nr; i++) cv[i * kNCV + r] = col[i];
     }
-    if (!read_at(f, h.addr[a++], cvprior, N * sizeof(float))) return fail("context vector priors");
-    if (!read_at(f, h.addr[a++], cvnorm2, N * sizeof(float))) return fail("context vector norms");
+    if (!read_at(f, h.addr[a++] + p0 * sizeof(float), cvprior, Nr * sizeof(float))) return fail("context vector priors");
+    if (!read_at(f, h.addr[a++] + p0 * sizeof(float), cvnorm2, Nr * sizeof(float))) return fail("context vector norms");
     for (int r = 0; r < kNSS; r++) {
-        if (!read_at(f, h.addr[a++], col.data(), N * sizeof(float))) return fail("SS probabilities");
-        for (uint64_t i = 0; i < N; i++) ss[i * kNSS + r] = col[i];
+        if (!read_at(f, h.addr[a++] + p0 * sizeof(float), col.data(), Nr * sizeof(float))) return fail("SS probabilities");
+        for (uint64_t i = 0; i < Nr; i++) ss[i * kNSS + r] = col[i];
     }
     a += 2;   // HDP1 cluster probabilities and indices: not used by this search path
-    if (!read_at(f, h.addr[a++], aa, N)) return fail("residues");
-    if (!read_at(f, h.addr[a++], ssstate, N)) return fail("SS states");
+    if (!read_at(f, h.addr[a++] + p0, aa, Nr)) return fail("residues");
+    if (!read_at(f, h.addr[a++] + p0, ssstate, Nr)) return fail("SS states");
     // the description section ends the file: its last end address must be there
     uint64_t dend = 0;
     if (!read_at(f, h.addr[a] + (P - 1) * sizeof(uint64_t), &dend, sizeof dend) || dend < h.addr[a + 1] ||
         dend > h.fsize)
         return fail("descriptions");
-    for (uint64_t i = 0; i < N; i++) {
+    for (uint64_t i = 0; i < Nr; i++) {
         const uint8_t c = ssstate[i];
         ssstate[i] = (c >= 'a' && c <= 'z') ? (uint8_t)(c - 'a' + 'A') : c;   // ' ': no SS prediction
     }

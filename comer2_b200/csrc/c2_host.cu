@@ -1060,6 +1060,43 @@ extern "C" c2_status c2_get_device_memory_use(const c2_handle* h, uint64_t* byte
     return C2_OK;
 }
 
+extern "C" c2_status c2_get_device_memory_info(const c2_handle* h, uint64_t* free_bytes, uint64_t* total_bytes)
+{
+    if (!h || !free_bytes || !total_bytes) return C2_ERR_ARG;
+    if (cudaSetDevice(h->device) != cudaSuccess) return C2_ERR_CUDA;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return C2_ERR_CUDA;
+    *free_bytes = fr;
+    *total_bytes = tot;
+    return C2_OK;
+}
+
+// Device bytes of a database upload of this size and of the per-profile
+// phase-1 buffers that come with it: the c2_upload_db allocations, and in the
+// tensor-core score mode the operands tc_prepare_db packs (at most
+// ceil(L / 32) * 4 tiles a profile, i.e. npositions / 8 + 4 nprofiles).
+extern "C" c2_status c2_db_device_bytes(const c2_handle* h, int64_t npositions, int32_t nprofiles, int32_t max_length,
+                                        uint64_t* bytes)
+{
+    if (!h || !bytes || npositions < 0 || nprofiles < 0 || max_length < 0) return C2_ERR_ARG;
+    const uint64_t N = (uint64_t)npositions, P = (uint64_t)nprofiles;
+    uint64_t b = N * DR_STRIDE * sizeof(float)                 // d_drec
+                 + P * NAA * sizeof(float)                     // d_pbkg
+                 + P * (sizeof(int) * 2 + sizeof(long long))   // d_plen, d_order, d_poff
+                 + P * (sizeof(float) + sizeof(unsigned))      // d_best, d_coords
+                 + (N + P) * 7 * sizeof(float)                 // d_dtrn
+                 + N * 2                                        // d_daa, d_dss
+                 + P * sizeof(float);                           // d_peno
+    const uint64_t lm = ((uint64_t)max_length + 31) & ~31ull;
+    b += (uint64_t)h->grid * P1_WARPS * 10 * lm * sizeof(float);   // d_bot
+    if (h->score_mode == C2_SCORE_BF16_TC) {
+        const uint64_t ntiles = N / 8 + 4 * P;
+        b += P * sizeof(long long) + ntiles * TC_TILE_WORDS * sizeof(unsigned) + N * P1C_TRS * sizeof(float);
+    }
+    *bytes = b;
+    return C2_OK;
+}
+
 extern "C" c2_status c2_set_wait_limit(c2_handle* h, uint32_t polls)
 {
     if (!h) return C2_ERR_ARG;

@@ -21,12 +21,17 @@
 // by COMER2_PARAMS); the options file (-p, the format of src/env/options.txt)
 // overrides the option values.  --dev-N selects the GPU (the first of a list;
 // the search runs on one GPU), --dev-mem bounds the device memory the search
-// may use (c2_set_device_memory_limit); the reference's other --dev-* and
+// may use (c2_set_device_memory_limit).  A database that does not fit in half
+// of that memory (or of the device's free memory) is searched in chunks of
+// consecutive profiles, each read from file while the previous one is
+// searched, as the reference's reader feeds its device in portions; the
+// results are those of a single search.  The reference's other --dev-* and
 // --io-* options are accepted and have no effect here.
 #include <sys/stat.h>
 #include <sys/types.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <cerrno>
 #include <cmath>
 #include <cstdint>
@@ -34,6 +39,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <functional>
+#include <future>
 #include <map>
 #include <memory>
 #include <sstream>
@@ -555,16 +562,46 @@ void ck_db(c2_status st, const char* err, const std::string& what)
     if (st != C2_OK) die(what + ": " + err);
 }
 
-// A database written by db2bin (<name>.bin), with its descriptions.
-Profiles read_db(const std::string& name)
+// A database written by db2bin (<name>.bin): every profile's length and
+// description, the profiles themselves read by range (read_db_range)
+struct DbFile {
+    std::string name, path;
+    std::vector<int32_t> lengths;
+    std::vector<std::string> desc;
+    int64_t npos = 0;
+    int nprof() const { return (int)lengths.size(); }
+};
+
+DbFile open_db(const std::string& name)
 {
+    DbFile F;
+    F.name = name;
     std::string path = name;
     if (path.size() > 4 && path.compare(path.size() - 4, 4, ".prd") == 0) path = path.substr(0, path.size() - 4);
     if (path.size() < 4 || path.compare(path.size() - 4, 4, ".bin") != 0) path += ".bin";
+    F.path = path;
     char err[512] = {0};
     int32_t P = 0;
+    ck_db(c2_db2bin_info(path.c_str(), &P, &F.npos, err, sizeof err), err, path);
+    F.lengths.resize(P);
+    ck_db(c2_db2bin_lengths(path.c_str(), F.lengths.data(), err, sizeof err), err, path);
+    size_t bytes = 0;
+    ck_db(c2_db2bin_descriptions(path.c_str(), nullptr, &bytes, nullptr, err, sizeof err), err, path);
+    std::vector<char> buf(bytes + 1, 0);
+    std::vector<int64_t> off(P);
+    ck_db(c2_db2bin_descriptions(path.c_str(), buf.data(), &bytes, off.data(), err, sizeof err), err, path);
+    F.desc.resize(P);
+    for (int k = 0; k < P; k++) F.desc[k] = std::string(buf.data() + off[k]);
+    return F;
+}
+
+// Profiles [k0, k1) of a database file
+Profiles read_db_range(const DbFile& F, int32_t k0, int32_t k1)
+{
     int64_t N = 0;
-    ck_db(c2_db2bin_info(path.c_str(), &P, &N, err, sizeof err), err, path);
+    for (int k = k0; k < k1; k++) N += F.lengths[k];
+    const int P = k1 - k0;
+    char err[512] = {0};
     Profiles D;
     D.lengths.resize(P);
     D.offsets.resize(P);
@@ -578,25 +615,80 @@ Profiles read_db(const std::string& name)
     D.ss.resize((size_t)N * 3);
     D.ssstate.resize(N);
     D.aa.resize(N);
-    ck_db(c2_db2bin_read(path.c_str(), D.lengths.data(), D.offsets.data(), D.bkg.data(), D.eno.data(), D.trn.data(),
-                         D.trg.data(), D.cv.data(), D.cvprior.data(), D.cvnorm2.data(), D.ss.data(), D.ssstate.data(),
-                         D.aa.data(), err, sizeof err),
-          err, path);
-    size_t bytes = 0;
-    ck_db(c2_db2bin_descriptions(path.c_str(), nullptr, &bytes, nullptr, err, sizeof err), err, path);
-    std::vector<char> buf(bytes + 1, 0);
-    std::vector<int64_t> off(P);
-    ck_db(c2_db2bin_descriptions(path.c_str(), buf.data(), &bytes, off.data(), err, sizeof err), err, path);
-    D.desc.resize(P);
+    ck_db(c2_db2bin_read_range(F.path.c_str(), k0, k1, D.lengths.data(), D.offsets.data(), D.bkg.data(), D.eno.data(),
+                               D.trn.data(), D.trg.data(), D.cv.data(), D.cvprior.data(), D.cvnorm2.data(),
+                               D.ss.data(), D.ssstate.data(), D.aa.data(), err, sizeof err),
+          err, F.path);
+    D.desc.assign(F.desc.begin() + k0, F.desc.begin() + k1);
     D.name.resize(P);
     D.has_ss.resize(P);
     for (int k = 0; k < P; k++) {
-        D.desc[k] = std::string(buf.data() + off[k]);
         // db2bin writes ' ' as the SS state of profiles without predictions
         bool ss = false;
         for (int64_t j = D.offsets[k]; j < D.offsets[k] + D.lengths[k] && !ss; j++) ss = D.ssstate[j] != ' ';
         D.has_ss[k] = ss ? 1 : 0;
     }
+    return D;
+}
+
+Profiles read_db(const std::string& name)
+{
+    const DbFile F = open_db(name);
+    if (F.nprof() == 0) return Profiles{};
+    return read_db_range(F, 0, F.nprof());
+}
+
+// The databases cut into chunks for the device: runs of consecutive profiles
+// (pieces of one or more files) whose upload fits in `cap` bytes
+// (c2_db_device_bytes); each chunk is uploaded with the totals of all
+// databases and searched in turn.  A profile too large for cap alone makes a
+// chunk of its own (its upload then reports the allocation failure).
+struct Piece {
+    int file;
+    int32_t k0, k1;
+};
+struct Chunk {
+    std::vector<Piece> pieces;
+    int64_t gbase = 0;   // index of the chunk's first profile over all databases
+    int32_t nprof = 0;
+    int64_t npos = 0;
+};
+
+std::vector<Chunk> plan_chunks(c2_handle* h, const std::vector<DbFile>& F, uint64_t cap)
+{
+    std::vector<Chunk> C;
+    Chunk cur;
+    int32_t lmax = 0;
+    int64_t g = 0;
+    auto fits = [&](int64_t n, int32_t p, int32_t l) {
+        uint64_t b = 0;
+        if (c2_db_device_bytes(h, n, p, l, &b) != C2_OK) die("c2_db_device_bytes failed");
+        return cap == 0 || b <= cap;
+    };
+    for (int f = 0; f < (int)F.size(); f++) {
+        for (int32_t k = 0; k < F[f].nprof(); k++, g++) {
+            const int32_t L = F[f].lengths[k];
+            if (cur.nprof > 0 && !fits(cur.npos + L, cur.nprof + 1, std::max(lmax, L))) {
+                C.push_back(cur);
+                cur = Chunk{};
+                lmax = 0;
+            }
+            if (cur.nprof == 0) cur.gbase = g;
+            if (cur.pieces.empty() || cur.pieces.back().file != f) cur.pieces.push_back(Piece{f, k, k});
+            cur.pieces.back().k1 = k + 1;
+            cur.nprof++;
+            cur.npos += L;
+            lmax = std::max(lmax, L);
+        }
+    }
+    if (cur.nprof > 0) C.push_back(cur);
+    return C;
+}
+
+Profiles read_chunk(const std::vector<DbFile>& F, const Chunk& c)
+{
+    Profiles D;
+    for (const Piece& p : c.pieces) D.append(read_db_range(F[p.file], p.k0, p.k1));
     return D;
 }
 
@@ -755,54 +847,126 @@ int run(int argc, char** argv)
     const bool qdb = qi.size() > 4 && (qi.compare(qi.size() - 4, 4, ".prd") == 0 || qi.compare(qi.size() - 4, 4, ".bin") == 0);
     Q = qdb ? read_db(qi) : read_text_profiles(qi);
     // databases, searched as one
-    Profiles D;
-    std::vector<std::string> dbnames;
+    std::vector<DbFile> F;
+    int64_t totN = 0, totP = 0;
     {
         std::stringstream ss(A.dbs);
         for (std::string nm; std::getline(ss, nm, ',');) {
             if (nm.empty()) continue;
-            dbnames.push_back(nm);
-            D.append(read_db(nm));
+            F.push_back(open_db(nm));
+            totN += F.back().npos;
+            totP += F.back().nprof();
         }
     }
-    if (D.nprof() == 0) die("no database profiles");
+    if (totP == 0) die("no database profiles");
     if (A.print_inputs) {
+        Profiles D;
+        for (const DbFile& f : F)
+            if (f.nprof() > 0) D.append(read_db_range(f, 0, f.nprof()));
         print_inputs(P, Q, D);
         return 0;
     }
-    note(1, "queries: " + std::to_string(Q.nprof()) + "; database: " + std::to_string(D.nprof()) + " profiles, " +
-                std::to_string(D.npos()) + " positions");
+    note(1, "queries: " + std::to_string(Q.nprof()) + "; database: " + std::to_string(totP) + " profiles, " +
+                std::to_string(totN) + " positions");
     c2_handle* h = nullptr;
     c2_status st = c2_create(A.device, &P.p, &h);
-    if (st != C2_OK) die("c2_create failed (status " + std::to_string((int)st) + "): check the options (MAPALN 1, SSEMODEL 0..2, SS and CV weights > 0)");
+    if (st != C2_OK) die("c2_create failed (status " + std::to_string((int)st) + "): check the options (MAPALN 0 or 1, SSEMODEL 0..2, SS and CV weights >= 0)");
     std::unique_ptr<c2_handle, c2_status (*)(c2_handle*)> guard(h, c2_destroy);
-    if (A.devmem_mb > 0) ck(h, c2_set_device_memory_limit(h, (uint64_t)A.devmem_mb << 20), "c2_set_device_memory_limit");
-    const c2_profiles dv = D.view();
-    ck(h, c2_upload_db(h, &dv, 0, 0), "c2_upload_db");
+    // device memory: the --dev-mem limit, or what is free on the device; half
+    // of what the handle does not hold yet goes to the database chunk, the
+    // rest to the query and the phase-2 scratch (split into candidate groups
+    // under the limit)
+    uint64_t limit = 0, used0 = 0;
+    if (A.devmem_mb > 0) {
+        limit = (uint64_t)A.devmem_mb << 20;
+        ck(h, c2_set_device_memory_limit(h, limit), "c2_set_device_memory_limit");
+    } else {
+        uint64_t fr = 0, tot = 0;
+        ck(h, c2_get_device_memory_info(h, &fr, &tot), "c2_get_device_memory_info");
+        limit = fr;
+    }
+    ck(h, c2_get_device_memory_use(h, &used0), "c2_get_device_memory_use");
+    if (limit <= used0) die("--dev-mem: the limit is below the memory the search's tables need");
+    const std::vector<Chunk> chunks = plan_chunks(h, F, (limit - used0) / 2);
+    note(1, "database in " + std::to_string(chunks.size()) + " chunk(s)");
     mkdirs(A.outdir);
     std::string qbase = base_name(qi);
     {
         const size_t pos = qbase.rfind('.');
         if (pos != std::string::npos && qbase.size() - pos <= 4) qbase = qbase.substr(0, pos);
     }
-    std::vector<const char*> dbn;
-    for (const auto& s : dbnames) dbn.push_back(s.c_str());
-    std::vector<const char*> ddesc;
-    for (const auto& s : D.desc) ddesc.push_back(s.c_str());
-    for (int qn = 0; qn < Q.nprof(); qn++) {
-        const Profiles q = Q.one(qn);
-        const c2_profiles qv = q.view();
-        int32_t nh = 0;
-        ck(h, c2_search(h, &qv, &nh), "c2_search");
-        size_t abytes = 0;
-        ck(h, c2_get_hits(h, nullptr, 0, nullptr, &abytes), "c2_get_hits");
-        std::vector<c2_hit> hits((size_t)std::max(nh, 1));
-        std::vector<char> alns(abytes + 1);
-        ck(h, c2_get_hits(h, hits.data(), nh, alns.data(), &abytes), "c2_get_hits");
+    // per query: the hits of every chunk (global profile indices), and the
+    // search space and thresholds (the same for every chunk: they depend on
+    // the query and the database totals only)
+    struct QueryHits {
+        std::vector<c2_hit> hits;
+        std::vector<char> alns;
         uint64_t sspace = 0, dlen = 0;
-        ck(h, c2_get_search_space(h, &sspace, &dlen), "c2_get_search_space");
         float thld = 0.f, logevthld = 0.f;
-        ck(h, c2_get_thresholds(h, &thld, &logevthld), "c2_get_thresholds");
+    };
+    std::vector<QueryHits> acc(Q.nprof());
+    std::vector<const char*> dbn;
+    for (const auto& f : F) dbn.push_back(f.name.c_str());
+    std::vector<std::string> desc_all;
+    std::vector<int32_t> len_all;
+    std::vector<float> eno_all((size_t)totP);
+    std::vector<uint8_t> ss_all((size_t)totP);
+    for (const auto& f : F) {
+        desc_all.insert(desc_all.end(), f.desc.begin(), f.desc.end());
+        len_all.insert(len_all.end(), f.lengths.begin(), f.lengths.end());
+    }
+    std::vector<Profiles> queries;
+    for (int qn = 0; qn < Q.nprof(); qn++) queries.push_back(Q.one(qn));
+    // chunk c + 1 is read from file while chunk c is searched
+    std::future<Profiles> next = std::async(std::launch::async, read_chunk, std::cref(F), std::cref(chunks[0]));
+    for (size_t c = 0; c < chunks.size(); c++) {
+        const Profiles D = next.get();
+        if (c + 1 < chunks.size())
+            next = std::async(std::launch::async, read_chunk, std::cref(F), std::cref(chunks[c + 1]));
+        const int64_t gb = chunks[c].gbase;
+        for (int k = 0; k < D.nprof(); k++) {
+            eno_all[(size_t)(gb + k)] = D.eno[k];
+            ss_all[(size_t)(gb + k)] = D.has_ss[k];
+        }
+        const c2_profiles dv = D.view();
+        ck(h, c2_upload_db(h, &dv, (uint64_t)totN, (uint64_t)totP), "c2_upload_db");
+        for (int qn = 0; qn < Q.nprof(); qn++) {
+            const c2_profiles qv = queries[qn].view();
+            int32_t nh = 0;
+            ck(h, c2_search(h, &qv, &nh), "c2_search");
+            size_t abytes = 0;
+            ck(h, c2_get_hits(h, nullptr, 0, nullptr, &abytes), "c2_get_hits");
+            std::vector<c2_hit> hits((size_t)std::max(nh, 1));
+            std::vector<char> alns(abytes + 1);
+            ck(h, c2_get_hits(h, hits.data(), nh, alns.data(), &abytes), "c2_get_hits");
+            QueryHits& a = acc[qn];
+            ck(h, c2_get_search_space(h, &a.sspace, &a.dlen), "c2_get_search_space");
+            ck(h, c2_get_thresholds(h, &a.thld, &a.logevthld), "c2_get_thresholds");
+            const int64_t base = (int64_t)a.alns.size();
+            for (int i = 0; i < nh; i++) {
+                hits[i].profile += (int32_t)gb;
+                hits[i].aln_offset += base;
+                a.hits.push_back(hits[i]);
+            }
+            a.alns.insert(a.alns.end(), alns.begin(), alns.begin() + (long)abytes);
+        }
+        if (chunks.size() > 1)
+            note(2, "chunk " + std::to_string(c + 1) + "/" + std::to_string(chunks.size()) + ": " +
+                        std::to_string(D.nprof()) + " profiles searched");
+    }
+    std::vector<const char*> ddesc;
+    for (const auto& s : desc_all) ddesc.push_back(s.c_str());
+    for (int qn = 0; qn < Q.nprof(); qn++) {
+        const Profiles& q = queries[qn];
+        QueryHits& a = acc[qn];
+        // one list over the chunks in the order of a single search: by log
+        // E-value, then profile index
+        std::stable_sort(a.hits.begin(), a.hits.end(), [](const c2_hit& x, const c2_hit& y) {
+            if (x.logE != y.logE) return x.logE < y.logE;
+            return x.profile < y.profile;
+        });
+        const int32_t nh = (int32_t)a.hits.size();
+        a.alns.push_back(0);
         c2_report_info r{};
         r.progname = "comer";
         r.progversion = kVersion;
@@ -813,11 +977,11 @@ int run(int argc, char** argv)
         r.query_has_ss = q.has_ss[0];
         r.db_names = dbn.data();
         r.n_db_names = (int32_t)dbn.size();
-        r.db_positions = (uint64_t)D.npos();
-        r.db_profiles = (uint64_t)D.nprof();
-        r.logevthld = logevthld;
-        r.searchspace = (double)sspace;
-        r.deltalen = (int32_t)dlen;
+        r.db_positions = (uint64_t)totN;
+        r.db_profiles = (uint64_t)totP;
+        r.logevthld = a.logevthld;
+        r.searchspace = (double)a.sspace;
+        r.deltalen = (int32_t)a.dlen;
         r.ref_lambda = P.p.ungapped_lambda;
         r.ref_K = P.p.ungapped_K;
         r.gapped_lambda = P.p.gapped_lambda;
@@ -830,13 +994,15 @@ int run(int argc, char** argv)
         r.nhits = P.opt_int("NOHITS", 700);
         r.nalns = P.opt_int("NOALNS", 700);
         r.db_desc = ddesc.data();
-        r.db_lengths = D.lengths.data();
-        r.db_eno = D.eno.data();
-        r.db_has_ss = D.has_ss.data();
+        r.db_lengths = len_all.data();
+        r.db_eno = eno_all.data();
+        r.db_has_ss = ss_all.data();
+        if (a.hits.empty()) a.hits.resize(1);   // nh = 0: a valid pointer, nothing read
+        const c2_hit* hp = a.hits.data();
         size_t obytes = 0;
-        ck(h, c2_format_report(A.format, &r, hits.data(), nh, alns.data(), nullptr, &obytes), "c2_format_report");
+        ck(h, c2_format_report(A.format, &r, hp, nh, a.alns.data(), nullptr, &obytes), "c2_format_report");
         std::vector<char> out(obytes + 1, 0);
-        ck(h, c2_format_report(A.format, &r, hits.data(), nh, alns.data(), out.data(), &obytes), "c2_format_report");
+        ck(h, c2_format_report(A.format, &r, hp, nh, a.alns.data(), out.data(), &obytes), "c2_format_report");
         const std::string fn = A.outdir + (A.outdir.empty() || A.outdir.back() == '/' ? "" : "/") + qbase + "__" +
                                std::to_string(qn) + (A.format == C2_REPORT_JSON ? ".json" : ".out");
         FILE* f = fopen(fn.c_str(), "wb");

@@ -29,6 +29,7 @@ EXPORTS = [
     "c2_run_phase1_static", "c2_set_score_mode", "c2_logz_fwd", "c2_logz_bwd", "c2_logz_cells",
     "c2_db2bin_info", "c2_db2bin_read", "c2_share_db", "c2_search_batch", "c2_format_report",
     "c2_set_wait_limit", "c2_get_pair_scores", "c2_db2bin_descriptions", "c2_set_device_memory_limit",
+    "c2_db2bin_lengths", "c2_db2bin_read_range", "c2_get_device_memory_info", "c2_db_device_bytes",
     "c2_get_device_memory_use", "c2_get_search_groups",
 ]
 
@@ -208,6 +209,11 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.c2_db2bin_info.argtypes = [C.c_char_p, _i32p, _i64p, C.c_char_p, C.c_size_t]
     lib.c2_db2bin_read.argtypes = [C.c_char_p, _i32p, _i64p, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _u8p, _u8p,
                                    C.c_char_p, C.c_size_t]
+    lib.c2_get_device_memory_info.argtypes = [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]
+    lib.c2_db_device_bytes.argtypes = [C.c_void_p, C.c_int64, C.c_int32, C.c_int32, P(C.c_uint64)]
+    lib.c2_db2bin_lengths.argtypes = [C.c_char_p, _i32p, C.c_char_p, C.c_size_t]
+    lib.c2_db2bin_read_range.argtypes = [C.c_char_p, C.c_int32, C.c_int32, _i32p, _i64p, _fp, _fp, _fp, _fp, _fp,
+                                         _fp, _fp, _fp, _u8p, _u8p, C.c_char_p, C.c_size_t]
     lib.c2_format_report.argtypes = [C.c_int32, P(c2_report_info), C.c_void_p, C.c_int32, C.c_void_p, C.c_char_p,
                                      P(C.c_size_t)]
     lib.c2_share_db.argtypes = [C.c_void_p, C.c_void_p]
@@ -383,6 +389,19 @@ class Handle:
         self._ck(self.lib.c2_get_device_memory_use(self._h, C.byref(n)), "c2_get_device_memory_use")
         return n.value
 
+    def memory_info(self):
+        """(free, total) bytes of the handle's device (c2_get_device_memory_info)."""
+        f, t = C.c_uint64(), C.c_uint64()
+        self._ck(self.lib.c2_get_device_memory_info(self._h, C.byref(f), C.byref(t)), "c2_get_device_memory_info")
+        return f.value, t.value
+
+    def db_device_bytes(self, npositions: int, nprofiles: int, max_length: int) -> int:
+        """Device bytes an upload of a database of these sizes holds (c2_db_device_bytes)."""
+        n = C.c_uint64()
+        self._ck(self.lib.c2_db_device_bytes(self._h, npositions, nprofiles, max_length, C.byref(n)),
+                 "c2_db_device_bytes")
+        return n.value
+
     def search_groups(self) -> int:
         """Candidate groups the last search ran its phase 2 in (c2_get_search_groups)."""
         n = C.c_int32()
@@ -513,9 +532,10 @@ class Handle:
         return n.value
 
 
-def read_db2bin(path: str):
-    """Read a database written by the reference's db2bin (format v2.2) into a
-    synth.ProfileSet (c2_db2bin_info / c2_db2bin_read; no GPU needed)."""
+def read_db2bin(path: str, k0: int = 0, k1: int = None):
+    """Read a database written by the reference's db2bin (format v2.2), or its
+    profiles [k0, k1) only, into a synth.ProfileSet (c2_db2bin_info /
+    c2_db2bin_read / c2_db2bin_read_range; no GPU needed)."""
     from .synth import ProfileSet
     lib = load()
     P, N = C.c_int32(), C.c_int64()
@@ -524,6 +544,16 @@ def read_db2bin(path: str):
     if st != C2_OK:
         raise C2Error("c2_db2bin_info: %s" % err.value.decode())
     P, N = P.value, N.value
+    whole = k0 == 0 and (k1 is None or k1 == P)
+    if not whole:
+        k1 = P if k1 is None else k1
+        if not 0 <= k0 < k1 <= P:
+            raise C2Error("profile range [%d, %d) outside the database's %d profiles" % (k0, k1, P))
+        every = np.zeros(P, np.int32)
+        st = lib.c2_db2bin_lengths(path.encode(), _ptr(every, _i32p), err, 512)
+        if st != C2_OK:
+            raise C2Error("c2_db2bin_lengths: %s" % err.value.decode())
+        P, N = k1 - k0, int(every[k0:k1].astype(np.int64).sum())
     lengths = np.zeros(P, np.int32)
     offsets = np.zeros(P, np.int64)
     bkg = np.zeros((P, 20), np.float32)
@@ -536,9 +566,13 @@ def read_db2bin(path: str):
     ss = np.zeros((N, 3), np.float32)
     sss = np.zeros(N, np.uint8)
     aa = np.zeros(N, np.uint8)
-    st = lib.c2_db2bin_read(path.encode(), _ptr(lengths, _i32p), _ptr(offsets, _i64p), _ptr(bkg, _fp), _ptr(eno, _fp),
-                            _ptr(trn, _fp), _ptr(trg, _fp), _ptr(cv, _fp), _ptr(cvp, _fp), _ptr(cvn, _fp),
-                            _ptr(ss, _fp), _ptr(sss, _u8p), _ptr(aa, _u8p), err, 512)
+    arrays = (_ptr(lengths, _i32p), _ptr(offsets, _i64p), _ptr(bkg, _fp), _ptr(eno, _fp), _ptr(trn, _fp),
+              _ptr(trg, _fp), _ptr(cv, _fp), _ptr(cvp, _fp), _ptr(cvn, _fp), _ptr(ss, _fp), _ptr(sss, _u8p),
+              _ptr(aa, _u8p), err, 512)
+    if whole:
+        st = lib.c2_db2bin_read(path.encode(), *arrays)
+    else:
+        st = lib.c2_db2bin_read_range(path.encode(), k0, k1, *arrays)
     if st != C2_OK:
         raise C2Error("c2_db2bin_read: %s" % err.value.decode())
     return ProfileSet(lengths, offsets, bkg, eno, trn, trg, cv, cvp, cvn, ss, sss, aa,

@@ -286,6 +286,19 @@ c2_status c2_set_device_memory_limit(c2_handle* h, uint64_t bytes);
 /* Device memory the handle's buffers hold now, in bytes. */
 c2_status c2_get_device_memory_use(const c2_handle* h, uint64_t* bytes);
 
+/* Free and total memory of the handle's device (cudaMemGetInfo). */
+c2_status c2_get_device_memory_info(const c2_handle* h, uint64_t* free_bytes, uint64_t* total_bytes);
+
+/* Device bytes that c2_upload_db of a database with these sizes (its longest
+ * profile max_length positions) holds, with the per-profile phase-1 buffers
+ * and, in the tensor-core score mode, the packed score operands: what a
+ * caller needs to cut a database too large for the budget into chunks, each
+ * uploaded with the whole database's totals and searched in turn (the
+ * reference's reader feeds the device in portions sized from --dev-mem:
+ * TdDataReader::GetNextData, src/libmycu/cupro/TdDataReader.cpp:543-570). */
+c2_status c2_db_device_bytes(const c2_handle* h, int64_t npositions, int32_t nprofiles, int32_t max_length,
+                             uint64_t* bytes);
+
 /* Number of candidate groups the last c2_search processed its phase 2 in
  * (1 unless a device memory budget split it).  After a search of several
  * groups, c2_get_pair_scores holds only the last group's pairs. */
@@ -328,6 +341,17 @@ c2_status c2_db2bin_info(const char* path, int32_t* nprofiles, int64_t* npositio
 c2_status c2_db2bin_read(const char* path, int32_t* lengths, int64_t* offsets, float* bkg, float* eno, float* trn,
                          float* trg, float* cv, float* cvprior, float* cvnorm2, float* ss, uint8_t* ssstate,
                          uint8_t* aa, char* err, size_t errlen);
+/* The same for profiles [k0, k1) only, so that a database larger than host
+ * or device memory streams through in chunks, as the reference's reader
+ * threads feed it to the device in portions (TdDataReader::GetNextData and
+ * ReadDataChunk, src/libmycu/cupro/TdDataReader.cpp:543-686).  The arrays are sized for the range (k1 - k0
+ * profiles, their positions, and their positions + profiles transition rows);
+ * offsets[] start at 0 for profile k0.  c2_db2bin_lengths gives every
+ * profile's length (nprofiles entries) to plan the ranges. */
+c2_status c2_db2bin_lengths(const char* path, int32_t* lengths, char* err, size_t errlen);
+c2_status c2_db2bin_read_range(const char* path, int32_t k0, int32_t k1, int32_t* lengths, int64_t* offsets,
+                               float* bkg, float* eno, float* trn, float* trg, float* cv, float* cvprior,
+                               float* cvnorm2, float* ss, uint8_t* ssstate, uint8_t* aa, char* err, size_t errlen);
 /* Profile descriptions of the same database (the section after the
  * description end addresses, PMProfileModel.cpp:1529-1533): buf == NULL gives
  * the bytes needed in *bytes; otherwise buf receives the NUL-terminated

@@ -123,3 +123,27 @@ def test_db2bin_truncated_and_corrupt_files(tmp_path):
     from comer2_b200.native import read_db2bin_descriptions
     assert read_db2bin(path).nprofiles == 4
     assert sorted(read_db2bin_descriptions(path)) == ["p%04d" % k for k in range(4)]
+
+
+@needs_ref
+def test_db2bin_range_reads_concatenate_to_the_whole(tmp_path):
+    """Profile ranges read with c2_db2bin_read_range, concatenated, give the
+    whole database field by field, transitions (one extra row per profile)
+    included; ranges outside the database are refused."""
+    from comer2_b200.native import C2Error, read_db2bin
+    rng = np.random.default_rng(7)
+    ps = S.random_profiles(rng, [31, 1, 140, 64, 7, 200, 2, 55])
+    path, _ = _make_db(tmp_path, ps)
+    W = read_db2bin(path)
+    for cuts in ([0, 3, 8], [0, 1, 2, 5, 8], [0, 7, 8]):
+        parts = [read_db2bin(path, a, b) for a, b in zip(cuts[:-1], cuts[1:])]
+        for a, b, R in zip(cuts[:-1], cuts[1:], parts):
+            assert np.array_equal(R.lengths, W.lengths[a:b])
+            assert np.array_equal(R.offsets, W.offsets[a:b] - W.offsets[a])
+        cat = S.concat(parts)
+        for f in ("lengths", "offsets", "bkg", "eno", "trn", "trg", "cv", "cvprior", "cvnorm2", "ss", "ssstate",
+                  "aa"):
+            assert np.array_equal(getattr(cat, f), getattr(W, f)), f
+    for a, b in ((-1, 2), (3, 3), (5, 2), (0, 9)):
+        with pytest.raises(C2Error):
+            read_db2bin(path, a, b)

@@ -77,3 +77,63 @@ def _one(P, k):
                         P.trn[o + k:o + k + L + 1], P.trg[o:o + L], P.cv[o:o + L], P.cvprior[o:o + L],
                         P.cvnorm2[o:o + L], P.ss[o:o + L], P.ssstate[o:o + L], P.aa[o:o + L],
                         P.trn_int[o + k:o + k + L + 1], P.trg_int[o:o + L])
+
+
+def _makedb(tmp, name, ps, ks):
+    pro = tmp / (name + "_pro")
+    pro.mkdir()
+    for k in ks:
+        with open(pro / ("p%04d.pro" % k), "w") as fh:
+            textfmt.write_profile(fh, ps, k, "p%04d" % k, "profile %d of the test database" % k)
+    opts = os.path.join(REF, "var", "options.txt")
+    subprocess.run([os.path.join(REF, "makedb"), "-o", str(tmp / name), "-p", opts, "-d", str(pro)],
+                   check=True, capture_output=True)
+    subprocess.run([os.path.join(REF, "db2bin"), "-d", str(tmp / name), "-p", opts], check=True,
+                   capture_output=True)
+    return str(tmp / name)
+
+
+@needs_ref
+def test_program_in_database_chunks_writes_the_same_files(tmp_path, params):
+    """A --dev-mem limit that holds about a third of the two databases at a
+    time: the program searches them in chunks (pieces of both files), each
+    uploaded with the totals of both, and writes the same result files, byte
+    for byte, as the search of the whole."""
+    from comer2_b200 import build as B
+    from comer2_b200.native import Handle, read_db2bin
+    rng = np.random.default_rng(32)
+    w = S.config(1, seed=7, scale=0.0015)
+    q2 = S.random_profiles(rng, [150])
+    n = w.db.nprofiles
+    dbs = [_makedb(tmp_path, "da", w.db, range(0, n // 2)), _makedb(tmp_path, "db", w.db, range(n // 2, n))]
+    qf = tmp_path / "two.pro"
+    with open(qf, "w") as fh:
+        textfmt.write_profile(fh, w.queries[0], 0, "q0", "first query")
+        textfmt.write_profile(fh, q2, 0, "q1", "second query")
+    # the limit: the handle's own tables, plus twice a chunk of a third of
+    # the positions (half of what remains goes to the chunk)
+    D = [read_db2bin(d + ".bin") for d in dbs]
+    N = sum(int(x.lengths.sum()) for x in D)
+    P = sum(x.nprofiles for x in D)
+    lmax = max(int(x.lengths.max()) for x in D)
+    h = Handle(params, 0)
+    used0 = h.memory_use()
+    fixed = h.db_device_bytes(0, 0, lmax)
+    whole = h.db_device_bytes(N, P, lmax)
+    h.close()
+    cap = fixed + (whole - fixed) // 3
+    mb = -(-(used0 + 2 * cap) // 2**20)
+    outs = {}
+    for tag, extra in (("whole", []), ("chunks", ["--dev-mem=%d" % mb])):
+        out = tmp_path / tag
+        for fmt in ("1", "0"):
+            r = subprocess.run([B.PROG, "-i", str(qf), "-d", ",".join(dbs), "-o", str(out), "-f", fmt, "-v"] + extra,
+                               capture_output=True, text=True, timeout=300)
+            assert r.returncode == 0, r.stderr
+            nchunks = int(r.stderr.split("database in ")[1].split(" chunk")[0])
+            assert (nchunks == 1) if tag == "whole" else (3 <= nchunks <= 5), r.stderr
+        outs[tag] = {f: open(out / f, "rb").read() for f in sorted(os.listdir(out))}
+    assert list(outs["whole"]) == ["two__0.json", "two__0.out", "two__1.json", "two__1.out"]
+    assert outs["whole"] == outs["chunks"]
+    doc = json.loads(outs["whole"]["two__0.json"])["comer_search"]
+    assert len(doc["search_hits"]) >= 3
