@@ -146,14 +146,15 @@ struct c2_handle {
     DevBuf<float> d_qrec, d_qbkg, d_qtrn, d_qcf, d_qcfx, d_qU;
     // differentiable alignment (c2_logz_fwd / c2_logz_bwd)
     std::vector<int> adj_prof;
-    std::vector<long long> adj_off;
-    long long adj_cells = 0;
+    std::vector<long long> adj_off, adj_roff;   // per pair: first cell (wavefront order), first row-buffer float
+    long long adj_cells = 0, adj_rows = 0;
+    int adj_Lmax = 0, adj_bgrid = 0;              // longest profile of the pairs; backward sweep CTAs
     bool adj_fwd_done = false;
     float adj_theta[7] = {0, 0, 0, 0, 0, 0, 0};
     float adj_wss = 0.f, adj_wcv = 0.f;
-    DevBuf<int> d_adjprof;
-    DevBuf<long long> d_adjoff;
-    DevBuf<float> d_adjbuf, d_adjlogz, d_adjgrad;
+    DevBuf<int> d_adjprof, d_adjprog, d_adjctr;
+    DevBuf<long long> d_adjoff, d_adjroff;
+    DevBuf<float> d_adjbuf, d_adjlogz, d_adjgrad, d_adjpart, d_adjscr;
     DevBuf<unsigned char> d_qaa, d_qss;
     float scorethld = 0.f, logevthld = 0.f;
     unsigned long long searchspace = 0, deltalen = 0;
@@ -1825,11 +1826,13 @@ extern "C" c2_status c2_run_phase1_static(c2_handle* h, float* d_best, uint32_t*
 static void fill_adj(c2_handle* h, AdjArgs& a)
 {
     memset(&a, 0, sizeof a);
-    const long long NC = h->adj_cells;
+    const long long NC = h->adj_cells, NR = h->adj_rows;
     a.Lq = h->Lq;
     a.npairs = (int)h->adj_prof.size();
+    a.nstrips = (h->Lq + 31) / 32;
     a.prof = h->d_adjprof.p;
     a.off = h->d_adjoff.p;
+    a.roff = h->d_adjroff.p;
     a.plen = h->db->d_plen.p;
     a.poff = h->db->d_poff.p;
     a.qrec = h->d_qrec.p;
@@ -1845,17 +1848,35 @@ static void fill_adj(c2_handle* h, AdjArgs& a)
     for (int k = 0; k < 7; k++) a.theta[k] = h->adj_theta[k];
     a.wss = h->adj_wss;
     a.wcv = h->adj_wcv;
-    a.ncells = NC;
     float* b = h->d_adjbuf.p;
-    a.p0 = b;
+    a.S = b;
     a.pss = b + NC;
     a.pcv = b + 2 * NC;
-    a.F = b + 3 * NC;
-    a.B = b + 8 * NC;
-    a.gS = b + 13 * NC;
-    a.post = b + 14 * NC;
+    a.gS = b + 3 * NC;
+    a.post = b + 4 * NC;
+    a.frow = b + 5 * NC;
+    a.brow = b + 5 * NC + NR;
+    const long long items = (long long)a.npairs * a.nstrips;
+    a.prog = h->d_adjprog.p;
+    a.zpart = h->d_adjpart.p;
+    a.gpart = h->d_adjpart.p + 2 * items;
+    a.scratch = h->d_adjscr.p;
+    a.scratch_stride = (long long)(h->adj_Lmax + 31) * 160;
+    a.counter = h->d_adjctr.p;
+    a.status = h->d_status.p;
+    a.spin = h->spin;
     a.logz = h->d_adjlogz.p;
     a.grad = h->d_adjgrad.p;
+}
+
+// device status after a sweep (a strip wait that timed out)
+static c2_status adj_status(c2_handle* h)
+{
+    int stw = 0;
+    CK(cudaMemcpyAsync(&stw, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (stw != 0) return fail(h, C2_ERR_DEVICE, "device status %d: %s", stw, status_text(stw));
+    return C2_OK;
 }
 
 extern "C" c2_status c2_logz_fwd(c2_handle* h, const int32_t* profiles, int32_t npairs, const float* theta, float wss,
@@ -1864,28 +1885,62 @@ extern "C" c2_status c2_logz_fwd(c2_handle* h, const int32_t* profiles, int32_t 
     if (!h || !profiles || npairs <= 0 || !logz) return C2_ERR_ARG;
     if (h->nprof <= 0 || h->Lq <= 0) return fail(h, C2_ERR_STATE, "logz_fwd needs a database and a query");
     CK(cudaSetDevice(h->device));
+    h->adj_fwd_done = false;
+    const int ns = (h->Lq + 31) / 32;
     h->adj_prof.assign(profiles, profiles + npairs);
     h->adj_off.resize(npairs);
-    long long acc = 0;
+    h->adj_roff.resize(npairs);
+    long long acc = 0, racc = 0;
+    int lmax = 0;
     for (int k = 0; k < npairs; k++) {
         if (profiles[k] < 0 || profiles[k] >= h->nprof)
             return fail(h, C2_ERR_ARG, "logz_fwd: profile %d out of range", profiles[k]);
+        const int L = h->h_plen[profiles[k]];
         h->adj_off[k] = acc;
-        acc += (long long)h->Lq * h->h_plen[profiles[k]];
+        h->adj_roff[k] = racc;
+        acc += (long long)ns * (L + 31) * 32;
+        racc += (long long)ns * 5 * L;
+        lmax = std::max(lmax, L);
     }
     h->adj_cells = acc;
+    h->adj_rows = racc;
+    h->adj_Lmax = lmax;
     for (int k = 0; k < 7; k++) h->adj_theta[k] = theta ? theta[k] : 0.f;
     h->adj_wss = wss;
     h->adj_wcv = wcv;
-    if (h->d_adjprof.ensure(npairs, h->budget) || h->d_adjoff.ensure(npairs, h->budget) || h->d_adjbuf.ensure((size_t)acc * 15, h->budget) ||
-        h->d_adjlogz.ensure(npairs, h->budget) || h->d_adjgrad.ensure((size_t)npairs * 9, h->budget))
+    const long long items = (long long)npairs * ns;
+    if (h->d_adjprof.ensure(npairs, h->budget) || h->d_adjoff.ensure(npairs, h->budget) ||
+        h->d_adjroff.ensure(npairs, h->budget) || h->d_adjbuf.ensure((size_t)(5 * acc + 2 * racc), h->budget) ||
+        h->d_adjlogz.ensure(npairs, h->budget) || h->d_adjgrad.ensure((size_t)npairs * 9, h->budget) ||
+        h->d_adjprog.ensure((size_t)(2 * items), h->budget) || h->d_adjpart.ensure((size_t)(11 * items), h->budget) ||
+        h->d_adjctr.ensure(2, h->budget))
         return fail(h, C2_ERR_NOMEM, "logz_fwd: scratch for %d pairs (%lld cells) failed", npairs, acc);
+    // persistent grids of the sweeps: as many CTAs as are resident (or as
+    // there are strips); backward sweep warps each hold a strip's forward
+    // states (32 rows x (Lmax + 31) columns x 5 floats), its grid halved while
+    // that scratch does not fit (the memory budget or the device)
+    int fwd_occ = 4, bwd_occ = 4;
+    CK(adj_occupancy(&fwd_occ, &bwd_occ));
+    const size_t per_cta = (size_t)ADJ_WARPS * (lmax + 31) * 160 * sizeof(float);
+    const long long want = std::min<long long>((long long)h->nsm * std::max(bwd_occ, 1), (items + ADJ_WARPS - 1) / ADJ_WARPS);
+    h->adj_bgrid = 0;
+    for (long long g = want; g >= 1 && h->adj_bgrid == 0; g /= 2)
+        if (h->d_adjscr.ensure((size_t)g * per_cta / sizeof(float), h->budget) == cudaSuccess) h->adj_bgrid = (int)g;
+    (void)cudaGetLastError();   // a refused allocation above is not an error of what follows
+    if (h->adj_bgrid == 0) return fail(h, C2_ERR_NOMEM, "logz_fwd: backward sweep scratch (%zu bytes per CTA) failed", per_cta);
     CK(cudaMemcpyAsync(h->d_adjprof.p, profiles, (size_t)npairs * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_adjoff.p, h->adj_off.data(), (size_t)npairs * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_adjroff.p, h->adj_roff.data(), (size_t)npairs * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(h->d_adjprog.p, 0, (size_t)items * sizeof(int), h->stream));
+    CK(cudaMemsetAsync(h->d_adjctr.p, 0, 2 * sizeof(int), h->stream));
+    CK(cudaMemsetAsync(h->d_status.p, 0, sizeof(int), h->stream));
     AdjArgs a;
     fill_adj(h, a);
-    CK(launch_adj_fwd(a, h->stream));
-    h->launches += 2;
+    const int grid = (int)std::min<long long>((long long)h->nsm * std::max(fwd_occ, 1), (items + ADJ_WARPS - 1) / ADJ_WARPS);
+    CK(launch_adj_fwd(a, grid, h->stream));
+    h->launches += 3;
+    c2_status st = adj_status(h);
+    if (st != C2_OK) return st;
     CK(cudaMemcpyAsync(logz, h->d_adjlogz.p, (size_t)npairs * 4, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     h->adj_fwd_done = true;
@@ -1899,8 +1954,13 @@ extern "C" c2_status c2_logz_bwd(c2_handle* h, float* grad)
     CK(cudaSetDevice(h->device));
     AdjArgs a;
     fill_adj(h, a);
-    CK(launch_adj_bwd(a, h->stream));
+    const long long items = (long long)a.npairs * a.nstrips;
+    CK(cudaMemsetAsync(h->d_adjprog.p + items, 0, (size_t)items * sizeof(int), h->stream));
+    CK(cudaMemsetAsync(h->d_adjctr.p + 1, 0, sizeof(int), h->stream));
+    CK(launch_adj_bwd(a, h->adj_bgrid, h->stream));
     h->launches += 2;
+    c2_status st = adj_status(h);
+    if (st != C2_OK) return st;
     CK(cudaMemcpyAsync(grad, h->d_adjgrad.p, (size_t)a.npairs * 9 * 4, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return C2_OK;
@@ -1913,15 +1973,19 @@ extern "C" c2_status c2_logz_cells(c2_handle* h, int32_t pair, float* dlogz_ds, 
         return fail(h, C2_ERR_STATE, "logz_cells: no such pair after logz_fwd/logz_bwd");
     CK(cudaSetDevice(h->device));
     const int Lq = h->Lq, L = h->h_plen[h->adj_prof[pair]];
-    const size_t n = (size_t)Lq * L;
+    const int ns = (Lq + 31) / 32;
+    const size_t n = (size_t)ns * (L + 31) * 32;
     std::vector<float> t(n);
     const long long NC = h->adj_cells;
     for (int w = 0; w < 2; w++) {
         float* dst = w ? post : dlogz_ds;
         if (!dst) continue;
-        CK(cudaMemcpy(t.data(), h->d_adjbuf.p + (13 + w) * NC + h->adj_off[pair], n * 4, cudaMemcpyDeviceToHost));
-        for (int j = 0; j < L; j++)
-            for (int i = 0; i < Lq; i++) dst[(size_t)i * L + j] = t[(size_t)j * Lq + i];   // row-major [Lq][L]
+        CK(cudaMemcpy(t.data(), h->d_adjbuf.p + (3 + w) * NC + h->adj_off[pair], n * 4, cudaMemcpyDeviceToHost));
+        // wavefront order -> row-major [Lq][L]
+        for (int i = 0; i < Lq; i++) {
+            const size_t rb = ((size_t)(i >> 5) * (L + 31) + (i & 31)) * 32 + (i & 31);
+            for (int j = 0; j < L; j++) dst[(size_t)i * L + j] = t[rb + (size_t)j * 32];
+        }
     }
     return C2_OK;
 }

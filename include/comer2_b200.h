@@ -364,7 +364,8 @@ c2_status c2_db2bin_descriptions(const char* path, char* buf, size_t* bytes, int
 /* Differentiable alignment (no counterpart in the reference, whose
  * forward-backward only feeds its MAP alignment).  Log-partition of the MAP
  * forward model -- the recursion of src/libmycu/cumapdp/CuBatchMAPDP_fwd.cu
- * with exact exp/log -- for the current query against db profiles
+ * with true exp/log (hardware forms, ~1e-7 relative) -- for the current
+ * query against db profiles
  * `profiles[0..npairs)`, over the score matrix S = s0 + wss*ss + wcv*cv
  * (amino-acid score; SS and context-vector terms before their weights) and
  * with theta[7] (MM MI MD IM II DM DD, may be NULL = 0) added to the query's
