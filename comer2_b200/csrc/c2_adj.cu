@@ -132,22 +132,23 @@ __global__ void __launch_bounds__(ADJ_WARPS * 32) adj_score_kernel(AdjArgs a)
     __shared__ float rings[ADJ_WARPS][64 * ADJ_REC];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float* ring = rings[wid];
-    const long long nitems = (long long)a.npairs * a.nstrips;
-    const long long nw = (long long)gridDim.x * ADJ_WARPS;
+    const int nw = gridDim.x * ADJ_WARPS;
     const ScoreConsts& sc = a.sc;
     const int card = sc.ssss_card;
-    for (long long it = (long long)blockIdx.x * ADJ_WARPS + wid; it < nitems; it += nw) {
-        const int m = (int)(it % a.npairs), s = (int)(it / a.npairs);
+    for (int it = blockIdx.x * ADJ_WARPS + wid; it < a.nitems; it += nw) {
+        const int2 ms = a.items_f[it];
+        const int m = ms.x, s = ms.y;
         const int p = a.prof[m];
-        const int L = a.plen[p], Lq = a.Lq;
+        const int L = a.plen[p], Lq = a.pLq[m];
         const int r = 32 * s + lane;
         const bool act = r < Lq;
-        const float* qr = a.qrec + (long long)(act ? r : 0) * QR_STRIDE;
+        const float* qr = a.qrec + (a.qpos[m] + (act ? r : 0)) * QR_STRIDE;
         const float* bd = a.pbkg + (long long)p * NAA;
+        const float* qb = a.qbkg + (long long)a.qidx[m] * NAA;
         // the query row's amino-acid odds for this pair, CV vector and SS values
         float qt[NAA], qc[NCV];
 #pragma unroll
-        for (int k = 0; k < NAA; k++) qt[k] = __fdividef(qr[QR_TRG + k], 0.5f * (a.qbkg[k] + bd[k]));
+        for (int k = 0; k < NAA; k++) qt[k] = __fdividef(qr[QR_TRG + k], 0.5f * (qb[k] + bd[k]));
 #pragma unroll
         for (int k = 0; k < NCV; k++) qc[k] = qr[QR_CV + k];
         const float qcn = qr[QR_CN], qpr = qr[QR_PRIOR], qhq = qr[QR_HQ];
@@ -279,20 +280,20 @@ __device__ __forceinline__ void adj_fwd_strip(const AdjArgs& a, int m, int s, in
                                               float* __restrict__ Fw, bool& broken, float& zm, float& zs)
 {
     const int p = a.prof[m];
-    const int L = a.plen[p], Lq = a.Lq, ns = a.nstrips;
+    const int L = a.plen[p], Lq = a.pLq[m], ns = (Lq + 31) >> 5;
     const long long cb = a.off[m] + (long long)s * (L + 31) * 32;
     const float* dt0 = a.dtrn + (a.poff[p] + p) * 7;
     const float* above = a.frow + a.roff[m] + (long long)(s > 0 ? s - 1 : 0) * 5 * L;   // read when s > 0
     float* mine_row = a.frow + a.roff[m] + (long long)s * 5 * L;
-    const int* pf = a.prog + (long long)m * ns;
+    const int* pf = a.prog + a.soff[m];
     const int r = 32 * s + lane;
     const bool act = r < Lq;
     const X5 INIT = {0.f, XLOG0, XLOG0, XLOG0, XLOG0};
     float q7[7];
-    xtrn_fwd(a.qtrn, r, Lq, q7);
+    xtrn_fwd(a.qtrn + (a.qpos[m] + a.qidx[m]) * 7, r, Lq, q7);
 #pragma unroll
     for (int k = 0; k < 7; k++) q7[k] += a.theta[k];
-    const float* cf = a.qcfx + (long long)(act ? r : 0) * 6;
+    const float* cf = a.qcfx + (a.qpos[m] + (act ? r : 0)) * 6;
     const X5 LB = (lane == 31) ? INIT : X5{0.f, cf[0], cf[1], cf[2], XLOG0};
     const X5 DB = (lane == 31 || lane == 0) ? INIT : X5{0.f, cf[3], cf[4], cf[5], XLOG0};
     const bool wr_row = !RECOMP && lane == 31 && s + 1 < ns;
@@ -349,7 +350,7 @@ __device__ __forceinline__ void adj_fwd_strip(const AdjArgs& a, int m, int s, in
             if (wr_row) {
                 mine_row[j] = nw.MM; mine_row[L + j] = nw.MI; mine_row[2 * L + j] = nw.IM;
                 mine_row[3 * L + j] = nw.DN; mine_row[4 * L + j] = nw.ND;
-                pipe_publish(a.prog + (long long)m * ns + s, j, L);
+                pipe_publish(a.prog + a.soff[m] + s, j, L);
             }
         }
         mine = nw;
@@ -363,14 +364,14 @@ __global__ void __launch_bounds__(ADJ_WARPS * 32) adj_fwd_kernel(AdjArgs a)
     __shared__ __align__(16) float rabs[ADJ_WARPS][32 * 8];
     __shared__ float trss[ADJ_WARPS][128 * 7];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int nitems = a.npairs * a.nstrips;
     bool broken = false;
     for (;;) {
         int item = 0;
         if (lane == 0) item = atomicAdd(a.counter, 1);
         item = __shfl_sync(FULL, item, 0);
-        if (item >= nitems) break;
-        const int m = item % a.npairs, s = item / a.npairs;
+        if (item >= a.nitems) break;
+        const int2 ms = a.items_f[item];
+        const int m = ms.x, s = ms.y;
         float zm = -INFINITY, zs = 0.f;
         adj_fwd_strip<false>(a, m, s, lane, rabs[wid], trss[wid], nullptr, broken, zm, zs);
         // combine the lanes' (max, sum) pairs
@@ -382,8 +383,9 @@ __global__ void __launch_bounds__(ADJ_WARPS * 32) adj_fwd_kernel(AdjArgs a)
             zm = mx;
         }
         if (lane == 0) {
-            a.zpart[2LL * item] = zm;
-            a.zpart[2LL * item + 1] = zs;
+            const long long o = a.soff[m] + s;
+            a.zpart[2 * o] = zm;
+            a.zpart[2 * o + 1] = zs;
         }
         __syncwarp();
     }
@@ -395,8 +397,9 @@ __global__ void adj_logz_kernel(AdjArgs a)
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= a.npairs) return;
     float zm = -INFINITY, zs = 0.f;
-    for (int s = 0; s < a.nstrips; s++) {
-        const long long it = (long long)s * a.npairs + m;
+    const int ns = (a.pLq[m] + 31) >> 5;
+    for (int s = 0; s < ns; s++) {
+        const long long it = a.soff[m] + s;
         const float om = a.zpart[2 * it], os = a.zpart[2 * it + 1];
         const float mx = fmaxf(zm, om);
         zs = (mx == -INFINITY) ? 0.f : zs * xexp(zm - mx) + os * xexp(om - mx);
@@ -422,7 +425,7 @@ __device__ __forceinline__ void adj_bwd_strip(const AdjArgs& a, int m, int s, in
                                               const float* __restrict__ Fw, bool& broken)
 {
     const int p = a.prof[m];
-    const int L = a.plen[p], Lq = a.Lq, ns = a.nstrips;
+    const int L = a.plen[p], Lq = a.pLq[m], ns = (Lq + 31) >> 5;
     const long long base = a.off[m];
     const long long cb = base + (long long)s * (L + 31) * 32;
     const float lz = a.logz[m];
@@ -431,19 +434,20 @@ __device__ __forceinline__ void adj_bwd_strip(const AdjArgs& a, int m, int s, in
     const float* below = a.brow + a.roff[m] + (long long)(has_below ? s + 1 : s) * 5 * L;   // read when has_below
     float* mine_row = a.brow + a.roff[m] + (long long)s * 5 * L;
     const float* fab = a.frow + a.roff[m] + (long long)(s > 0 ? s - 1 : 0) * 5 * L;   // row 32 s - 1 (s > 0)
-    const int* pb = a.prog + (long long)a.npairs * ns + (long long)m * ns + (has_below ? s + 1 : s);
+    const int* pb = a.prog + a.nitems + a.soff[m] + (has_below ? s + 1 : s);
     const int t = lane;
     const int lf = 31 - t;            // the lane's row within the strip
     const int i = 32 * s + lf;
     const bool act = i < Lq;
     const X5 INIT = {0.f, XLOG0, XLOG0, XLOG0, XLOG0};
     float qb[7], qf[7];
-    xtrn_bwd(a.qtrn, i, Lq, qb);
-    xtrn_fwd(a.qtrn, i, Lq, qf);
+    const float* qt0 = a.qtrn + (a.qpos[m] + a.qidx[m]) * 7;
+    xtrn_bwd(qt0, i, Lq, qb);
+    xtrn_fwd(qt0, i, Lq, qf);
 #pragma unroll
     for (int k = 0; k < 7; k++) { qb[k] += a.theta[k]; qf[k] += a.theta[k]; }
     // column -1 states of row i (the forward's left and diagonal at column 0)
-    const float* cf = a.qcfx + (long long)(act ? i : 0) * 6;
+    const float* cf = a.qcfx + (a.qpos[m] + (act ? i : 0)) * 6;
     const X5 LB = (lf == 31) ? INIT : X5{0.f, cf[0], cf[1], cf[2], XLOG0};
     const X5 DB = (lf == 31 || lf == 0) ? INIT : X5{0.f, cf[3], cf[4], cf[5], XLOG0};
     const bool wr_row = (t == 31) && s > 0;
@@ -569,7 +573,7 @@ __device__ __forceinline__ void adj_bwd_strip(const AdjArgs& a, int m, int s, in
             if (wr_row) {
                 mine_row[ca] = nw.MM; mine_row[L + ca] = nw.MI; mine_row[2 * L + ca] = nw.IM;
                 mine_row[3 * L + ca] = nw.DN; mine_row[4 * L + ca] = nw.ND;
-                pipe_publish(a.prog + (long long)a.npairs * ns + (long long)m * ns + s, jm, L);
+                pipe_publish(a.prog + a.nitems + a.soff[m] + s, jm, L);
             }
         }
         mine = nw;
@@ -584,7 +588,7 @@ __device__ __forceinline__ void adj_bwd_strip(const AdjArgs& a, int m, int s, in
         g[f] = v;
     }
     if (lane == 0) {
-        float* o = a.gpart + ((long long)(ns - 1 - s) * a.npairs + m) * 9;
+        float* o = a.gpart + (a.soff[m] + s) * 9;
 #pragma unroll
         for (int f = 0; f < 9; f++) o[f] = g[f];
     }
@@ -596,14 +600,14 @@ __global__ void __launch_bounds__(ADJ_WARPS * 32) adj_bwd_kernel(AdjArgs a)
     __shared__ float trss[ADJ_WARPS][128 * 7];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float* Fw = a.scratch + ((long long)blockIdx.x * ADJ_WARPS + wid) * a.scratch_stride;
-    const int nitems = a.npairs * a.nstrips;
     bool broken = false;
     for (;;) {
         int item = 0;
         if (lane == 0) item = atomicAdd(a.counter + 1, 1);
         item = __shfl_sync(FULL, item, 0);
-        if (item >= nitems) break;
-        const int m = item % a.npairs, s = a.nstrips - 1 - item / a.npairs;
+        if (item >= a.nitems) break;
+        const int2 ms = a.items_b[item];
+        const int m = ms.x, s = ms.y;
         float zm = 0.f, zs = 0.f;
         adj_fwd_strip<true>(a, m, s, lane, rabs[wid], trss[wid], Fw, broken, zm, zs);
         __syncwarp();
@@ -618,8 +622,9 @@ __global__ void adj_gsum_kernel(AdjArgs a)
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= a.npairs * 9) return;
     const int m = x / 9, f = x % 9;
+    const int ns = (a.pLq[m] + 31) >> 5;
     float v = 0.f;
-    for (int s = 0; s < a.nstrips; s++) v += a.gpart[((long long)(a.nstrips - 1 - s) * a.npairs + m) * 9 + f];
+    for (int s = 0; s < ns; s++) v += a.gpart[(a.soff[m] + s) * 9 + f];
     a.grad[x] = v;
 }
 
@@ -633,8 +638,7 @@ cudaError_t adj_occupancy(int* fwd_ctas_per_sm, int* bwd_ctas_per_sm)
 cudaError_t launch_adj_fwd(const AdjArgs& a, int grid, cudaStream_t st)
 {
     if (a.npairs <= 0) return cudaSuccess;
-    const long long items = (long long)a.npairs * a.nstrips;
-    const int sgrid = (int)std::min<long long>((items + 3) / 4, 1184);
+    const int sgrid = std::min((a.nitems + ADJ_WARPS - 1) / ADJ_WARPS, 1184);
     adj_score_kernel<<<sgrid, 128, 0, st>>>(a);
     adj_fwd_kernel<<<grid, ADJ_WARPS * 32, 0, st>>>(a);
     adj_logz_kernel<<<(a.npairs + 127) / 128, 128, 0, st>>>(a);

@@ -145,16 +145,20 @@ struct c2_handle {
     std::vector<float> h_qrec;
     DevBuf<float> d_qrec, d_qbkg, d_qtrn, d_qcf, d_qcfx, d_qU;
     // differentiable alignment (c2_logz_fwd / c2_logz_bwd)
-    std::vector<int> adj_prof;
+    std::vector<int> adj_prof, adj_Lq;
     std::vector<long long> adj_off, adj_roff;   // per pair: first cell (wavefront order), first row-buffer float
     long long adj_cells = 0, adj_rows = 0;
-    int adj_Lmax = 0, adj_bgrid = 0;              // longest profile of the pairs; backward sweep CTAs
-    bool adj_fwd_done = false;
+    int adj_Lmax = 0, adj_bgrid = 0, adj_nitems = 0;   // longest profile of the pairs; backward CTAs; strips
+    bool adj_fwd_done = false, adj_batch = false;      // adj_batch: the pairs' queries are in d_adjq*
     float adj_theta[7] = {0, 0, 0, 0, 0, 0, 0};
     float adj_wss = 0.f, adj_wcv = 0.f;
-    DevBuf<int> d_adjprof, d_adjprog, d_adjctr;
-    DevBuf<long long> d_adjoff, d_adjroff;
+    DevBuf<int> d_adjprof, d_adjprog, d_adjctr, d_adjLq, d_adjqidx;
+    DevBuf<long long> d_adjoff, d_adjroff, d_adjqpos, d_adjsoff;
+    DevBuf<int2> d_adjitems;
     DevBuf<float> d_adjbuf, d_adjlogz, d_adjgrad, d_adjpart, d_adjscr;
+    DevBuf<float> d_adjqrec, d_adjqtrn, d_adjqcfx, d_adjqbkg;   // queries of c2_set_query_batch
+    std::vector<int> adj_qlen;                                   // their lengths
+    std::vector<long long> adj_qstart;                           // and first rows
     DevBuf<unsigned char> d_qaa, d_qss;
     float scorethld = 0.f, logevthld = 0.f;
     unsigned long long searchspace = 0, deltalen = 0;
@@ -715,6 +719,50 @@ extern "C" c2_status c2_share_db(c2_handle* dst, const c2_handle* src)
     return C2_OK;
 }
 
+// Score fields of the query records (profile 0 of q): target probabilities,
+// context vector, CV norm and prior, SS probabilities, P(H) + 0.1
+static void qrec_score_fields(const c2_handle* h, const c2_profiles* q, float* qrec)
+{
+    const int Lq = q->lengths[0];
+    const float lok = h->sc.lokappa0;
+    for (int r = 0; r < Lq; r++) {
+        float* rr = qrec + (size_t)r * QR_STRIDE;
+        memcpy(rr + QR_TRG, q->trg + (size_t)r * NAA, NAA * 4);
+        memcpy(rr + QR_CV, q->cv + (size_t)r * NCV, NCV * 4);
+        rr[QR_CN] = (q->cvnorm2[r] + 1.0f) + lok;
+        const float pr = q->cvprior[r];
+        rr[QR_PRIOR] = h->prm.mapaln ? pr : (float)(int)pr;
+        const float* s3 = q->ss + (size_t)r * NSS;
+        rr[QR_SS + 0] = s3[0]; rr[QR_SS + 1] = s3[1]; rr[QR_SS + 2] = s3[2];
+        rr[QR_HQ] = s3[2] + 0.1f;
+    }
+}
+
+// Column -1 states of the query rows in the log-partition model (the MAP
+// forward's boundary with exact exp/log): per row MI IM DN of the row and of
+// the row before
+static void colm1_exact(const c2_profiles* q, float* qx)
+{
+    const int Lq = q->lengths[0];
+    auto xl2 = [](double a, double b) { const double m = std::max(a, b); return std::log(std::exp(a - m) + std::exp(b - m)) + m; };
+    double pMI = 0, pIM = 0, pDN = 0;
+    for (int r = 0; r < Lq; r++) {
+        float t[7];
+        trn_of(q, 0, r, t);
+        const double L0 = -99.0;
+        double uMI = L0, uDN = L0;
+        if (r % 32 != 0) { uMI = pMI; uDN = pDN; }
+        const double mi = xl2((0.0 + t[TMM]) + L0, (uMI + t[TMM]) + L0);
+        const double im = (r % 32 == 0) ? xl2((0.0 + t[TMI]) + L0, (L0 + t[TII]) + L0)
+                                        : xl2((0.0 + t[TMI]) + L0, ((((0.0 + t[TMI]) + L0) + t[TII]) + L0));
+        const double dn = xl2(0.0 + t[TMD], uDN + t[TDD]);
+        float* c = qx + (size_t)r * 6;
+        c[0] = (float)mi; c[1] = (float)im; c[2] = (float)dn;
+        c[3] = (float)pMI; c[4] = (float)pIM; c[5] = (float)pDN;
+        pMI = mi; pIM = im; pDN = dn;
+    }
+}
+
 extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
 {
     if (!h) return C2_ERR_ARG;
@@ -745,17 +793,9 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
         else cIM[r] = (0.f + t[TMI]) + LOG0;
         cDN[r] = hmax(uMM + t[TMD], uDN + t[TDD]);
     }
-    const float lok = h->sc.lokappa0;
+    qrec_score_fields(h, q, h->h_qrec.data());
     for (int r = 0; r < Lq; r++) {
         float* rr = h->h_qrec.data() + (size_t)r * QR_STRIDE;
-        memcpy(rr + QR_TRG, q->trg + (size_t)r * NAA, NAA * 4);
-        memcpy(rr + QR_CV, q->cv + (size_t)r * NCV, NCV * 4);
-        rr[QR_CN] = (q->cvnorm2[r] + 1.0f) + lok;
-        const float pr = q->cvprior[r];
-        rr[QR_PRIOR] = h->prm.mapaln ? pr : (float)(int)pr;
-        const float* s3 = q->ss + (size_t)r * NSS;
-        rr[QR_SS + 0] = s3[0]; rr[QR_SS + 1] = s3[1]; rr[QR_SS + 2] = s3[2];
-        rr[QR_HQ] = s3[2] + 0.1f;
         trn_of(q, 0, r, rr + QR_TRN);
         rr[QR_C + 0] = cMI[r]; rr[QR_C + 1] = cIM[r]; rr[QR_C + 2] = cDN[r];
         if (r > 0) { rr[QR_CP + 0] = cMI[r - 1]; rr[QR_CP + 1] = cIM[r - 1]; rr[QR_CP + 2] = cDN[r - 1]; }
@@ -856,25 +896,7 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
         CK(cudaMemcpyAsync(h->d_qcf.p, qcf.data(), qcf.size() * 4, cudaMemcpyHostToDevice, h->stream));
         // the same column -1 states with exact exp/log, for the log-partition model
         std::vector<float> qx((size_t)Lq * 6, 0.f);
-        {
-            auto xl2 = [](double a, double b) { const double m = std::max(a, b); return std::log(std::exp(a - m) + std::exp(b - m)) + m; };
-            double pMI = 0, pIM = 0, pDN = 0;
-            for (int r = 0; r < Lq; r++) {
-                float t[7];
-                trn_of(q, 0, r, t);
-                const double L0 = -99.0;
-                double uMI = L0, uDN = L0;
-                if (r % 32 != 0) { uMI = pMI; uDN = pDN; }
-                const double mi = xl2((0.0 + t[TMM]) + L0, (uMI + t[TMM]) + L0);
-                const double im = (r % 32 == 0) ? xl2((0.0 + t[TMI]) + L0, (L0 + t[TII]) + L0)
-                                                : xl2((0.0 + t[TMI]) + L0, ((((0.0 + t[TMI]) + L0) + t[TII]) + L0));
-                const double dn = xl2(0.0 + t[TMD], uDN + t[TDD]);
-                float* c = qx.data() + (size_t)r * 6;
-                c[0] = (float)mi; c[1] = (float)im; c[2] = (float)dn;
-                c[3] = (float)pMI; c[4] = (float)pIM; c[5] = (float)pDN;
-                pMI = mi; pIM = im; pDN = dn;
-            }
-        }
+        colm1_exact(q, qx.data());
         if (h->d_qcfx.ensure(qx.size(), h->budget)) return fail(h, C2_ERR_NOMEM, "query side arrays allocation failed");
         CK(cudaMemcpyAsync(h->d_qcfx.p, qx.data(), qx.size() * 4, cudaMemcpyHostToDevice, h->stream));
         CK(cudaStreamSynchronize(h->stream));
@@ -1823,28 +1845,42 @@ extern "C" c2_status c2_run_phase1_static(c2_handle* h, float* d_best, uint32_t*
 // Differentiable alignment (no counterpart in the reference): log-partition
 // of the MAP forward model and its gradients (model in c2_adj.cu).
 
+static c2_profiles query_view(const c2_profiles* qs, int k, const int64_t* zero);
+
 static void fill_adj(c2_handle* h, AdjArgs& a)
 {
     memset(&a, 0, sizeof a);
     const long long NC = h->adj_cells, NR = h->adj_rows;
-    a.Lq = h->Lq;
     a.npairs = (int)h->adj_prof.size();
-    a.nstrips = (h->Lq + 31) / 32;
+    a.nitems = h->adj_nitems;
     a.prof = h->d_adjprof.p;
+    a.pLq = h->d_adjLq.p;
+    a.qpos = h->d_adjqpos.p;
+    a.qidx = h->d_adjqidx.p;
+    a.soff = h->d_adjsoff.p;
+    a.items_f = h->d_adjitems.p;
+    a.items_b = h->d_adjitems.p + h->adj_nitems;
     a.off = h->d_adjoff.p;
     a.roff = h->d_adjroff.p;
     a.plen = h->db->d_plen.p;
     a.poff = h->db->d_poff.p;
-    a.qrec = h->d_qrec.p;
     a.drec = h->db->d_drec.p;
     a.pbkg = h->db->d_pbkg.p;
-    a.qbkg = h->d_qbkg.p;
+    if (h->adj_batch) {
+        a.qrec = h->d_adjqrec.p;
+        a.qbkg = h->d_adjqbkg.p;
+        a.qtrn = h->d_adjqtrn.p;
+        a.qcfx = h->d_adjqcfx.p;
+    } else {
+        a.qrec = h->d_qrec.p;
+        a.qbkg = h->d_qbkg.p;
+        a.qtrn = h->d_qtrn.p;
+        a.qcfx = h->d_qcfx.p;
+    }
     a.ssss = h->d_ssss.p;
     a.cvvals = h->d_cvvals.p;
     a.sc = h->sc;
-    a.qtrn = h->d_qtrn.p;
     a.dtrn = h->db->d_dtrn.p;
-    a.qcfx = h->d_qcfx.p;
     for (int k = 0; k < 7; k++) a.theta[k] = h->adj_theta[k];
     a.wss = h->adj_wss;
     a.wcv = h->adj_wcv;
@@ -1856,10 +1892,9 @@ static void fill_adj(c2_handle* h, AdjArgs& a)
     a.post = b + 4 * NC;
     a.frow = b + 5 * NC;
     a.brow = b + 5 * NC + NR;
-    const long long items = (long long)a.npairs * a.nstrips;
     a.prog = h->d_adjprog.p;
     a.zpart = h->d_adjpart.p;
-    a.gpart = h->d_adjpart.p + 2 * items;
+    a.gpart = h->d_adjpart.p + 2LL * h->adj_nitems;
     a.scratch = h->d_adjscr.p;
     a.scratch_stride = (long long)(h->adj_Lmax + 31) * 160;
     a.counter = h->d_adjctr.p;
@@ -1879,40 +1914,65 @@ static c2_status adj_status(c2_handle* h)
     return C2_OK;
 }
 
-extern "C" c2_status c2_logz_fwd(c2_handle* h, const int32_t* profiles, int32_t npairs, const float* theta, float wss,
-                                 float wcv, float* logz)
+// The forward sweep over pairs (query qidx[k] of length Lq[k] from row
+// qpos[k] of the query arrays, db profile profiles[k]): per-pair layout,
+// work item tables, scratch, launch.
+static c2_status logz_fwd_pairs(c2_handle* h, const int32_t* profiles, const int* Lq, const long long* qpos,
+                                const int* qidx, int32_t npairs, const float* theta, float wss, float wcv,
+                                float* logz)
 {
-    if (!h || !profiles || npairs <= 0 || !logz) return C2_ERR_ARG;
-    if (h->nprof <= 0 || h->Lq <= 0) return fail(h, C2_ERR_STATE, "logz_fwd needs a database and a query");
-    CK(cudaSetDevice(h->device));
     h->adj_fwd_done = false;
-    const int ns = (h->Lq + 31) / 32;
     h->adj_prof.assign(profiles, profiles + npairs);
+    h->adj_Lq.assign(Lq, Lq + npairs);
     h->adj_off.resize(npairs);
     h->adj_roff.resize(npairs);
-    long long acc = 0, racc = 0;
-    int lmax = 0;
+    std::vector<long long> soff(npairs);
+    long long acc = 0, racc = 0, sacc = 0;
+    int lmax = 0, nsmax = 0;
     for (int k = 0; k < npairs; k++) {
         if (profiles[k] < 0 || profiles[k] >= h->nprof)
             return fail(h, C2_ERR_ARG, "logz_fwd: profile %d out of range", profiles[k]);
         const int L = h->h_plen[profiles[k]];
+        const int ns = (Lq[k] + 31) / 32;
         h->adj_off[k] = acc;
         h->adj_roff[k] = racc;
+        soff[k] = sacc;
         acc += (long long)ns * (L + 31) * 32;
         racc += (long long)ns * 5 * L;
+        sacc += ns;
         lmax = std::max(lmax, L);
+        nsmax = std::max(nsmax, ns);
+    }
+    if (sacc > 0x7fffffff) return fail(h, C2_ERR_CAPACITY, "logz_fwd: %lld strips", sacc);
+    const int items = (int)sacc;
+    // work items: the forward sweep by strip, the backward sweep by strip
+    // from each pair's last one
+    std::vector<int2> it((size_t)2 * items);
+    {
+        size_t f = 0, b = items;
+        for (int s = 0; s < nsmax; s++)
+            for (int k = 0; k < npairs; k++) {
+                const int ns = (Lq[k] + 31) / 32;
+                if (s < ns) {
+                    it[f++] = make_int2(k, s);
+                    it[b++] = make_int2(k, ns - 1 - s);
+                }
+            }
     }
     h->adj_cells = acc;
     h->adj_rows = racc;
     h->adj_Lmax = lmax;
+    h->adj_nitems = items;
     for (int k = 0; k < 7; k++) h->adj_theta[k] = theta ? theta[k] : 0.f;
     h->adj_wss = wss;
     h->adj_wcv = wcv;
-    const long long items = (long long)npairs * ns;
     if (h->d_adjprof.ensure(npairs, h->budget) || h->d_adjoff.ensure(npairs, h->budget) ||
-        h->d_adjroff.ensure(npairs, h->budget) || h->d_adjbuf.ensure((size_t)(5 * acc + 2 * racc), h->budget) ||
+        h->d_adjroff.ensure(npairs, h->budget) || h->d_adjLq.ensure(npairs, h->budget) ||
+        h->d_adjqpos.ensure(npairs, h->budget) || h->d_adjqidx.ensure(npairs, h->budget) ||
+        h->d_adjsoff.ensure(npairs, h->budget) || h->d_adjitems.ensure((size_t)2 * items, h->budget) ||
+        h->d_adjbuf.ensure((size_t)(5 * acc + 2 * racc), h->budget) ||
         h->d_adjlogz.ensure(npairs, h->budget) || h->d_adjgrad.ensure((size_t)npairs * 9, h->budget) ||
-        h->d_adjprog.ensure((size_t)(2 * items), h->budget) || h->d_adjpart.ensure((size_t)(11 * items), h->budget) ||
+        h->d_adjprog.ensure((size_t)2 * items, h->budget) || h->d_adjpart.ensure((size_t)11 * items, h->budget) ||
         h->d_adjctr.ensure(2, h->budget))
         return fail(h, C2_ERR_NOMEM, "logz_fwd: scratch for %d pairs (%lld cells) failed", npairs, acc);
     // persistent grids of the sweeps: as many CTAs as are resident (or as
@@ -1929,6 +1989,11 @@ extern "C" c2_status c2_logz_fwd(c2_handle* h, const int32_t* profiles, int32_t 
     (void)cudaGetLastError();   // a refused allocation above is not an error of what follows
     if (h->adj_bgrid == 0) return fail(h, C2_ERR_NOMEM, "logz_fwd: backward sweep scratch (%zu bytes per CTA) failed", per_cta);
     CK(cudaMemcpyAsync(h->d_adjprof.p, profiles, (size_t)npairs * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_adjLq.p, Lq, (size_t)npairs * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_adjqpos.p, qpos, (size_t)npairs * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_adjqidx.p, qidx, (size_t)npairs * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_adjsoff.p, soff.data(), (size_t)npairs * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_adjitems.p, it.data(), it.size() * sizeof(int2), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_adjoff.p, h->adj_off.data(), (size_t)npairs * 8, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_adjroff.p, h->adj_roff.data(), (size_t)npairs * 8, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemsetAsync(h->d_adjprog.p, 0, (size_t)items * sizeof(int), h->stream));
@@ -1947,6 +2012,82 @@ extern "C" c2_status c2_logz_fwd(c2_handle* h, const int32_t* profiles, int32_t 
     return C2_OK;
 }
 
+extern "C" c2_status c2_logz_fwd(c2_handle* h, const int32_t* profiles, int32_t npairs, const float* theta, float wss,
+                                 float wcv, float* logz)
+{
+    if (!h || !profiles || npairs <= 0 || !logz) return C2_ERR_ARG;
+    if (h->nprof <= 0 || h->Lq <= 0) return fail(h, C2_ERR_STATE, "logz_fwd needs a database and a query");
+    CK(cudaSetDevice(h->device));
+    h->adj_batch = false;
+    const std::vector<int> Lq(npairs, h->Lq), qidx(npairs, 0);
+    const std::vector<long long> qpos(npairs, 0);
+    return logz_fwd_pairs(h, profiles, Lq.data(), qpos.data(), qidx.data(), npairs, theta, wss, wcv, logz);
+}
+
+extern "C" c2_status c2_set_query_batch(c2_handle* h, const c2_profiles* queries)
+{
+    if (!h || !queries) return C2_ERR_ARG;
+    c2_status st = check_profiles(h, queries);
+    if (st != C2_OK) return st;
+    CK(cudaSetDevice(h->device));
+    const int nq = queries->nprofiles;
+    // the queries' rows as c2_set_query packs them (score fields, exact
+    // column -1 states), raw transitions and backgrounds, concatenated; the
+    // queries packed by up to 16 host threads
+    const long long N = queries->npositions;
+    std::vector<float> qrec((size_t)N * QR_STRIDE, 0.f), qcf((size_t)N * 6, 0.f);
+    {
+        std::atomic<int> next(0);
+        auto work = [&]() {
+            const int64_t zero = 0;
+            for (int q; (q = next.fetch_add(1)) < nq;) {
+                const c2_profiles v = query_view(queries, q, &zero);
+                const size_t o = (size_t)queries->offsets[q];
+                qrec_score_fields(h, &v, qrec.data() + o * QR_STRIDE);
+                colm1_exact(&v, qcf.data() + o * 6);
+            }
+        };
+        const int nt = std::max(1, std::min(16, nq / 8));
+        std::vector<std::thread> th;
+        for (int t = 1; t < nt; t++) th.emplace_back(work);
+        work();
+        for (auto& t : th) t.join();
+    }
+    if (h->d_adjqrec.ensure(qrec.size(), h->budget) || h->d_adjqcfx.ensure(qcf.size(), h->budget) ||
+        h->d_adjqtrn.ensure((size_t)(N + nq) * 7, h->budget) || h->d_adjqbkg.ensure((size_t)nq * NAA, h->budget))
+        return fail(h, C2_ERR_NOMEM, "set_query_batch: query arrays for %d queries failed", nq);
+    CK(cudaMemcpyAsync(h->d_adjqrec.p, qrec.data(), qrec.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_adjqcfx.p, qcf.data(), qcf.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_adjqtrn.p, queries->trn, (size_t)(N + nq) * 7 * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_adjqbkg.p, queries->bkg, (size_t)nq * NAA * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));   // the host arrays above are freed on return
+    h->adj_qlen.assign(queries->lengths, queries->lengths + nq);
+    h->adj_qstart.assign(queries->offsets, queries->offsets + nq);
+    h->adj_fwd_done = false;
+    return C2_OK;
+}
+
+extern "C" c2_status c2_logz_fwd_batch(c2_handle* h, const int32_t* query_of_pair, const int32_t* profiles,
+                                       int32_t npairs, const float* theta, float wss, float wcv, float* logz)
+{
+    if (!h || !query_of_pair || !profiles || npairs <= 0 || !logz) return C2_ERR_ARG;
+    if (h->nprof <= 0) return fail(h, C2_ERR_STATE, "logz_fwd_batch needs a database");
+    if (h->adj_qlen.empty()) return fail(h, C2_ERR_STATE, "logz_fwd_batch needs c2_set_query_batch");
+    CK(cudaSetDevice(h->device));
+    const int nq = (int)h->adj_qlen.size();
+    std::vector<int> Lq(npairs), qidx(npairs);
+    std::vector<long long> qpos(npairs);
+    for (int k = 0; k < npairs; k++) {
+        const int q = query_of_pair[k];
+        if (q < 0 || q >= nq) return fail(h, C2_ERR_ARG, "logz_fwd_batch: query %d of pair %d out of range", q, k);
+        Lq[k] = h->adj_qlen[q];
+        qpos[k] = h->adj_qstart[q];
+        qidx[k] = q;
+    }
+    h->adj_batch = true;
+    return logz_fwd_pairs(h, profiles, Lq.data(), qpos.data(), qidx.data(), npairs, theta, wss, wcv, logz);
+}
+
 extern "C" c2_status c2_logz_bwd(c2_handle* h, float* grad)
 {
     if (!h || !grad) return C2_ERR_ARG;
@@ -1954,7 +2095,7 @@ extern "C" c2_status c2_logz_bwd(c2_handle* h, float* grad)
     CK(cudaSetDevice(h->device));
     AdjArgs a;
     fill_adj(h, a);
-    const long long items = (long long)a.npairs * a.nstrips;
+    const long long items = h->adj_nitems;
     CK(cudaMemsetAsync(h->d_adjprog.p + items, 0, (size_t)items * sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_adjctr.p + 1, 0, sizeof(int), h->stream));
     CK(launch_adj_bwd(a, h->adj_bgrid, h->stream));
@@ -1972,7 +2113,7 @@ extern "C" c2_status c2_logz_cells(c2_handle* h, int32_t pair, float* dlogz_ds, 
     if (!h->adj_fwd_done || pair < 0 || pair >= (int)h->adj_prof.size())
         return fail(h, C2_ERR_STATE, "logz_cells: no such pair after logz_fwd/logz_bwd");
     CK(cudaSetDevice(h->device));
-    const int Lq = h->Lq, L = h->h_plen[h->adj_prof[pair]];
+    const int Lq = h->adj_Lq[pair], L = h->h_plen[h->adj_prof[pair]];
     const int ns = (Lq + 31) / 32;
     const size_t n = (size_t)ns * (L + 31) * 32;
     std::vector<float> t(n);

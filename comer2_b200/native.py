@@ -30,6 +30,7 @@ EXPORTS = [
     "c2_db2bin_info", "c2_db2bin_read", "c2_share_db", "c2_search_batch", "c2_format_report",
     "c2_set_wait_limit", "c2_get_pair_scores", "c2_db2bin_descriptions", "c2_set_device_memory_limit",
     "c2_db2bin_lengths", "c2_db2bin_read_range", "c2_get_device_memory_info", "c2_db_device_bytes",
+    "c2_logz_fwd_batch", "c2_set_query_batch",
     "c2_get_device_memory_use", "c2_get_search_groups",
 ]
 
@@ -205,6 +206,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.c2_db2bin_descriptions.argtypes = [C.c_char_p, C.c_void_p, P(C.c_size_t), _i64p, C.c_char_p, C.c_size_t]
     lib.c2_logz_fwd.argtypes = [C.c_void_p, _i32p, C.c_int32, _fp, C.c_float, C.c_float, _fp]
     lib.c2_logz_bwd.argtypes = [C.c_void_p, _fp]
+    lib.c2_set_query_batch.argtypes = [C.c_void_p, P(c2_profiles)]
+    lib.c2_logz_fwd_batch.argtypes = [C.c_void_p, _i32p, _i32p, C.c_int32, _fp, C.c_float, C.c_float, _fp]
     lib.c2_logz_cells.argtypes = [C.c_void_p, C.c_int32, _fp, _fp]
     lib.c2_db2bin_info.argtypes = [C.c_char_p, _i32p, _i64p, C.c_char_p, C.c_size_t]
     lib.c2_db2bin_read.argtypes = [C.c_char_p, _i32p, _i64p, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _u8p, _u8p,
@@ -361,6 +364,30 @@ class Handle:
         self._ck(self.lib.c2_logz_fwd(self._h, _ptr(pr, _i32p), int(pr.shape[0]), _ptr(th, _fp),
                                       float(wss), float(wcv), _ptr(out, _fp)), "c2_logz_fwd")
         self._adj_n = int(pr.shape[0])
+        self._adj_Lq = np.full(pr.shape[0], self.Lq, np.int64)
+        return out
+
+    def set_query_batch(self, queries: ProfileSet):
+        """Pack and upload the queries of logz_fwd_batch (c2_set_query_batch)."""
+        k = _Keep()
+        qs = make_profiles(queries, k)
+        self._ck(self.lib.c2_set_query_batch(self._h, C.byref(qs)), "c2_set_query_batch")
+        self._adj_qlen = np.asarray(queries.lengths, np.int64).copy()
+
+    def logz_fwd_batch(self, query_of_pair, profiles, theta=None, wss: float = 0.0, wcv: float = 0.0) -> np.ndarray:
+        """Log-partition of independent pairs: query query_of_pair[k] of the set_query_batch
+        queries vs db profile profiles[k] (c2_logz_fwd_batch)."""
+        qi = np.ascontiguousarray(query_of_pair, np.int32)
+        pr = np.ascontiguousarray(profiles, np.int32)
+        if qi.shape != pr.shape:
+            raise C2Error("logz_fwd_batch: query_of_pair and profiles differ in length")
+        th = np.zeros(7, np.float32) if theta is None else np.ascontiguousarray(theta, np.float32)
+        out = np.zeros(pr.shape[0], np.float32)
+        self._ck(self.lib.c2_logz_fwd_batch(self._h, _ptr(qi, _i32p), _ptr(pr, _i32p), int(pr.shape[0]),
+                                            _ptr(th, _fp), float(wss), float(wcv), _ptr(out, _fp)),
+                 "c2_logz_fwd_batch")
+        self._adj_n = int(pr.shape[0])
+        self._adj_Lq = self._adj_qlen[qi]
         return out
 
     def logz_bwd(self) -> np.ndarray:
@@ -370,9 +397,11 @@ class Handle:
         return g
 
     def logz_cells(self, k: int, L: int):
-        """(dlogZ/dS, MM posterior) of pair k, each [Lq][L] (L: the pair's db profile length)."""
-        ds = np.zeros((self.Lq, L), np.float32)
-        po = np.zeros((self.Lq, L), np.float32)
+        """(dlogZ/dS, MM posterior) of pair k, each [Lq][L] (Lq: the pair's query length, L: its db
+        profile length)."""
+        lq = int(self._adj_Lq[k])
+        ds = np.zeros((lq, L), np.float32)
+        po = np.zeros((lq, L), np.float32)
         self._ck(self.lib.c2_logz_cells(self._h, int(k), _ptr(ds, _fp), _ptr(po, _fp)), "c2_logz_cells")
         return ds, po
 

@@ -370,16 +370,29 @@ c2_status c2_db2bin_descriptions(const char* path, char* buf, size_t* bytes, int
  * (amino-acid score; SS and context-vector terms before their weights) and
  * with theta[7] (MM MI MD IM II DM DD, may be NULL = 0) added to the query's
  * transition log-probabilities in every cell update.  logz[k] receives
- * log sum over cells exp(F.MM) of pair k.  Keeps the forward states for
- * c2_logz_bwd; a new query or c2_logz_fwd call replaces them. */
+ * log sum over cells exp(F.MM) of pair k.  Keeps what c2_logz_bwd needs
+ * (the scores and each 32-row strip's last forward row: the backward sweep
+ * recomputes a strip's forward states from the row above it); a new query or
+ * c2_logz_fwd call replaces them. */
 c2_status c2_logz_fwd(c2_handle* h, const int32_t* profiles, int32_t npairs, const float* theta, float wss,
                       float wcv, float* logz);
+
+/* The same for npairs independent pairs (a training batch): pair k aligns
+ * query query_of_pair[k] of the queries given to c2_set_query_batch (their
+ * own lengths; the handle's search query is not used or changed) with db
+ * profile profiles[k].  c2_logz_bwd and c2_logz_cells then serve these
+ * pairs.  c2_set_query_batch packs and uploads the queries once (profiles of
+ * up to 65,535 positions, the c2_profiles field set). */
+c2_status c2_set_query_batch(c2_handle* h, const c2_profiles* queries);
+c2_status c2_logz_fwd_batch(c2_handle* h, const int32_t* query_of_pair, const int32_t* profiles, int32_t npairs,
+                            const float* theta, float wss, float wcv, float* logz);
 
 /* Gradients of the last c2_logz_fwd: grad[9 * k + t] = dlogZ_k/dtheta_t
  * (t < 7), grad[9 * k + 7] = dlogZ_k/dwss, grad[9 * k + 8] = dlogZ_k/dwcv. */
 c2_status c2_logz_bwd(c2_handle* h, float* grad);
 
-/* Per-cell results of pair k after c2_logz_bwd, row-major [Lq][L]:
+/* Per-cell results of pair k after c2_logz_bwd, row-major [Lq][L] (Lq the
+ * pair's query length, L its db profile length):
  * dlogz_ds = dlogZ/dS (expected MM emissions), post = MM state posterior
  * exp(F.MM + B.MM - logZ).  Either pointer may be NULL. */
 c2_status c2_logz_cells(c2_handle* h, int32_t pair, float* dlogz_ds, float* post);

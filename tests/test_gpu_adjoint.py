@@ -113,3 +113,46 @@ def test_torch_autograd_wrapper(params):
     assert wss.grad.item() == pytest.approx(want[7], rel=1e-5, abs=1e-5)
     assert wcv.grad.item() == pytest.approx(want[8], rel=1e-5, abs=1e-5)
     h.close()
+
+
+def test_batch_of_independent_pairs(params, orc64):
+    """c2_logz_fwd_batch: pairs with their own queries (lengths 20, 45, 70
+    and 33; one strip, and several with a partial last strip), query 1 used
+    twice, against the oracle's log-partition and finite-difference
+    gradients of each pair, and the same values as the one-query call for
+    the pairs of one query."""
+    from comer2_b200.native import Handle
+    rng = np.random.default_rng(12)
+    qs = [S.random_profiles(rng, [n]) for n in (20, 45, 70, 33)]
+    parts = [S.planted_homolog(rng, qs[i], L, seg_lo=10, seg_hi=18) for i, L in ((0, 50), (1, 36), (2, 64), (3, 27))]
+    db = S.concat(parts + [S.random_profiles(rng, [58])])
+    Q = S.concat(qs)
+    qof = np.array([0, 1, 2, 3, 1], np.int32)
+    prof = np.array([0, 1, 2, 3, 4], np.int32)
+    wss, wcv = params.ssswgt, params.cvswgt
+    h = Handle(params, 0)
+    h.upload_db(db)
+    h.set_query_batch(Q)
+    z = h.logz_fwd_batch(qof, prof, THETA, wss, wcv)
+    g = h.logz_bwd()
+    hstep = 1e-4
+    for k in range(len(prof)):
+        qo, do = orc64.profile(qs[qof[k]]), orc64.profile(db, int(prof[k]))
+        Sk, ss, cv = _oracle_S(orc64, qo, do, wss, wcv)
+        assert z[k] == pytest.approx(orc64.logz(qo, do, Sk, THETA), rel=2e-4), k
+        for t in (0, 2, 4):
+            tp = THETA.copy(); tp[t] += hstep
+            tm = THETA.copy(); tm[t] -= hstep
+            fd = (orc64.logz(qo, do, Sk, tp) - orc64.logz(qo, do, Sk, tm)) / (2 * hstep)
+            assert abs(g[k, t] - fd) <= 2e-3 * max(1.0, abs(fd)), (k, t, g[k, t], fd)
+        fcv = (orc64.logz(qo, do, Sk + hstep * cv, THETA) - orc64.logz(qo, do, Sk - hstep * cv, THETA)) / (2 * hstep)
+        assert abs(g[k, 8] - fcv) <= 2e-3 * max(1.0, abs(fcv)), (k, g[k, 8], fcv)
+    ds, post = h.logz_cells(2, int(db.lengths[2]))
+    assert ds.shape == (70, int(db.lengths[2])) and (ds <= post + 1e-5).all()
+    # pairs 1 and 4 share query 1: the one-query call gives the same values
+    h.set_query(qs[1])
+    z1 = h.logz_fwd([1, 4], THETA, wss, wcv)
+    g1 = h.logz_bwd()
+    assert np.array_equal(z1, z[[1, 4]])
+    assert np.array_equal(g1, g[[1, 4]])
+    h.close()
