@@ -207,27 +207,32 @@ __global__ void __launch_bounds__(ADJ_WARPS * 32) adj_score_kernel(AdjArgs a)
 }
 
 // ---------------------------------------------------------------------------
-// Row buffer of a strip's neighbour, one 32-column chunk at a time, in the
-// warp's shared buffer rab[32][8] (slot l: chunk column l).  Forward: row
-// 32 s - 1 (frow of strip s - 1) at columns c0 + l; backward: row 32 s + 32
-// (brow of strip s + 1) at mirrored columns c0 + l, i.e. L - 1 - c0 - l.
-// WAIT: the neighbour strip is being swept now; wait for the chunk first.
+// Row buffer of a strip's neighbour, ADJ_RG columns at a time, in the warp's
+// shared buffer rab[32][8] (slot c & 31: column c).  Forward: row 32 s - 1
+// (frow of strip s - 1) at columns c0 + l; backward: row 32 s + 32 (brow of
+// strip s + 1) at mirrored columns c0 + l, i.e. L - 1 - c0 - l.  WAIT: the
+// neighbour strip is being swept now; wait for those columns first (a strip
+// then trails its neighbour by about 32 + ADJ_RG columns).
+constexpr int ADJ_RG = 8;
 template <bool MIRROR, bool WAIT>
 __device__ __forceinline__ void adj_load_row(const AdjArgs& a, float* rab, const float* __restrict__ row, bool have,
                                              const int* flag, int c0, int L, int lane, bool& broken)
 {
-    if (WAIT && have) pipe_wait(flag, min(c0 + 32, L), lane, a.status, broken, a.spin);
+    if (WAIT && have) pipe_wait(flag, min(c0 + ADJ_RG, L), lane, a.status, broken, a.spin);
     const int c = c0 + lane;
-    const float init[5] = {0.f, XLOG0, XLOG0, XLOG0, XLOG0};
-    float v[5];
+    if (lane < ADJ_RG) {
+        const float init[5] = {0.f, XLOG0, XLOG0, XLOG0, XLOG0};
+        float v[5];
 #pragma unroll
-    for (int f = 0; f < 5; f++) {
-        const int col = MIRROR ? L - 1 - c : c;
-        v[f] = (have && c < L) ? (WAIT ? __ldcg(row + (long long)f * L + col) : row[(long long)f * L + col]) : init[f];
+        for (int f = 0; f < 5; f++) {
+            const int col = MIRROR ? L - 1 - c : c;
+            v[f] = (have && c < L) ? (WAIT ? __ldcg(row + (long long)f * L + col) : row[(long long)f * L + col])
+                                   : init[f];
+        }
+        float* o = rab + (c & 31) * 8;
+        *reinterpret_cast<float4*>(o) = make_float4(v[0], v[1], v[2], v[3]);
+        o[4] = v[4];
     }
-    __syncwarp();
-    *reinterpret_cast<float4*>(rab + lane * 8) = make_float4(v[0], v[1], v[2], v[3]);
-    rab[lane * 8 + 4] = v[4];
     __syncwarp();
 }
 
@@ -320,8 +325,11 @@ __device__ __forceinline__ void adj_fwd_strip(const AdjArgs& a, int m, int s, in
             const float4 ba = *reinterpret_cast<const float4*>(rab + src * 8);
             const float b4 = rab[src * 8 + 4];
             if (lane == 0) up = X5{ba.x, ba.y, ba.z, ba.w, b4};
-            if (src == 31) {
+            if ((src & (ADJ_RG - 1)) == ADJ_RG - 1) {
+                __syncwarp();
                 adj_load_row<false, !RECOMP>(a, rab, above, s > 0, pwait, k + 1, L, lane, broken);
+            }
+            if (src == 31) {
                 if (k + 33 <= L) adj_stage_trn<false>(trs, dt0, k + 33, L, lane);
                 __syncwarp();
             }
@@ -502,8 +510,11 @@ __device__ __forceinline__ void adj_bwd_strip(const AdjArgs& a, int m, int s, in
             const float4 ba = *reinterpret_cast<const float4*>(rab + src * 8);
             const float b4 = rab[src * 8 + 4];
             if (lane == 0) dn = X5{ba.x, ba.y, ba.z, ba.w, b4};
-            if (src == 31) {
+            if ((src & (ADJ_RG - 1)) == ADJ_RG - 1) {
+                __syncwarp();
                 adj_load_row<true, true>(a, rab, below, has_below, pb, k + 1, L, lane, broken);
+            }
+            if (src == 31) {
                 if (k + 33 <= L) adj_stage_trn<true>(trs, dt0, k + 33, L, lane);
                 __syncwarp();
             }

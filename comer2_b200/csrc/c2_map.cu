@@ -21,6 +21,10 @@
 
 namespace c2 {
 
+// columns of the row above a strip loaded (and waited for) at a time
+constexpr int MAP_RG = 8;
+
+
 #define FULL 0xffffffffu
 constexpr float MLOG0 = -99.f;
 constexpr int MAPW = 4;     // warps per CTA of the MAP DP sweep
@@ -250,20 +254,20 @@ __device__ __forceinline__ void map_fwd_item(const MapArgs& a, const float* __re
             float t7[7];
 #pragma unroll
             for (int i = 0; i < 7; i++) t7[i] = MLOG0;
-            // row above the strip, one chunk at a time, in the warp's shared
-            // buffer rab[32][8] (slot i: column 32 c + i), waited for and loaded
-            // at the end of the chunk before
+            // row above the strip, MAP_RG columns at a time, in the warp's shared
+            // buffer rab[32][8] (slot c & 31: column c), waited for and loaded
+            // a group ahead (the strip trails the one above by ~32 + MAP_RG columns)
             const float binit[5] = {0.f, MLOG0, MLOG0, MLOG0, MLOG0};
-            if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken, a.spin);
-            {
+            if (s > 0) pipe_wait(pf + s - 1, min(MAP_RG, L), lane, a.status, broken, a.spin);
+            __syncwarp();
+            if (lane < MAP_RG) {
                 float v[5];
 #pragma unroll
                 for (int f = 0; f < 5; f++) v[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : binit[f];
-                __syncwarp();
                 *reinterpret_cast<float4*>(rab + lane * 8) = make_float4(v[0], v[1], v[2], v[3]);
                 rab[lane * 8 + 4] = v[4];
-                __syncwarp();
             }
+            __syncwarp();
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             // column k's score is loaded one step ahead, from L2: each chunk's
             // columns are prefetched a chunk earlier
@@ -287,17 +291,19 @@ __device__ __forceinline__ void map_fwd_item(const MapArgs& a, const float* __re
                     const float4 ba = *reinterpret_cast<const float4*>(rab + src * 8);
                     const float b4 = rab[src * 8 + 4];
                     if (lane == 0) up = S5{ba.x, ba.y, ba.z, ba.w, b4};
-                    if (src == 31) {
-                        if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken, a.spin);
-                        float v[5];
-#pragma unroll
-                        for (int f = 0; f < 5; f++) {
+                    if ((src & (MAP_RG - 1)) == MAP_RG - 1) {
+                        // the next group of columns into slots this step does not read
+                        if (s > 0 && k + 1 < L)
+                            pipe_wait(pf + s - 1, min(k + 1 + MAP_RG, L), lane, a.status, broken, a.spin);
+                        if (lane < MAP_RG) {
                             const int cc = k + 1 + lane;
-                            v[f] = (s > 0 && cc < L) ? __ldcg(botr + f * L + cc) : binit[f];
+                            float v[5];
+#pragma unroll
+                            for (int f = 0; f < 5; f++) v[f] = (s > 0 && cc < L) ? __ldcg(botr + f * L + cc) : binit[f];
+                            float* o = rab + (cc & 31) * 8;
+                            *reinterpret_cast<float4*>(o) = make_float4(v[0], v[1], v[2], v[3]);
+                            o[4] = v[4];
                         }
-                        __syncwarp();
-                        *reinterpret_cast<float4*>(rab + lane * 8) = make_float4(v[0], v[1], v[2], v[3]);
-                        rab[lane * 8 + 4] = v[4];
                     }
                 }
                 __syncwarp();
@@ -422,20 +428,20 @@ __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __re
             float t7[7];
 #pragma unroll
             for (int i = 0; i < 7; i++) t7[i] = MLOG0;
-            // row above the strip, one chunk at a time, in the warp's shared
-            // buffer rab[32][8] (slot i: column 32 c + i), waited for and loaded
-            // at the end of the chunk before
+            // row above the strip, MAP_RG columns at a time, in the warp's shared
+            // buffer rab[32][8] (slot c & 31: column c), waited for and loaded
+            // a group ahead (the strip trails the one above by ~32 + MAP_RG columns)
             const float binit[5] = {0.f, MLOG0, MLOG0, MLOG0, MLOG0};
-            if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken, a.spin);
-            {
+            if (s > 0) pipe_wait(pf + s - 1, min(MAP_RG, L), lane, a.status, broken, a.spin);
+            __syncwarp();
+            if (lane < MAP_RG) {
                 float v[5];
 #pragma unroll
                 for (int f = 0; f < 5; f++) v[f] = (s > 0 && lane < L) ? __ldcg(botr + f * L + lane) : binit[f];
-                __syncwarp();
                 *reinterpret_cast<float4*>(rab + lane * 8) = make_float4(v[0], v[1], v[2], v[3]);
                 rab[lane * 8 + 4] = v[4];
-                __syncwarp();
             }
+            __syncwarp();
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             const bool hasdn = act && r + 1 < Lq;
             // the diagonal-successor score of mirrored column k is loaded one step
@@ -471,17 +477,19 @@ __device__ __forceinline__ void map_bwd_item(const MapArgs& a, const float* __re
                     const float4 ba = *reinterpret_cast<const float4*>(rab + src * 8);
                     const float b4 = rab[src * 8 + 4];
                     if (lane == 0) dn = S5{ba.x, ba.y, ba.z, ba.w, b4};
-                    if (src == 31) {
-                        if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken, a.spin);
-                        float v[5];
-#pragma unroll
-                        for (int f = 0; f < 5; f++) {
+                    if ((src & (MAP_RG - 1)) == MAP_RG - 1) {
+                        // the next group of columns into slots this step does not read
+                        if (s > 0 && k + 1 < L)
+                            pipe_wait(pf + s - 1, min(k + 1 + MAP_RG, L), lane, a.status, broken, a.spin);
+                        if (lane < MAP_RG) {
                             const int cc = k + 1 + lane;
-                            v[f] = (s > 0 && cc < L) ? __ldcg(botr + f * L + cc) : binit[f];
+                            float v[5];
+#pragma unroll
+                            for (int f = 0; f < 5; f++) v[f] = (s > 0 && cc < L) ? __ldcg(botr + f * L + cc) : binit[f];
+                            float* o = rab + (cc & 31) * 8;
+                            *reinterpret_cast<float4*>(o) = make_float4(v[0], v[1], v[2], v[3]);
+                            o[4] = v[4];
                         }
-                        __syncwarp();
-                        *reinterpret_cast<float4*>(rab + lane * 8) = make_float4(v[0], v[1], v[2], v[3]);
-                        rab[lane * 8 + 4] = v[4];
                     }
                 }
                 __syncwarp();
@@ -606,8 +614,10 @@ __global__ void __launch_bounds__(MAPW * 32, 8) map_dp_kernel(MapArgs a)
             const bool act = r < Lq;
             float mine = 0.f, upp = 0.f;
             // row above the strip, one chunk at a time (lane i: column 32 c + i)
-            if (s > 0) pipe_wait(pf + s - 1, min(32, L), lane, a.status, broken, a.spin);
-            float bcur = (s > 0 && lane < L) ? __ldcg(botr + lane) : 0.f;
+            // lane c & 31 holds column c of the row above, MAP_RG columns
+            // loaded at a time, a group ahead
+            if (s > 0) pipe_wait(pf + s - 1, min(MAP_RG, L), lane, a.status, broken, a.spin);
+            float bcur = (s > 0 && lane < MAP_RG && lane < L) ? __ldcg(botr + lane) : 0.f;
             const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
             // F + B of the next step's cells is loaded one step ahead, from L2:
             // each chunk of 32 steps (32 lines of 128 bytes) is prefetched a
@@ -626,9 +636,13 @@ __global__ void __launch_bounds__(MAPW * 32, 8) map_dp_kernel(MapArgs a)
                     const int src = k & 31;
                     const float b0 = __shfl_sync(FULL, bcur, src);
                     if (lane == 0) up = b0;
+                    if ((src & (MAP_RG - 1)) == MAP_RG - 1) {
+                        if (s > 0 && k + 1 < L)
+                            pipe_wait(pf + s - 1, min(k + 1 + MAP_RG, L), lane, a.status, broken, a.spin);
+                        const int d = (lane - (k + 1)) & 31;
+                        if (d < MAP_RG) bcur = (s > 0 && k + 1 + d < L) ? __ldcg(botr + k + 1 + d) : 0.f;
+                    }
                     if (src == 31) {
-                        if (s > 0 && k + 1 < L) pipe_wait(pf + s - 1, min(k + 33, L), lane, a.status, broken, a.spin);
-                        bcur = (s > 0 && k + 1 + lane < L) ? __ldcg(botr + k + 1 + lane) : 0.f;
                         pf_line(fs, k + 33 + lane, W);
                         pf_line(bs, k + 33 + lane, W);
                     }
