@@ -123,6 +123,8 @@ struct c2_handle {
     int nsm = 0;
     int grid = 0;
     int score_mode = C2_SCORE_FP32;   // phase-1 score arithmetic (c2_set_score_mode)
+    int p1_reserve = 0;               // SMs the phase-1 kernels leave free (multi-query batches)
+    int batch_reserve = -1;           // c2_set_batch_sm_reserve (-1: nsm / BATCH_RESERVE_DIV)
     std::shared_ptr<Budget> budget = std::make_shared<Budget>();   // c2_set_device_memory_limit
     unsigned spin = PIPE_SPIN;        // polls before a phase-2 strip wait gives up (c2_set_wait_limit)
     // parameters
@@ -1040,7 +1042,7 @@ extern "C" c2_status c2_run_phase1(c2_handle* h)
         a.qaa = h->d_qaaf.p;
         a.tc = tc_consts(h->sc);
         cudaError_t oe = cudaSuccess;
-        int gt = h->nsm * p1t_blocks_per_sm(h->sc.cvcard, &oe);
+        int gt = (h->nsm - h->p1_reserve) * p1t_blocks_per_sm(h->sc.cvcard, &oe);
         if (gt < 1)
             return fail(h, C2_ERR_CUDA, "tensor-core phase-1 kernel does not fit on an SM (%s)",
                         cudaGetErrorString(oe));
@@ -1051,7 +1053,7 @@ extern "C" c2_status c2_run_phase1(c2_handle* h)
     }
     // chunked kernel: one CTA of P1C_WARPS warps per SM, within the boundary-row slots
     // allocated for the strip kernel's grid (h->grid x P1_WARPS)
-    int gc = h->nsm * p1c_blocks_per_sm(h->sc.cvcard);
+    int gc = (h->nsm - h->p1_reserve) * p1c_blocks_per_sm(h->sc.cvcard);
     if (gc < 1) return fail(h, C2_ERR_CUDA, "phase-1 kernel does not fit on an SM");
     gc = std::min(gc, h->grid * P1_WARPS / P1C_WARPS);
     CK(launch_p1(a, h->d_qbkg.p, P1K_CHUNKED, gc, h->stream));
@@ -2162,6 +2164,8 @@ static c2_profiles query_view(const c2_profiles* qs, int k, const int64_t* zero)
     return v;
 }
 
+constexpr int BATCH_RESERVE_DIV = 18;   // SMs left free by phase 1 in a multi-worker batch: nsm / 18
+
 static c2_status batch_workers(c2_handle* h, int nw)
 {
     // workers made for an earlier database are remade
@@ -2188,10 +2192,25 @@ static c2_status batch_workers(c2_handle* h, int nw)
         }
         h->workers.push_back(w);
     }
+    // with more than one worker, a query's phase 2 (latency-bound strip
+    // sweeps, host round trips) runs beside the next query's phase 1, whose
+    // persistent grid leaves a few SMs free for it
+    const int reserve = nw <= 1 ? 0
+                        : h->batch_reserve >= 0 ? std::min(h->batch_reserve, h->nsm - 1)
+                                                : std::max(1, h->nsm / BATCH_RESERVE_DIV);
+    h->p1_reserve = reserve;
     for (c2_handle* w : h->workers) {
         w->score_mode = h->score_mode;
         w->spin = h->spin;
+        w->p1_reserve = reserve;
     }
+    return C2_OK;
+}
+
+extern "C" c2_status c2_set_batch_sm_reserve(c2_handle* h, int32_t nsm)
+{
+    if (!h) return C2_ERR_ARG;
+    h->batch_reserve = nsm < 0 ? -1 : nsm;
     return C2_OK;
 }
 
@@ -2209,7 +2228,7 @@ extern "C" c2_status c2_search_batch(c2_handle* h, const c2_profiles* queries, i
     for (int i = 0; i < nw - 1; i++) ws.push_back(h->workers[i]);
     std::atomic<int> next(0);
     std::mutex mu;       // serialises the callbacks and the first error
-    std::mutex gpu_mu;   // one query's kernel sequence at a time (see below)
+    std::mutex p1_mu;    // one query's phase 1 at a time (see below)
     c2_status first = C2_OK;
     std::string first_err;
     auto run = [&](c2_handle* w) {
@@ -2222,16 +2241,18 @@ extern "C" c2_status c2_search_batch(c2_handle* h, const c2_profiles* queries, i
             const c2_profiles v = query_view(queries, q, &zero);
             int32_t nh = 0;
             size_t nb = 0;
-            // The query's host-side preparation, and below its hit copy and
-            // callback, overlap other workers; its kernels run alone: the
-            // phase-1 kernels hold every SM with one persistent CTA, and a
-            // strip-pipelined phase-2 sweep started beside them would run on
-            // the few SMs left and stall its own chains.
+            // The query's host-side preparation, its phase 2 and its hit copy
+            // and callback overlap other workers; phase 1 runs one query at a
+            // time (its persistent grid holds every SM but the few reserved
+            // for the phase-2 sweeps of the query before).
             c2_status s = c2_set_query(w, &v);
             if (s == C2_OK) {
-                std::lock_guard<std::mutex> g(gpu_mu);
+                std::lock_guard<std::mutex> g(p1_mu);
+                s = c2_run_phase1(w);
+                if (s == C2_OK && cudaStreamSynchronize(w->stream) != cudaSuccess) s = C2_ERR_CUDA;
+            }
+            if (s == C2_OK) {
                 int32_t n = 0;
-                if (s == C2_OK) s = c2_run_phase1(w);
                 if (s == C2_OK) s = c2_run_finalize(w, &n);
                 if (s == C2_OK) s = c2_run_stats(w, &n);
                 if (s == C2_OK) s = c2_run_map(w, &nh);
@@ -2259,6 +2280,7 @@ extern "C" c2_status c2_search_batch(c2_handle* h, const c2_profiles* queries, i
     for (int i = 1; i < nw; i++) th.emplace_back(run, ws[i]);
     run(ws[0]);
     for (auto& t : th) t.join();
+    h->p1_reserve = 0;   // the handle's own searches use every SM again
     if (first != C2_OK) return fail(h, first, "search_batch: %s", first_err.c_str());
     return C2_OK;
 }

@@ -30,7 +30,7 @@ EXPORTS = [
     "c2_db2bin_info", "c2_db2bin_read", "c2_share_db", "c2_search_batch", "c2_format_report",
     "c2_set_wait_limit", "c2_get_pair_scores", "c2_db2bin_descriptions", "c2_set_device_memory_limit",
     "c2_db2bin_lengths", "c2_db2bin_read_range", "c2_get_device_memory_info", "c2_db_device_bytes",
-    "c2_logz_fwd_batch", "c2_set_query_batch",
+    "c2_logz_fwd_batch", "c2_set_query_batch", "c2_set_batch_sm_reserve",
     "c2_get_device_memory_use", "c2_get_search_groups",
 ]
 
@@ -207,6 +207,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.c2_logz_fwd.argtypes = [C.c_void_p, _i32p, C.c_int32, _fp, C.c_float, C.c_float, _fp]
     lib.c2_logz_bwd.argtypes = [C.c_void_p, _fp]
     lib.c2_set_query_batch.argtypes = [C.c_void_p, P(c2_profiles)]
+    lib.c2_set_batch_sm_reserve.argtypes = [C.c_void_p, C.c_int32]
     lib.c2_logz_fwd_batch.argtypes = [C.c_void_p, _i32p, _i32p, C.c_int32, _fp, C.c_float, C.c_float, _fp]
     lib.c2_logz_cells.argtypes = [C.c_void_p, C.c_int32, _fp, _fp]
     lib.c2_db2bin_info.argtypes = [C.c_char_p, _i32p, _i64p, C.c_char_p, C.c_size_t]
@@ -523,7 +524,7 @@ class Handle:
         self.Lq = int(q.lengths[0])
         return self.hits_arrays(n.value) if arrays else self.hits(n.value)
 
-    def search_batch(self, queries: ProfileSet, nworkers: int = 1):
+    def search_batch(self, queries: ProfileSet, nworkers: int = 2):
         """Search every profile of queries over the uploaded database with nworkers
         worker handles sharing it (c2_search_batch).  Returns one (records,
         alignments) pair per query, as hits_arrays() gives them."""
@@ -549,6 +550,10 @@ class Handle:
         if errs:
             raise C2Error("c2_search_batch: queries failed: %s" % errs)
         return out
+
+    def set_batch_sm_reserve(self, nsm: int):
+        """SMs phase 1 leaves to phase 2 in a multi-worker search_batch (-1: default)."""
+        self._ck(self.lib.c2_set_batch_sm_reserve(self._h, int(nsm)), "c2_set_batch_sm_reserve")
 
     def share_db(self, src: "Handle"):
         """Search the database uploaded to src from this handle as well (c2_share_db)."""

@@ -218,8 +218,16 @@ typedef void (*c2_batch_cb)(void* user, int32_t query, c2_status status, const c
  * and CUDA stream each; cb receives each query's results as it completes
  * (serialised, from the worker threads).  Replaces the query loop of the
  * reference's JobDispatcher and DevCommThread
- * (src/libmycu/cualn/JobDispatcher.cpp:967-1213, DevCommThread.cpp:155-356). */
+ * (src/libmycu/cualn/JobDispatcher.cpp:967-1213, DevCommThread.cpp:155-356).
+ * Phase 1 runs one query at a time; with two or more workers a query's
+ * phase 2 runs beside the next query's phase 1, whose grid then leaves some
+ * SMs free (c2_set_batch_sm_reserve; default nsm / 18, 8 on a B200).  Two
+ * workers are the fastest on the 64-query configuration. */
 c2_status c2_search_batch(c2_handle* h, const c2_profiles* queries, int32_t nworkers, c2_batch_cb cb, void* user);
+
+/* SMs the phase-1 kernels of a multi-worker c2_search_batch leave to the
+ * phase-2 sweeps running beside them (-1: the default, nsm / 18). */
+c2_status c2_set_batch_sm_reserve(c2_handle* h, int32_t nsm);
 
 /* Result files in the reference's formats (-f 0 Plain, -f 1 JSON): the
  * writers' inputs besides the hits, as the comer program has them. */
