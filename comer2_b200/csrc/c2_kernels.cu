@@ -1169,6 +1169,12 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
     tmem_fence_after();
     const unsigned tq = tmem_base + ((unsigned)(32 * (wid & 3)) << 16) + (unsigned)((wid >> 2) * 128);
     unsigned tph = 0;   // phase parity of the tile slot's barrier
+    // a tile wait that gave up: the warp issues no further tile copies and
+    // waits for none, and before it exits waits (bounded) once more for the
+    // copy it gave up on, so that no copy into this CTA's shared memory is in
+    // flight when the CTA ends
+    bool tbroken = false;
+    unsigned tpend = 0;
 
     const long long slotw = (long long)blockIdx.x * P1T_WARPS + wid;
     const int Lmax = (int)(a.botstride / 10);
@@ -1296,7 +1302,7 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
             // tile T + 1 loads while tile T's products and epilogue run (and
             // the first tile of a chunk during the DP stage before it)
             const int ntile = 4 * nch;
-            if (lane == 0) bulk_load(btile, tb0, TC_TILE_WORDS * 4, tbar);
+            if (lane == 0 && !tbroken) bulk_load(btile, tb0, TC_TILE_WORDS * 4, tbar);
             for (int m = 0; 32 * m < kend; m++) {
                 if (m < nch) {
                     cp_async_wait_1();   // column records of chunk m have landed
@@ -1315,9 +1321,12 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
 #pragma unroll 2
                     for (int nt = 0; nt < 4; nt++) {
                         const int T = 4 * m + nt;
-                        const bool got = mbar_wait(tbar, tph);
+                        if (!tbroken && !__all_sync(FULL, mbar_wait(tbar, tph))) {
+                            tbroken = true;
+                            tpend = tph;
+                            if (lane == 0 && a.status) atomicCAS(a.status, 0, PIPE_ERR_TIMEOUT);
+                        }
                         tph ^= 1u;
-                        if (!got && lane == 0 && a.status) atomicCAS(a.status, 0, PIPE_ERR_TIMEOUT);
                         const unsigned* bt = btile + lane * 2;
                         uint2 B[3][2][2];
 #pragma unroll
@@ -1329,7 +1338,7 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
                                     B[d][kt][sp] = *reinterpret_cast<const uint2*>(bt + ((d * 2 + kt) * 2 + sp) * 64);
                         // slot free once every lane holds its fragments: tile T + 1 into it
                         __syncwarp();
-                        if (lane == 0 && T + 1 < ntile) {
+                        if (lane == 0 && T + 1 < ntile && !tbroken) {
                             // the warp's reads of the slot before the async-proxy write
                             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                             bulk_load(btile, tb0 + (long long)(T + 1) * TC_TILE_WORDS, TC_TILE_WORDS * 4, tbar);
@@ -1439,6 +1448,7 @@ p1t_kernel(P1Args a, const float* __restrict__ qbkg)
         }
         __syncwarp();
     }
+    if (tbroken) (void)mbar_wait(tbar, tpend);
     // every warp is past its last TMEM access: the allocating warp frees it
     tmem_fence_before();
     __syncthreads();
