@@ -23,6 +23,8 @@ namespace c2 {
 
 // columns of the row above a strip loaded (and waited for) at a time
 constexpr int MAP_RG = 8;
+// steps of F + B loaded ahead by the MAP DP sweep
+constexpr int MAPDP_Q = 4;
 
 
 #define FULL 0xffffffffu
@@ -627,52 +629,68 @@ __global__ void __launch_bounds__(MAPW * 32, 8) map_dp_kernel(MapArgs a)
             pf_line(fs, 32 + lane, W);
             pf_line(bs, lane, W);
             pf_line(bs, 32 + lane, W);
-            float nfb = fs[lane] + bs[lane];
-            for (int k = 0; k < W; k++) {
-                const float fbk = nfb;   // F + B of this step's cell
-                if (k + 1 < W) nfb = fs[(long long)(k + 1) * 32 + lane] + bs[(long long)(k + 1) * 32 + lane];
-                float up = __shfl_up_sync(FULL, mine, 1);
-                {
-                    const int src = k & 31;
-                    const float b0 = __shfl_sync(FULL, bcur, src);
-                    if (lane == 0) up = b0;
-                    if ((src & (MAP_RG - 1)) == MAP_RG - 1) {
-                        if (s > 0 && k + 1 < L)
-                            pipe_wait(pf + s - 1, min(k + 1 + MAP_RG, L), lane, a.status, broken, a.spin);
-                        const int d = (lane - (k + 1)) & 31;
-                        if (d < MAP_RG) bcur = (s > 0 && k + 1 + d < L) ? __ldcg(botr + k + 1 + d) : 0.f;
+            // F and B of step k + MAPDP_Q are loaded at step k (a queue of
+            // MAPDP_Q steps in registers, the step loop unrolled by MAPDP_Q so
+            // that every queue slot is a fixed register)
+            float qf[MAPDP_Q], qb[MAPDP_Q];
+#pragma unroll
+            for (int u = 0; u < MAPDP_Q; u++) {
+                qf[u] = (u < W) ? fs[(long long)u * 32 + lane] : 0.f;
+                qb[u] = (u < W) ? bs[(long long)u * 32 + lane] : 0.f;
+            }
+            for (int k0 = 0; k0 < W; k0 += MAPDP_Q) {
+#pragma unroll
+                for (int u = 0; u < MAPDP_Q; u++) {
+                    const int k = k0 + u;
+                    if (k >= W) break;
+                    const float fbk = qf[u] + qb[u];   // F + B of this step's cell
+                    if (k + MAPDP_Q < W) {
+                        qf[u] = fs[(long long)(k + MAPDP_Q) * 32 + lane];
+                        qb[u] = bs[(long long)(k + MAPDP_Q) * 32 + lane];
                     }
-                    if (src == 31) {
-                        pf_line(fs, k + 33 + lane, W);
-                        pf_line(bs, k + 33 + lane, W);
+                    float up = __shfl_up_sync(FULL, mine, 1);
+                    {
+                        const int src = k & 31;
+                        const float b0 = __shfl_sync(FULL, bcur, src);
+                        if (lane == 0) up = b0;
+                        if ((src & (MAP_RG - 1)) == MAP_RG - 1) {
+                            if (s > 0 && k + 1 < L)
+                                pipe_wait(pf + s - 1, min(k + 1 + MAP_RG, L), lane, a.status, broken, a.spin);
+                            const int d = (lane - (k + 1)) & 31;
+                            if (d < MAP_RG) bcur = (s > 0 && k + 1 + d < L) ? __ldcg(botr + k + 1 + d) : 0.f;
+                        }
+                        if (src == 31) {
+                            pf_line(fs, k + 33 + lane, W);
+                            pf_line(bs, k + 33 + lane, W);
+                        }
                     }
+                    __syncwarp();
+                    const int j = k - lane;
+                    float left = mine, diag = upp;
+                    if (j == 0) { left = 0.f; diag = 0.f; }
+                    const bool valid = act && j >= 0 && j < L;
+                    float v = 0.f;
+                    int b = BT_STOP;
+                    if (j >= 0 && j < L) {
+                        const bool crn = (Lq <= r + edge && j <= edge + r - Lq) || (L - edge + r <= j && r < edge);
+                        const float fbv = (!act || crn) ? 0.f : fbk;
+                        v = (diag + fexp(fbv - logZ)) - a.minpp;
+                        if (v > 0.f) b = BT_DIAG; else v = 0.f;
+                        if (valid && v > best) { best = v; brow = r; bcol = j; }
+                        if (v < up - gap) { v = up - gap; b = BT_UP; }
+                        if (v < left - gap) { v = left - gap; b = BT_LEFT; }
+                    }
+                    if (valid) bout[j & 31][lane] = (signed char)b;
+                    if (wr_bot && j >= 0 && j < L) {
+                        botw[j] = v;
+                        pipe_publish(pf + s, j, L);
+                    }
+                    mine = v;
+                    upp = up;
+                    const int cfl = k - 31;
+                    if (cfl >= 0 && cfl < L && act) bt[(long long)cfl * Lq + r] = bout[cfl & 31][lane];
+                    __syncwarp();
                 }
-                __syncwarp();
-                const int j = k - lane;
-                float left = mine, diag = upp;
-                if (j == 0) { left = 0.f; diag = 0.f; }
-                const bool valid = act && j >= 0 && j < L;
-                float v = 0.f;
-                int b = BT_STOP;
-                if (j >= 0 && j < L) {
-                    const bool crn = (Lq <= r + edge && j <= edge + r - Lq) || (L - edge + r <= j && r < edge);
-                    const float fbv = (!act || crn) ? 0.f : fbk;
-                    v = (diag + fexp(fbv - logZ)) - a.minpp;
-                    if (v > 0.f) b = BT_DIAG; else v = 0.f;
-                    if (valid && v > best) { best = v; brow = r; bcol = j; }
-                    if (v < up - gap) { v = up - gap; b = BT_UP; }
-                    if (v < left - gap) { v = left - gap; b = BT_LEFT; }
-                }
-                if (valid) bout[j & 31][lane] = (signed char)b;
-                if (wr_bot && j >= 0 && j < L) {
-                    botw[j] = v;
-                    pipe_publish(pf + s, j, L);
-                }
-                mine = v;
-                upp = up;
-                const int cfl = k - 31;
-                if (cfl >= 0 && cfl < L && act) bt[(long long)cfl * Lq + r] = bout[cfl & 31][lane];
-                __syncwarp();
             }
         }
 #pragma unroll
