@@ -1085,6 +1085,18 @@ extern "C" c2_status c2_get_device_memory_use(const c2_handle* h, uint64_t* byte
     return C2_OK;
 }
 
+extern "C" c2_status c2_get_device_count(int32_t* count)
+{
+    if (!count) return C2_ERR_ARG;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        (void)cudaGetLastError();
+        n = 0;
+    }
+    *count = n;
+    return C2_OK;
+}
+
 extern "C" c2_status c2_get_device_memory_info(const c2_handle* h, uint64_t* free_bytes, uint64_t* total_bytes)
 {
     if (!h || !free_bytes || !total_bytes) return C2_ERR_ARG;

@@ -19,12 +19,14 @@
 // the context-vector score map and the SS18 model weights of the reference's
 // install come from comer2_params.json beside the library (or the file named
 // by COMER2_PARAMS); the options file (-p, the format of src/env/options.txt)
-// overrides the option values.  --dev-N selects the GPU (the first of a list;
-// the search runs on one GPU), --dev-mem bounds the device memory the search
-// may use (c2_set_device_memory_limit).  A database that does not fit in half
-// of that memory (or of the device's free memory) is searched in chunks of
-// consecutive profiles, each read from file while the previous one is
-// searched, as the reference's reader feeds its device in portions; the
+// overrides the option values.  --dev-N selects the GPUs (a count or a list),
+// --dev-mem bounds the device memory the search may use on each
+// (c2_set_device_memory_limit).  A database that does not fit in half
+// of that memory (or of the device's free memory), or that is spread over
+// several GPUs, is searched in chunks of consecutive profiles, as the
+// reference's reader feeds its devices in portions: the chunks go round-robin
+// to the GPUs, and a GPU with more than one chunk holds two handles, the next
+// chunk read from file and uploaded on one while the other is searched.  The
 // results are those of a single search.  The reference's other --dev-* and
 // --io-* options are accepted and have no effect here.
 #include <sys/stat.h>
@@ -42,6 +44,9 @@
 #include <functional>
 #include <future>
 #include <map>
+#include <exception>
+#include <thread>
+#include <mutex>
 #include <memory>
 #include <sstream>
 #include <stdexcept>
@@ -722,7 +727,8 @@ void usage(FILE* f, const char* prog)
             "-o <output_directory>       Directory of output files for each query.\n"
             "-f <file_format>            Format of output files: 0, Plain; 1, JSON.  Default=0\n"
             "-p <options_file>           Input file of options (the format of options.txt).\n"
-            "--dev-N=(<number>|,<id_list>) GPU to use (the first of a list).  Default=1\n"
+            "--dev-N=(<number>|,<id_list>) GPUs to use: a number, or a list starting with a comma;\n"
+            "                            the database is split across them.  Default=1\n"
             "--dev-mem=<megabytes>       Maximum amount of GPU memory the search may use.\n"
             "-v [<level_number>]         Verbose mode.\n"
             "-h                          This text.\n",
@@ -733,7 +739,7 @@ struct Args {
     std::string query, dbs, outdir = ".", options;
     bool print_inputs = false;   // print the parsed parameters and profiles, search nothing
     int format = 0;
-    int device = 0;
+    std::vector<int> devices{0};   // --dev-N: GPUs to search on
     long long devmem_mb = 0;
 };
 
@@ -763,8 +769,20 @@ Args parse_args(int argc, char** argv)
             a.print_inputs = true;
         } else if (s.rfind("--dev-N=", 0) == 0) {
             const std::string v = s.substr(8);
-            // ",<id>,<id>...": the first listed GPU; "<n>": the first GPU
-            a.device = (!v.empty() && v[0] == ',') ? atoi(v.c_str() + 1) : 0;
+            // ",<id>,<id>...": the listed GPUs; "<n>": GPUs 0 .. n-1 (at most
+            // as many as there are)
+            a.devices.clear();
+            if (!v.empty() && v[0] == ',') {
+                std::stringstream ds(v.substr(1));
+                for (std::string id; std::getline(ds, id, ',');)
+                    if (!id.empty()) a.devices.push_back(atoi(id.c_str()));
+            } else {
+                int32_t have = 0;
+                c2_get_device_count(&have);
+                const int n = std::max(1, std::min(atoi(v.c_str()), std::max(1, (int)have)));
+                for (int d = 0; d < n; d++) a.devices.push_back(d);
+            }
+            if (a.devices.empty()) die("--dev-N: no GPU given");
         } else if (s.rfind("--dev-mem=", 0) == 0) {
             a.devmem_mb = atoll(s.c_str() + 10);
         } else if (s.rfind("--dev-", 0) == 0 || s.rfind("--io-", 0) == 0) {
@@ -868,18 +886,28 @@ int run(int argc, char** argv)
     }
     note(1, "queries: " + std::to_string(Q.nprof()) + "; database: " + std::to_string(totP) + " profiles, " +
                 std::to_string(totN) + " positions");
-    c2_handle* h = nullptr;
-    c2_status st = c2_create(A.device, &P.p, &h);
-    if (st != C2_OK) die("c2_create failed (status " + std::to_string((int)st) + "): check the options (MAPALN 0 or 1, SSEMODEL 0..2, SS and CV weights >= 0)");
+    // Device memory (per GPU): the --dev-mem limit, or what is free on the
+    // device.  Half of what a handle does not hold yet goes to its database
+    // chunk, the rest to the query and the phase-2 scratch (split into
+    // candidate groups under the limit).  A database in more than one chunk
+    // per GPU is double-buffered: two handles per GPU, each with half of the
+    // memory, the next chunk read and uploaded on one while the other is
+    // searched.  With several GPUs the chunks go round-robin to the GPUs.
+    const int ndev = (int)A.devices.size();
+    auto make_handle = [&](int dev, uint64_t lim) {
+        c2_handle* hh = nullptr;
+        const c2_status st = c2_create(dev, &P.p, &hh);
+        if (st != C2_OK)
+            die("c2_create on GPU " + std::to_string(dev) + " failed (status " + std::to_string((int)st) +
+                "): check the GPU and the options (MAPALN 0 or 1, SSEMODEL 0..2, SS and CV weights >= 0)");
+        if (A.devmem_mb > 0) ck(hh, c2_set_device_memory_limit(hh, lim), "c2_set_device_memory_limit");
+        return hh;
+    };
+    c2_handle* h = make_handle(A.devices[0], (uint64_t)A.devmem_mb << 20);
     std::unique_ptr<c2_handle, c2_status (*)(c2_handle*)> guard(h, c2_destroy);
-    // device memory: the --dev-mem limit, or what is free on the device; half
-    // of what the handle does not hold yet goes to the database chunk, the
-    // rest to the query and the phase-2 scratch (split into candidate groups
-    // under the limit)
     uint64_t limit = 0, used0 = 0;
     if (A.devmem_mb > 0) {
         limit = (uint64_t)A.devmem_mb << 20;
-        ck(h, c2_set_device_memory_limit(h, limit), "c2_set_device_memory_limit");
     } else {
         uint64_t fr = 0, tot = 0;
         ck(h, c2_get_device_memory_info(h, &fr, &tot), "c2_get_device_memory_info");
@@ -887,8 +915,25 @@ int run(int argc, char** argv)
     }
     ck(h, c2_get_device_memory_use(h, &used0), "c2_get_device_memory_use");
     if (limit <= used0) die("--dev-mem: the limit is below the memory the search's tables need");
-    const std::vector<Chunk> chunks = plan_chunks(h, F, (limit - used0) / 2);
-    note(1, "database in " + std::to_string(chunks.size()) + " chunk(s)");
+    std::vector<Chunk> chunks = plan_chunks(h, F, (limit - used0) / 2);
+    bool dbuf = false;   // two handles per GPU
+    if (chunks.size() > 1 || ndev > 1) {
+        if (limit / 2 <= used0) die("--dev-mem: the limit is below the memory two searches' tables need");
+        uint64_t cap = (limit / 2 - used0) / 2;
+        if (ndev > 1) {
+            // at least one chunk per GPU
+            int32_t lmax = 0;
+            for (const auto& f : F)
+                for (int32_t L : f.lengths) lmax = std::max(lmax, L);
+            uint64_t all = 0;
+            ck(h, c2_db_device_bytes(h, totN, (int32_t)totP, lmax, &all), "c2_db_device_bytes");
+            cap = std::min<uint64_t>(cap, all / (uint64_t)ndev + 1);
+        }
+        chunks = plan_chunks(h, F, cap);
+        dbuf = chunks.size() > (size_t)ndev;
+        if (dbuf && A.devmem_mb > 0) ck(h, c2_set_device_memory_limit(h, limit / 2), "c2_set_device_memory_limit");
+    }
+    note(1, "database in " + std::to_string(chunks.size()) + " chunk(s) on " + std::to_string(ndev) + " GPU(s)");
     mkdirs(A.outdir);
     std::string qbase = base_name(qi);
     {
@@ -905,6 +950,7 @@ int run(int argc, char** argv)
         float thld = 0.f, logevthld = 0.f;
     };
     std::vector<QueryHits> acc(Q.nprof());
+    std::mutex acc_mu;
     std::vector<const char*> dbn;
     for (const auto& f : F) dbn.push_back(f.name.c_str());
     std::vector<std::string> desc_all;
@@ -917,31 +963,40 @@ int run(int argc, char** argv)
     }
     std::vector<Profiles> queries;
     for (int qn = 0; qn < Q.nprof(); qn++) queries.push_back(Q.one(qn));
-    // chunk c + 1 is read from file while chunk c is searched
-    std::future<Profiles> next = std::async(std::launch::async, read_chunk, std::cref(F), std::cref(chunks[0]));
-    for (size_t c = 0; c < chunks.size(); c++) {
-        const Profiles D = next.get();
-        if (c + 1 < chunks.size())
-            next = std::async(std::launch::async, read_chunk, std::cref(F), std::cref(chunks[c + 1]));
-        const int64_t gb = chunks[c].gbase;
+    // read a chunk from file and upload it to handle hh (with the totals of
+    // all databases)
+    auto load = [&](size_t ci, c2_handle* hh) {
+        const Profiles D = read_chunk(F, chunks[ci]);
+        const int64_t gb = chunks[ci].gbase;
         for (int k = 0; k < D.nprof(); k++) {
             eno_all[(size_t)(gb + k)] = D.eno[k];
             ss_all[(size_t)(gb + k)] = D.has_ss[k];
         }
         const c2_profiles dv = D.view();
-        ck(h, c2_upload_db(h, &dv, (uint64_t)totN, (uint64_t)totP), "c2_upload_db");
+        ck(hh, c2_upload_db(hh, &dv, (uint64_t)totN, (uint64_t)totP), "c2_upload_db");
+    };
+    // every query against the chunk uploaded to hh; hits into acc
+    auto search_chunk = [&](size_t ci, c2_handle* hh) {
+        const int64_t gb = chunks[ci].gbase;
         for (int qn = 0; qn < Q.nprof(); qn++) {
             const c2_profiles qv = queries[qn].view();
             int32_t nh = 0;
-            ck(h, c2_search(h, &qv, &nh), "c2_search");
+            ck(hh, c2_search(hh, &qv, &nh), "c2_search");
             size_t abytes = 0;
-            ck(h, c2_get_hits(h, nullptr, 0, nullptr, &abytes), "c2_get_hits");
+            ck(hh, c2_get_hits(hh, nullptr, 0, nullptr, &abytes), "c2_get_hits");
             std::vector<c2_hit> hits((size_t)std::max(nh, 1));
             std::vector<char> alns(abytes + 1);
-            ck(h, c2_get_hits(h, hits.data(), nh, alns.data(), &abytes), "c2_get_hits");
+            ck(hh, c2_get_hits(hh, hits.data(), nh, alns.data(), &abytes), "c2_get_hits");
+            uint64_t sspace = 0, dlen = 0;
+            float thld = 0.f, logevthld = 0.f;
+            ck(hh, c2_get_search_space(hh, &sspace, &dlen), "c2_get_search_space");
+            ck(hh, c2_get_thresholds(hh, &thld, &logevthld), "c2_get_thresholds");
+            std::lock_guard<std::mutex> lk(acc_mu);
             QueryHits& a = acc[qn];
-            ck(h, c2_get_search_space(h, &a.sspace, &a.dlen), "c2_get_search_space");
-            ck(h, c2_get_thresholds(h, &a.thld, &a.logevthld), "c2_get_thresholds");
+            a.sspace = sspace;
+            a.dlen = dlen;
+            a.thld = thld;
+            a.logevthld = logevthld;
             const int64_t base = (int64_t)a.alns.size();
             for (int i = 0; i < nh; i++) {
                 hits[i].profile += (int32_t)gb;
@@ -950,9 +1005,62 @@ int run(int argc, char** argv)
             }
             a.alns.insert(a.alns.end(), alns.begin(), alns.begin() + (long)abytes);
         }
-        if (chunks.size() > 1)
-            note(2, "chunk " + std::to_string(c + 1) + "/" + std::to_string(chunks.size()) + ": " +
-                        std::to_string(D.nprof()) + " profiles searched");
+        note(2, "chunk " + std::to_string(ci + 1) + "/" + std::to_string(chunks.size()) + " searched");
+    };
+    // one worker per GPU over its chunks (ci = w, w + ndev, ...)
+    auto worker = [&](int w) {
+        std::vector<size_t> mine;
+        for (size_t ci = (size_t)w; ci < chunks.size(); ci += (size_t)ndev) mine.push_back(ci);
+        if (mine.empty()) return;
+        const uint64_t lim = dbuf ? limit / 2 : limit;
+        std::unique_ptr<c2_handle, c2_status (*)(c2_handle*)> h0(w == 0 ? nullptr : make_handle(A.devices[w], lim),
+                                                                 c2_destroy);
+        std::unique_ptr<c2_handle, c2_status (*)(c2_handle*)> h1(mine.size() > 1 ? make_handle(A.devices[w], lim)
+                                                                                 : nullptr,
+                                                                 c2_destroy);
+        c2_handle* H[2] = {w == 0 ? h : h0.get(), h1.get()};
+        load(mine[0], H[0]);
+        for (size_t i = 0; i < mine.size(); i++) {
+            std::exception_ptr up_err;
+            std::thread up;
+            if (i + 1 < mine.size())
+                up = std::thread([&, i]() {
+                    try {
+                        load(mine[i + 1], H[(i + 1) & 1]);
+                    } catch (...) {
+                        up_err = std::current_exception();
+                    }
+                });
+            std::exception_ptr err;
+            try {
+                search_chunk(mine[i], H[i & 1]);
+            } catch (...) {
+                err = std::current_exception();
+            }
+            if (up.joinable()) up.join();
+            if (err) std::rethrow_exception(err);
+            if (up_err) std::rethrow_exception(up_err);
+        }
+    };
+    {
+        std::vector<std::exception_ptr> errs(ndev);
+        std::vector<std::thread> th;
+        for (int w = 1; w < ndev; w++)
+            th.emplace_back([&, w]() {
+                try {
+                    worker(w);
+                } catch (...) {
+                    errs[w] = std::current_exception();
+                }
+            });
+        try {
+            worker(0);
+        } catch (...) {
+            errs[0] = std::current_exception();
+        }
+        for (auto& t : th) t.join();
+        for (auto& e : errs)
+            if (e) std::rethrow_exception(e);
     }
     std::vector<const char*> ddesc;
     for (const auto& s : desc_all) ddesc.push_back(s.c_str());

@@ -30,7 +30,7 @@ EXPORTS = [
     "c2_db2bin_info", "c2_db2bin_read", "c2_share_db", "c2_search_batch", "c2_format_report",
     "c2_set_wait_limit", "c2_get_pair_scores", "c2_db2bin_descriptions", "c2_set_device_memory_limit",
     "c2_db2bin_lengths", "c2_db2bin_read_range", "c2_get_device_memory_info", "c2_db_device_bytes",
-    "c2_logz_fwd_batch", "c2_set_query_batch", "c2_set_batch_sm_reserve",
+    "c2_logz_fwd_batch", "c2_set_query_batch", "c2_set_batch_sm_reserve", "c2_get_device_count",
     "c2_get_device_memory_use", "c2_get_search_groups",
 ]
 
@@ -208,6 +208,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.c2_logz_bwd.argtypes = [C.c_void_p, _fp]
     lib.c2_set_query_batch.argtypes = [C.c_void_p, P(c2_profiles)]
     lib.c2_set_batch_sm_reserve.argtypes = [C.c_void_p, C.c_int32]
+    lib.c2_get_device_count.argtypes = [_i32p]
     lib.c2_logz_fwd_batch.argtypes = [C.c_void_p, _i32p, _i32p, C.c_int32, _fp, C.c_float, C.c_float, _fp]
     lib.c2_logz_cells.argtypes = [C.c_void_p, C.c_int32, _fp, _fp]
     lib.c2_db2bin_info.argtypes = [C.c_char_p, _i32p, _i64p, C.c_char_p, C.c_size_t]

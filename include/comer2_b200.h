@@ -294,6 +294,10 @@ c2_status c2_set_device_memory_limit(c2_handle* h, uint64_t bytes);
 /* Device memory the handle's buffers hold now, in bytes. */
 c2_status c2_get_device_memory_use(const c2_handle* h, uint64_t* bytes);
 
+/* Number of CUDA devices (0 when none is usable): the reference's --dev-N
+ * option uses up to that many (src/comer/comer.h:50-57, comer.cpp:192-194). */
+c2_status c2_get_device_count(int32_t* count);
+
 /* Free and total memory of the handle's device (cudaMemGetInfo). */
 c2_status c2_get_device_memory_info(const c2_handle* h, uint64_t* free_bytes, uint64_t* total_bytes);
 

@@ -95,23 +95,31 @@ def _makedb(tmp, name, ps, ks):
 
 @needs_ref
 def test_program_in_database_chunks_writes_the_same_files(tmp_path, params):
-    """A --dev-mem limit that holds about a third of the two databases at a
-    time: the program searches them in chunks (pieces of both files), each
-    uploaded with the totals of both, and writes the same result files, byte
-    for byte, as the search of the whole."""
+    """The same queries against two databases (4,000 short profiles, a few
+    homologs planted) three ways: whole on one GPU; under a --dev-mem limit
+    that splits them into chunks spanning both files, double-buffered (the
+    next chunk uploaded on a second handle while the current one is
+    searched); and split across two GPU workers (--dev-N=,0,0, both on GPU
+    0 here).  Every chunk is uploaded with the totals of both databases, so
+    the result files are the same byte for byte."""
     from comer2_b200 import build as B
     from comer2_b200.native import Handle, read_db2bin
     rng = np.random.default_rng(32)
-    w = S.config(1, seed=7, scale=0.0015)
-    q2 = S.random_profiles(rng, [150])
-    n = w.db.nprofiles
-    dbs = [_makedb(tmp_path, "da", w.db, range(0, n // 2)), _makedb(tmp_path, "db", w.db, range(n // 2, n))]
+    q0 = S.random_profiles(rng, [110])
+    q1 = S.random_profiles(rng, [90])
+    hom = [S.planted_homolog(rng, q0, int(L), seg_lo=25, seg_hi=40) for L in (45, 52, 60)]
+    db = S.concat([S.random_profiles(rng, list(rng.integers(30, 61, 1997)))] + hom +
+                  [S.random_profiles(rng, list(rng.integers(30, 61, 2000)))])
+    n = db.nprofiles
+    dbs = [_makedb(tmp_path, "da", db, range(0, n // 2)), _makedb(tmp_path, "db", db, range(n // 2, n))]
     qf = tmp_path / "two.pro"
     with open(qf, "w") as fh:
-        textfmt.write_profile(fh, w.queries[0], 0, "q0", "first query")
-        textfmt.write_profile(fh, q2, 0, "q1", "second query")
-    # the limit: the handle's own tables, plus twice a chunk of a third of
-    # the positions (half of what remains goes to the chunk)
+        textfmt.write_profile(fh, q0, 0, "q0", "first query")
+        textfmt.write_profile(fh, q1, 0, "q1", "second query")
+    # the program's chunk plan: one handle's database bytes within half of
+    # what it does not hold, two handles per GPU (each half the limit) once
+    # there is more than one chunk; the limit is set for chunks of about a
+    # quarter of the positions
     D = [read_db2bin(d + ".bin") for d in dbs]
     N = sum(int(x.lengths.sum()) for x in D)
     P = sum(x.nprofiles for x in D)
@@ -121,19 +129,22 @@ def test_program_in_database_chunks_writes_the_same_files(tmp_path, params):
     fixed = h.db_device_bytes(0, 0, lmax)
     whole = h.db_device_bytes(N, P, lmax)
     h.close()
-    cap = fixed + (whole - fixed) // 3
-    mb = -(-(used0 + 2 * cap) // 2**20)
-    outs = {}
-    for tag, extra in (("whole", []), ("chunks", ["--dev-mem=%d" % mb])):
+    cap2 = fixed + (whole - fixed) // 4
+    limit = 2 * (2 * cap2 + used0)
+    assert (limit - used0) // 2 < whole   # one handle cannot hold the whole database
+    mb = -(-limit // 2**20)
+    outs, nchunks = {}, {}
+    for tag, extra in (("whole", []), ("dbuf", ["--dev-mem=%d" % mb]), ("gpus", ["--dev-N=,0,0"])):
         out = tmp_path / tag
         for fmt in ("1", "0"):
             r = subprocess.run([B.PROG, "-i", str(qf), "-d", ",".join(dbs), "-o", str(out), "-f", fmt, "-v"] + extra,
-                               capture_output=True, text=True, timeout=300)
+                               capture_output=True, text=True, timeout=600)
             assert r.returncode == 0, r.stderr
-            nchunks = int(r.stderr.split("database in ")[1].split(" chunk")[0])
-            assert (nchunks == 1) if tag == "whole" else (3 <= nchunks <= 5), r.stderr
+            nchunks[tag] = int(r.stderr.split("database in ")[1].split(" chunk")[0])
         outs[tag] = {f: open(out / f, "rb").read() for f in sorted(os.listdir(out))}
+    assert nchunks["whole"] == 1 and 3 <= nchunks["dbuf"] <= 6 and nchunks["gpus"] >= 2, nchunks
     assert list(outs["whole"]) == ["two__0.json", "two__0.out", "two__1.json", "two__1.out"]
-    assert outs["whole"] == outs["chunks"]
+    assert outs["whole"] == outs["dbuf"]
+    assert outs["whole"] == outs["gpus"]
     doc = json.loads(outs["whole"]["two__0.json"])["comer_search"]
     assert len(doc["search_hits"]) >= 3
