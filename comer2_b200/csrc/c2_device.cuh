@@ -99,17 +99,23 @@ constexpr int P1C_RING = 64, P1C_TRS = 12, P1C_CVREP = 16;
 constexpr int BND_ND = 32 * 4, BND_FLOATS = 32 * 5;
 constexpr int P1C_WARP_FLOATS =
     P1C_RING * 32 + P1C_RING * P1C_TRS + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE + BND_FLOATS;
-// chunked traceback sweep: p1c_kernel's per-warp layout plus a [32][33]-byte
-// traceback column ring; 11 warps per SM with CV table replicas of 8
-constexpr int P1TC_WARPS = 11, P1TC_CVREP = 8;
+// traceback sweep over the stored score matrices: per warp the score ring, the
+// transition ring, the row above and a [32][33]-byte traceback column ring;
+// 16 warps per SM.  P1TC_CVREP: CV table replicas of the phase-2 score kernel
+constexpr int P1TC_WARPS = 16, P1TC_CVREP = 8;
+constexpr int P1TC_WARP_FLOATS = P1C_RING * 32 + P1C_RING * P1C_TRS + BND_FLOATS;
+// phase-2 score kernel: 8 warps per CTA, per warp the SS row table and the
+// record staging ring; the CV table (P1TC_CVREP replicas) per CTA
+constexpr int P2S_WARPS = 8;
+constexpr int P2S_WARP_FLOATS = MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE;
 
 // Largest CV maps the shared-memory layouts hold (opt-in shared memory per CTA
-// on sm_100: 227 KB): the traceback sweep, which every search runs, and the
+// on sm_100: 227 KB): the phase-2 score kernel, which every search runs, and the
 // tensor-core phase-1 kernel (whose 16 bytes of static shared memory hold the
 // TMEM address).  The reference's cvs2s map has 93 entries.
 constexpr int SMEM_CTA_MAX = 227 * 1024;
 constexpr int P1TC_MAX_CVCARD =
-    (SMEM_CTA_MAX - P1TC_WARPS * 32 * 33 - P1TC_WARPS * P1C_WARP_FLOATS * 4) / (P1TC_CVREP * 4);
+    (SMEM_CTA_MAX - P2S_WARPS * P2S_WARP_FLOATS * 4) / (P1TC_CVREP * 4);
 // tensor-core kernel: score ring of 64 anti-diagonals with 36 floats each (the
 // fragment-layout writes and the per-lane wavefront reads are both free of
 // bank conflicts), a column-record ring of 3 chunks plus a mirror of its first

@@ -1233,13 +1233,13 @@ static c2_status finalize_set(c2_handle* h, const std::vector<int>& cand, int32_
     a.worder = h->d_worder.p;
     a.items = h->d_tbitems.p;
     const long long nitems = (long long)nc * ((h->Lq + 31) / 32);
-    CK(cudaMemsetAsync(h->d_counter.p, 0, sizeof(int), h->stream));
+    CK(cudaMemsetAsync(h->d_counter.p, 0, 2 * sizeof(int), h->stream));   // the sweep's and the score kernel's
     CK(cudaMemsetAsync(h->d_prog.p, 0, (size_t)nitems * sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_tbkey.p, 0, (size_t)nc * sizeof(unsigned long long), h->stream));
     // one CTA of P1TC_WARPS warps per SM, one warp per (candidate, strip) work item at most
     const int grid = (int)std::min<long long>(h->nsm, (nitems + P1TC_WARPS - 1) / P1TC_WARPS);
-    CK(launch_p1(a, h->d_qbkg.p, P1K_TRACEBACK, grid, h->stream));
-    h->launches++;
+    CK(launch_p1(a, h->d_qbkg.p, P1K_TRACEBACK, grid, h->stream));   // p2s_kernel, then p1tc_kernel
+    h->launches += 2;
     FinArgs f;
     f.Lq = h->Lq;
     f.ncand = nc;

@@ -18,10 +18,13 @@
 //    transitions passed down the lanes the same way;
 //  * the strip's last row is handed to the next strip through a per-warp
 //    boundary buffer (global memory, L2 resident).
-// The traceback sweep (p1tc_kernel) recomputes the same DP for the pairs
-// that pass the phase-1 threshold and stores their scores and btck codes
-// column-major for the finalisation, statistics and MAP stages.
+// For the pairs that pass the phase-1 threshold, p2s_kernel stores the FP32
+// scores column-major for the finalisation, statistics and MAP stages, and the
+// traceback sweep (p1tc_kernel) runs the same DP on them again, storing btck
+// codes.
 #include <cuda_bf16.h>
+
+#include <algorithm>
 
 #include "c2_device.cuh"
 
@@ -714,29 +717,105 @@ p1c_kernel(P1Args a, const float* __restrict__ qbkg)
 // published the columns of chunk m + 1 of its last row (loaded into registers
 // during the stage) and publishes its own last row once per chunk.  The
 // arithmetic is p1c_kernel's, so the maxima equal phase 1's in the FP32 form.
-__global__ void __launch_bounds__(P1TC_WARPS * 32, 1)
-p1tc_kernel(P1Args a, const float* __restrict__ qbkg)
+// Phase-2 score matrices: the FP32 scores and modular scores of every cell of
+// the candidate pairs, column-major per pair (the layout of the finalisation,
+// statistics and MAP stages), by cell_score -- the arithmetic of phase 1's
+// FP32 form.  One warp per (candidate, strip) at a time, lanes own query rows,
+// db records staged in shared memory as in phase 1; no dependencies between
+// work items, so every resident warp works.
+__global__ void __launch_bounds__(P2S_WARPS * 32)
+p2s_kernel(P1Args a, const float* __restrict__ qbkg)
 {
     extern __shared__ float smem[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int cvcard = a.sc.cvcard;
     const int card = a.sc.ssss_card;
-    __shared__ signed char btr_all[P1TC_WARPS][32][33];
-    signed char(*btr)[33] = btr_all[wid];
     float* cvtab = smem;                                      // [cvcard][P1TC_CVREP]
-    float* wb = smem + cvcard * P1TC_CVREP + wid * P1C_WARP_FLOATS;
-    float* ring = wb;                                         // [P1C_RING][32] scores
-    float* trn = ring + P1C_RING * 32;                        // [P1C_RING][P1C_TRS] transitions
-    float* U = trn + P1C_RING * P1C_TRS;                      // [card][32]
+    float* U = smem + cvcard * P1TC_CVREP + wid * P2S_WARP_FLOATS;   // [card][32]
     float* rec = U + MAX_SSSS_CARD * 32;                      // [REC_SLOTS][DR_STRIDE] db records
-    float* bnd = rec + REC_SLOTS * DR_STRIDE;                 // [BND_FLOATS] row above the strip
     for (int i = threadIdx.x; i < cvcard * P1TC_CVREP; i += blockDim.x) cvtab[i] = a.cvvals[i / P1TC_CVREP];
     __syncthreads();
-
     const int Lq = a.Lq;
     const int nstrips = (Lq + 31) >> 5;
     const int nitems = a.nwork * nstrips;
     const ScoreConsts sc = a.sc;
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.counter + 1, 1);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= nitems) break;
+        const int cand = a.worder[item / nstrips];
+        const int s = item % nstrips;
+        const int p = a.order[cand];
+        const int L = a.plen[p];
+        const float* __restrict__ dr = a.drec + a.poff[p] * DR_STRIDE;
+        const float* __restrict__ bd = a.pbkg + (long long)p * NAA;
+        const long long coff = a.cand_off[cand];
+        float* smt = a.smat + coff;
+        float* mmt = a.mmat + coff;
+        const int r = s * 32 + lane;
+        const bool act = r < Lq;
+        const float* __restrict__ qr = a.qrec + (long long)(act ? r : Lq - 1) * QR_STRIDE;
+        RowOps R;
+#pragma unroll
+        for (int i = 0; i < NAA; i++)
+            R.Qt[i] = __fdividef(qr[QR_TRG + i], 0.5f * (qbkg[i] + bd[i]));
+#pragma unroll
+        for (int i = 0; i < NCV; i++) R.qcv[i] = qr[QR_CV + i];
+        R.cq = qr[QR_CN];
+        R.pq = qr[QR_PRIOR];
+        R.hq = qr[QR_HQ];
+        __syncwarp();
+        {
+            // this strip's SS row tables (built once per query, c2_set_query)
+            const float* __restrict__ us = a.qU + (long long)s * MAX_SSSS_CARD * 32 + lane;
+#pragma unroll 8
+            for (int c = 0; c < card; c++) U[c * 32 + lane] = __ldg(us + c * 32);
+        }
+        stage_chunk(rec, dr, 0, L, lane);
+        stage_chunk(rec, dr, 1, L, lane);
+        for (int c = 0; c < L; c++) {
+            if ((c & (REC_CHUNK - 1)) == 0) {
+                cp_async_wait_1();
+                __syncwarp();
+            }
+            const float* rc = rec + (c & (REC_SLOTS - 1)) * DR_STRIDE;
+            float mod;
+            const float Sc = cell_score<P1TC_CVREP>(R, reinterpret_cast<const float4*>(rc), U, cvtab, sc, lane, mod);
+            if (act) {
+                smt[(long long)c * Lq + r] = Sc;
+                mmt[(long long)c * Lq + r] = mod;
+            }
+            if ((c & (REC_CHUNK - 1)) == REC_CHUNK - 1) {
+                __syncwarp();
+                stage_chunk(rec, dr, (c >> REC_CHUNK_LOG) + 2, L, lane);
+            }
+        }
+        cp_async_wait_all();
+        __syncwarp();
+    }
+}
+
+// Traceback sweep over the candidate pairs: the FP32 Viterbi DP again, on the
+// score matrices p2s_kernel wrote (read a 32-column chunk at a time into the
+// anti-diagonal ring), with the btck code of every cell stored column-major
+// and the strips of a pair pipelined over warps.
+__global__ void __launch_bounds__(P1TC_WARPS * 32, 1)
+p1tc_kernel(P1Args a, const float* __restrict__ qbkg)
+{
+    extern __shared__ float smem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __shared__ signed char btr_all[P1TC_WARPS][32][33];
+    signed char(*btr)[33] = btr_all[wid];
+    float* wb = smem + wid * P1TC_WARP_FLOATS;
+    float* ring = wb;                                         // [P1C_RING][32] scores
+    float* trn = ring + P1C_RING * 32;                        // [P1C_RING][P1C_TRS] transitions
+    float* bnd = trn + P1C_RING * P1C_TRS;                    // [BND_FLOATS] row above the strip
+    (void)qbkg;
+
+    const int Lq = a.Lq;
+    const int nstrips = (Lq + 31) >> 5;
+    const int nitems = a.nwork * nstrips;
     bool broken = false;
 
     for (;;) {
@@ -751,12 +830,10 @@ p1tc_kernel(P1Args a, const float* __restrict__ qbkg)
         const int L = a.plen[p];
         const long long off = a.poff[p];
         const float* __restrict__ dr = a.drec + off * DR_STRIDE;
-        const float* __restrict__ bd = a.pbkg + (long long)p * NAA;
         const int edge = corner_edge(Lq, L);
         const long long coff = a.cand_off[cand];
         signed char* bt = a.btck + coff;
-        float* smt = a.smat + coff;
-        float* mmt = a.mmat + coff;
+        const float* smt = a.smat + coff;
         float* pb = a.bnd + (coff / Lq) * 10;
         const float* botr = pb + ((s + 1) & 1) * 5 * L;   // last row of strip s-1
         float* botw = pb + (s & 1) * 5 * L;
@@ -764,21 +841,6 @@ p1tc_kernel(P1Args a, const float* __restrict__ qbkg)
         const int r = s * 32 + lane;
         const bool act = r < Lq;
         const float* __restrict__ qr = a.qrec + (long long)(act ? r : Lq - 1) * QR_STRIDE;
-        RowOps R;
-#pragma unroll
-        for (int i = 0; i < NAA; i++)
-            R.Qt[i] = __fdividef(qr[QR_TRG + i], 0.5f * (qbkg[i] + bd[i]));
-#pragma unroll
-        for (int i = 0; i < NCV; i++) R.qcv[i] = qr[QR_CV + i];
-        R.cq = qr[QR_CN];
-        R.pq = qr[QR_PRIOR];
-        R.hq = qr[QR_HQ];
-        {
-            // this strip's SS row tables (built once per query, c2_set_query)
-            const float* __restrict__ us = a.qU + (long long)s * MAX_SSSS_CARD * 32 + lane;
-#pragma unroll 8
-            for (int c = 0; c < card; c++) U[c * 32 + lane] = __ldg(us + c * 32);
-        }
         WfLane D;
         {
             float q7[7];
@@ -805,34 +867,22 @@ p1tc_kernel(P1Args a, const float* __restrict__ qbkg)
         const bool wr_bot = (lane == 31) && (s + 1 < nstrips);
         __syncwarp();
         bnd_put(bnd, lane, bc[0], bc[1], bc[2], bc[3], bc[4]);
-        stage_chunk(rec, dr, 0, L, lane);
-        stage_chunk(rec, dr, 1, L, lane);
         const int nch = (L + 31) >> 5;
         const int kend = L + 31;
         for (int m = 0; 32 * m < kend; m++) {
-            // ---- score stage: columns [32m, min(32m + 32, L))
+            // ---- score stage: columns [32m, min(32m + 32, L)) from the score
+            // matrix (the lanes' rows of one column: one 128-byte line), and
+            // the columns' transitions
             if (m < nch) {
                 const int c0 = 32 * m, c1 = min(c0 + 32, L);
                 const bool hasc = __any_sync(FULL, cA >= c0 || cB < c1);
+#pragma unroll 8
                 for (int c = c0; c < c1; c++) {
-                    if ((c & (REC_CHUNK - 1)) == 0) {
-                        cp_async_wait_1();
-                        __syncwarp();
-                    }
-                    const float* rc = rec + (c & (REC_SLOTS - 1)) * DR_STRIDE;
-                    float mod;
-                    float Sc = cell_score<P1TC_CVREP>(R, reinterpret_cast<const float4*>(rc), U, cvtab, sc, lane, mod);
-                    if (act) {
-                        smt[(long long)c * Lq + r] = Sc;
-                        mmt[(long long)c * Lq + r] = mod;
-                    }
+                    float Sc = act ? __ldcg(smt + (long long)c * Lq + r) : 0.f;
                     if (hasc && (c <= cA || c >= cB)) Sc = -9.f;
                     ring[((c + lane) & (P1C_RING - 1)) * 32 + lane] = Sc;
-                    if (lane < DPT_N) trn[(c & (P1C_RING - 1)) * P1C_TRS + lane] = rc[DR_TRN + dpt_src(lane)];
-                    if ((c & (REC_CHUNK - 1)) == REC_CHUNK - 1) {
-                        __syncwarp();
-                        stage_chunk(rec, dr, (c >> REC_CHUNK_LOG) + 2, L, lane);
-                    }
+                    if (lane < DPT_N)
+                        trn[(c & (P1C_RING - 1)) * P1C_TRS + lane] = __ldg(dr + (long long)c * DR_STRIDE + DR_TRN + dpt_src(lane));
                 }
             }
             // the row above for chunk m + 1, loaded while this stage runs
@@ -870,7 +920,6 @@ p1tc_kernel(P1Args a, const float* __restrict__ qbkg)
             bnd_put(bnd, lane, D.bnxt[0], D.bnxt[1], D.bnxt[2], D.bnxt[3], D.bnxt[4]);
             __syncwarp();
         }
-        cp_async_wait_all();
         // the strip's maximum: largest score, then smallest row, then smallest column
         float best = D.best;
         int brow = (best > 0.f) ? r : 0x7fffffff;
@@ -1610,9 +1659,23 @@ cudaError_t launch_p1(const P1Args& a, const float* qbkg, int which, int grid, c
     }
     const size_t sm = p1_smem_bytes(a.sc.cvcard);
     if (which == P1K_TRACEBACK) {
-        const size_t smt = (size_t)(a.sc.cvcard * P1TC_CVREP + P1TC_WARPS * P1C_WARP_FLOATS) * sizeof(float);
-        cudaError_t e = cudaFuncSetAttribute(p1tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
+        // the score matrices first (their own work counter, a.counter[1]),
+        // then the sweep over them
+        const size_t sms = (size_t)(a.sc.cvcard * P1TC_CVREP + P2S_WARPS * P2S_WARP_FLOATS) * sizeof(float);
+        cudaError_t e = cudaFuncSetAttribute(p2s_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms);
         if (e != cudaSuccess) return e;
+        int occ = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p2s_kernel, P2S_WARPS * 32, sms)) != cudaSuccess)
+            return e;
+        int dev = 0, nsm = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        const long long nit = (long long)a.nwork * ((a.Lq + 31) / 32);
+        const int gs = (int)std::min<long long>((long long)std::max(occ, 1) * nsm, (nit + P2S_WARPS - 1) / P2S_WARPS);
+        p2s_kernel<<<gs, P2S_WARPS * 32, sms, st>>>(a, qbkg);
+        const size_t smt = (size_t)P1TC_WARPS * P1TC_WARP_FLOATS * sizeof(float);
+        if ((e = cudaFuncSetAttribute(p1tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt)) != cudaSuccess)
+            return e;
         p1tc_kernel<<<grid, P1TC_WARPS * 32, smt, st>>>(a, qbkg);
     } else {
         cudaFuncSetAttribute(p1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

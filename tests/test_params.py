@@ -76,13 +76,13 @@ def test_library_exports_header_symbols():
 
 def test_create_rejects_cv_maps_beyond_shared_memory(params):
     """c2_create refuses, before touching a device, a CV map larger than the
-    traceback sweep's shared-memory layout holds (169 entries; the reference's
-    map has 93)."""
+    FP32 score kernels' shared-memory tables hold (256 entries; the
+    reference's map has 93)."""
     import copy
     from comer2_b200 import native
     lib = native.load()
     p = copy.deepcopy(params)
-    card = 200
+    card = 300
     p.cvs2s_keys = np.arange(card, dtype=np.float32) * 0.5 - 2.5
     p.cvs2s_values = np.zeros(card, np.float32)
     assert p.cvs2s_card == card
