@@ -342,15 +342,25 @@ __global__ void __launch_bounds__(SCF * NDS, 2) stats_kernel(StatsArgs a)
     for (int k = tid; k < NSCALED; k += SCF * NDS) hist[k] = 0u;
     __syncthreads();
     // histogram of rint(32 s), s clamped to [-10, 10]: warp ty takes db
-    // columns, its lanes the query rows of a column (coalesced reads)
+    // columns, its lanes the query rows of a column (coalesced reads), eight
+    // rows per lane loaded before their counts are added (loads in flight)
     for (int x = ty; x < L; x += NDS) {
         if (a.xuninf && a.daa[off + x] == 'X') continue;
         const float* __restrict__ col = sm + (long long)x * Lq;
-        for (int y = tx; y < Lq; y += SCF) {
-            if (a.xuninf && a.qaa[y] == 'X') continue;
-            float s = col[y];
-            s = s < -10.f ? -10.f : (s > 10.f ? 10.f : s);
-            atomicAdd(&hist[(int)rintf(s * SCF) - SMIN], 1u);
+        for (int y0 = tx; y0 < Lq; y0 += 8 * SCF) {
+            float v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int y = y0 + u * SCF;
+                v[u] = y < Lq ? col[y] : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int y = y0 + u * SCF;
+                if (y >= Lq || (a.xuninf && a.qaa[y] == 'X')) continue;
+                const float s = v[u] < -10.f ? -10.f : (v[u] > 10.f ? 10.f : v[u]);
+                atomicAdd(&hist[(int)rintf(s * SCF) - SMIN], 1u);
+            }
         }
     }
     __syncthreads();
