@@ -332,6 +332,46 @@ def adjoint_workload(args):
     h.close()
 
 
+def kernel_list(args):
+    """Device time of every kernel (and copy / set) of one search of a
+    single-query workload, BF16 score form, database and query resident, from
+    the CUDA activity records of torch.profiler (CUPTI): real launch times of a
+    normal run, not a replaying profiler's.  One JSON line per kernel name."""
+    import collections
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    from comer2_b200 import params as P, synth as S
+    from comer2_b200.native import Handle, SCORE_BF16_TC
+    if args.workload not in (0, 1, 4):
+        raise SystemExit("--kernel-list: workloads 0, 1 and 4")
+    w = S.config(args.workload, seed=0, scale=args.scale)
+    q = w.queries[0]
+    h = Handle(P.load_default(), 0)
+    h.upload_db(w.db)
+    h.set_score_mode(SCORE_BF16_TC)
+    h.search(q)
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        h.search(q)
+        torch.cuda.synchronize()
+    agg = collections.OrderedDict()
+    for e in prof.events():
+        if e.device_type.name != "CUDA":
+            continue
+        nm = e.name.split("(")[0]
+        low = nm.lower()
+        if "memset" in low or "memcpy" in low:
+            nm = "[memset]" if "memset" in low else "[memcpy]"
+        a = agg.setdefault(nm, [0, 0.0])
+        a[0] += 1
+        a[1] += e.device_time_total
+    tot = sum(v[1] for v in agg.values())
+    for k, (n, t) in sorted(agg.items(), key=lambda x: -x[1][1]):
+        print(json.dumps({"workload": args.workload, "kernel": k, "launches": n, "ms": round(t / 1e3, 3),
+                          "share": round(t / tot, 4)}))
+    h.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -343,9 +383,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--score-mode", default="bf16", choices=["fp32", "bf16"],
                     help="phase-1 score contractions: FP32 CUDA cores or split-BF16 tensor cores")
+    ap.add_argument("--kernel-list", action="store_true",
+                    help="instead of the bench line: the device time of every kernel of one search of the "
+                         "workload (0, 1 or 4), from a CUPTI activity trace (torch.profiler), one JSON line each")
     ap.add_argument("--workload", type=int, default=1, choices=sorted(WORKLOADS),
                     help="synthetic configuration (1: the headline; 2: 64 queries through the batch call)")
     args = ap.parse_args()
+    if args.kernel_list:
+        return kernel_list(args)
     if args.workload == 2:
         return batch_workload(args)
     if args.workload == 3:
