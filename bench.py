@@ -243,7 +243,7 @@ def batch_workload(args):
     for name, mode in (("bf16", SCORE_BF16_TC), ("fp32", SCORE_FP32)):
         h.set_score_mode(mode)
         for _ in range(max(1, args.warmup)):
-            h.search_batch(S.concat(w.queries[:4]), nworkers=2)
+            h.search_batch(qs, nworkers=2)
         ts, nh = [], 0
         for _ in range(max(1, args.steps)):
             torch.cuda.synchronize()
