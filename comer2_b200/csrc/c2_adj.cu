@@ -24,16 +24,18 @@
 // rows of one pair per warp, strips handed out by a global counter in the
 // order of their dependencies (all pairs' strip 0, then strip 1, ...; the
 // backward sweep from the last strip up), so a pair is swept by up to
-// nstrips warps at once, each trailing the strip it depends on by about one
-// 32-column chunk (bounded waits on published progress, as the phase-2
-// sweeps).  Checkpointing: the forward sweep keeps only the last row of every
-// strip (5 states x L per strip, the rows the next strip reads) and each
-// strip's partial log-sum; the backward sweep recomputes its strip's forward
-// states from the checkpoint row above into a per-warp scratch (32 rows x
-// (L + 31) x 5 states), then runs the outside recursion over the same rows
-// (bottom row first) and forms every edge posterior of the strip as it goes,
-// so neither F nor B is ever stored for the whole matrix: memory per cell is
-// the 3 score arrays and the 2 outputs.
+// nstrips warps at once, each trailing the strip it depends on by about 40
+// columns (bounded waits on published progress, as the phase-2 sweeps).
+// Memory: the forward sweep keeps the last row of every strip (5 states x L
+// per strip, the rows the next strip reads) and each strip's partial log-sum,
+// and, when they fit (20 bytes a cell), every forward state.  The backward
+// sweep takes its strip's forward states from there, or -- checkpointing,
+// when they did not fit -- recomputes them from the checkpoint row above into
+// a per-warp scratch (32 rows x (L + 31) x 5 states); it then runs the
+// outside recursion over the same rows (bottom row first) and forms every
+// edge posterior of the strip as it goes.  B is never stored for the matrix,
+// and with checkpointing neither is F: memory per cell is then the 3 score
+// arrays and the 2 outputs.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -348,10 +350,11 @@ __device__ __forceinline__ void adj_fwd_strip(const AdjArgs& a, int m, int s, in
         nw.DN = xlse2(up.MM + q7[TMD], up.DN + q7[TDD]);
         nw.ND = xlse2(left.MM + t7[TMD], left.ND + t7[TDD]);
         if (valid) {
-            if (RECOMP) {
+            if (RECOMP || Fw) {
                 float* o = Fw + (long long)k * 160 + lane;
                 o[0] = nw.MM; o[32] = nw.MI; o[64] = nw.IM; o[96] = nw.DN; o[128] = nw.ND;
-            } else {
+            }
+            if (!RECOMP) {
                 if (nw.MM > zm) { zs = zs * xexp(zm - nw.MM) + 1.f; zm = nw.MM; }
                 else zs += xexp(nw.MM - zm);
             }
@@ -381,7 +384,9 @@ __global__ void __launch_bounds__(ADJ_WARPS * 32) adj_fwd_kernel(AdjArgs a)
         const int2 ms = a.items_f[item];
         const int m = ms.x, s = ms.y;
         float zm = -INFINITY, zs = 0.f;
-        adj_fwd_strip<false>(a, m, s, lane, rabs[wid], trss[wid], nullptr, broken, zm, zs);
+        // the strip's forward states kept for the backward sweep when they fit
+        float* Fw = a.Fall ? a.Fall + 5 * a.off[m] + (long long)s * (a.plen[a.prof[m]] + 31) * 160 : nullptr;
+        adj_fwd_strip<false>(a, m, s, lane, rabs[wid], trss[wid], Fw, broken, zm, zs);
         // combine the lanes' (max, sum) pairs
 #pragma unroll
         for (int o = 16; o >= 1; o >>= 1) {
@@ -610,7 +615,7 @@ __global__ void __launch_bounds__(ADJ_WARPS * 32) adj_bwd_kernel(AdjArgs a)
     __shared__ __align__(16) float rabs[ADJ_WARPS][32 * 8];
     __shared__ float trss[ADJ_WARPS][128 * 7];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    float* Fw = a.scratch + ((long long)blockIdx.x * ADJ_WARPS + wid) * a.scratch_stride;
+    float* const scr = a.Fall ? nullptr : a.scratch + ((long long)blockIdx.x * ADJ_WARPS + wid) * a.scratch_stride;
     bool broken = false;
     for (;;) {
         int item = 0;
@@ -619,8 +624,16 @@ __global__ void __launch_bounds__(ADJ_WARPS * 32) adj_bwd_kernel(AdjArgs a)
         if (item >= a.nitems) break;
         const int2 ms = a.items_b[item];
         const int m = ms.x, s = ms.y;
-        float zm = 0.f, zs = 0.f;
-        adj_fwd_strip<true>(a, m, s, lane, rabs[wid], trss[wid], Fw, broken, zm, zs);
+        const float* Fw;
+        if (a.Fall) {
+            // the forward sweep kept the strip's states
+            Fw = a.Fall + 5 * a.off[m] + (long long)s * (a.plen[a.prof[m]] + 31) * 160;
+        } else {
+            // checkpointing: the strip's states again, from the row above
+            float zm = 0.f, zs = 0.f;
+            adj_fwd_strip<true>(a, m, s, lane, rabs[wid], trss[wid], scr, broken, zm, zs);
+            Fw = scr;
+        }
         __syncwarp();
         adj_bwd_strip(a, m, s, lane, rabs[wid], trss[wid], Fw, broken);
         __syncwarp();

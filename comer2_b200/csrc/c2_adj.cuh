@@ -50,7 +50,9 @@ struct AdjArgs {
     int* prog;              // [2][nitems] columns published of frow / brow rows (by soff + strip)
     float* zpart;           // [nitems][2] (max, scaled sum) of a strip's exp(F.MM)
     float* gpart;           // [nitems][9] a strip's gradient sums
-    float* scratch;         // per backward warp: forward states of its strip, [(Lmax + 31) * 5 * 32]
+    float* Fall;            // forward states of every strip, when they fit (else null): strip s of
+                            // pair m at Fall + 5 off[m] + s (L + 31) 160, [step][state][lane]
+    float* scratch;         // per backward warp (Fall null): forward states of its strip, [(Lmax + 31) * 5 * 32]
     long long scratch_stride;
     int* counter;           // [2] work counters of the forward and backward sweeps
     int* status;            // device status (PIPE_ERR_TIMEOUT)

@@ -158,6 +158,8 @@ struct c2_handle {
     DevBuf<long long> d_adjoff, d_adjroff, d_adjqpos, d_adjsoff;
     DevBuf<int2> d_adjitems;
     DevBuf<float> d_adjbuf, d_adjlogz, d_adjgrad, d_adjpart, d_adjscr;
+    DevBuf<float> d_adjF;            // all forward states, when they fit (no recompute in the backward sweep)
+    bool adj_keepF = false;
     DevBuf<float> d_adjqrec, d_adjqtrn, d_adjqcfx, d_adjqbkg;   // queries of c2_set_query_batch
     std::vector<int> adj_qlen;                                   // their lengths
     std::vector<long long> adj_qstart;                           // and first rows
@@ -1909,6 +1911,7 @@ static void fill_adj(c2_handle* h, AdjArgs& a)
     a.prog = h->d_adjprog.p;
     a.zpart = h->d_adjpart.p;
     a.gpart = h->d_adjpart.p + 2LL * h->adj_nitems;
+    a.Fall = h->adj_keepF ? h->d_adjF.p : nullptr;
     a.scratch = h->d_adjscr.p;
     a.scratch_stride = (long long)(h->adj_Lmax + 31) * 160;
     a.counter = h->d_adjctr.p;
@@ -1995,13 +1998,31 @@ static c2_status logz_fwd_pairs(c2_handle* h, const int32_t* profiles, const int
     // that scratch does not fit (the memory budget or the device)
     int fwd_occ = 4, bwd_occ = 4;
     CK(adj_occupancy(&fwd_occ, &bwd_occ));
-    const size_t per_cta = (size_t)ADJ_WARPS * (lmax + 31) * 160 * sizeof(float);
     const long long want = std::min<long long>((long long)h->nsm * std::max(bwd_occ, 1), (items + ADJ_WARPS - 1) / ADJ_WARPS);
-    h->adj_bgrid = 0;
-    for (long long g = want; g >= 1 && h->adj_bgrid == 0; g /= 2)
-        if (h->d_adjscr.ensure((size_t)g * per_cta / sizeof(float), h->budget) == cudaSuccess) h->adj_bgrid = (int)g;
-    (void)cudaGetLastError();   // a refused allocation above is not an error of what follows
-    if (h->adj_bgrid == 0) return fail(h, C2_ERR_NOMEM, "logz_fwd: backward sweep scratch (%zu bytes per CTA) failed", per_cta);
+    h->adj_bgrid = (int)want;
+    // The forward sweep keeps every forward state (20 bytes a cell) when that
+    // takes at most a quarter of the free device memory and fits the budget;
+    // otherwise the backward sweep recomputes each strip's states from the
+    // checkpoint row above into per-warp scratch (32 rows x (Lmax + 31)
+    // columns x 5 floats), its grid halved while that scratch does not fit.
+    h->adj_keepF = false;
+    {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && (size_t)acc * 5 * sizeof(float) <= fr / 4 &&
+            h->d_adjF.ensure((size_t)acc * 5, h->budget) == cudaSuccess)
+            h->adj_keepF = true;
+        (void)cudaGetLastError();   // a refused allocation is not an error of what follows
+    }
+    if (!h->adj_keepF) {
+        h->d_adjF.release();
+        const size_t per_cta = (size_t)ADJ_WARPS * (lmax + 31) * 160 * sizeof(float);
+        h->adj_bgrid = 0;
+        for (long long g = want; g >= 1 && h->adj_bgrid == 0; g /= 2)
+            if (h->d_adjscr.ensure((size_t)g * per_cta / sizeof(float), h->budget) == cudaSuccess) h->adj_bgrid = (int)g;
+        (void)cudaGetLastError();
+        if (h->adj_bgrid == 0)
+            return fail(h, C2_ERR_NOMEM, "logz_fwd: backward sweep scratch (%zu bytes per CTA) failed", per_cta);
+    }
     CK(cudaMemcpyAsync(h->d_adjprof.p, profiles, (size_t)npairs * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_adjLq.p, Lq, (size_t)npairs * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d_adjqpos.p, qpos, (size_t)npairs * 8, cudaMemcpyHostToDevice, h->stream));

@@ -156,3 +156,49 @@ def test_batch_of_independent_pairs(params, orc64):
     assert np.array_equal(z1, z[[1, 4]])
     assert np.array_equal(g1, g[[1, 4]])
     h.close()
+
+
+def test_checkpointed_backward_matches_kept_states(params):
+    """With room for every forward state the backward sweep reads them; under
+    a device memory budget that leaves no room for them it recomputes each
+    strip's states from the checkpoint row above (strip-row checkpointing).
+    Both give the same log-partitions, gradients and per-cell values, bit for
+    bit (the recomputation is the same arithmetic)."""
+    from comer2_b200.native import Handle
+    rng = np.random.default_rng(21)
+    qs = [S.random_profiles(rng, [n]) for n in (70, 41)]
+    parts = [S.planted_homolog(rng, qs[i % 2], L, seg_lo=15, seg_hi=30) for i, L in enumerate((64, 90, 57))]
+    db = S.concat(parts)
+    Q = S.concat(qs)
+    qof, prof = np.array([0, 1, 0], np.int32), np.array([0, 1, 2], np.int32)
+    wss, wcv = params.ssswgt, params.cvswgt
+    res = []
+    limit = 0
+    for run in range(2):
+        h = Handle(params, 0)
+        h.upload_db(db)
+        h.set_query_batch(Q)
+        if run == 1:
+            h.set_memory_limit(limit)
+        z = h.logz_fwd_batch(qof, prof, THETA, wss, wcv)
+        g = h.logz_bwd()
+        cells = [h.logz_cells(k, int(db.lengths[prof[k]])) for k in range(3)]
+        res.append((z, g, cells))
+        if run == 0:
+            # every budget byte the first run used, less the forward states
+            # (5 floats a cell in wavefront order), plus one backward CTA's
+            # scratch and a margin smaller than the forward states
+            nc = sum(((int(Q.lengths[q]) + 31) // 32) * (int(db.lengths[p]) + 31) * 32 for q, p in zip(qof, prof))
+            lmax = int(db.lengths.max())
+            one_cta = 4 * (lmax + 31) * 160 * 4
+            fbytes = 20 * nc
+            assert fbytes > one_cta + (64 << 10)
+            limit = h.memory_use() - fbytes + one_cta + (64 << 10)
+        else:
+            assert h.memory_use() <= limit
+        h.close()
+    (z0, g0, c0), (z1, g1, c1) = res
+    assert np.array_equal(z0, z1)
+    assert np.array_equal(g0, g1)
+    for (a0, b0), (a1, b1) in zip(c0, c1):
+        assert np.array_equal(a0, a1) and np.array_equal(b0, b1)
