@@ -643,6 +643,37 @@ static c2_status upload_records(c2_handle* h, const c2_profiles* d)
         b ^= 1;
         k0 = k1;
     }
+    // the raw transitions ([N + P][7] floats, the MAP and statistics stages'
+    // copy) through the same buffers: copied into a pinned buffer by the host
+    // threads while the previous piece goes over the bus, instead of one
+    // synchronous copy from pageable memory
+    {
+        const size_t total = (size_t)(N + P) * 7 * sizeof(float);
+        const size_t piece = (size_t)cap * DR_STRIDE * 4;
+        const char* src = reinterpret_cast<const char*>(d->trn);
+        char* dst = reinterpret_cast<char*>(h->db->d_dtrn.p);
+        for (size_t o = 0; o < total; o += piece) {
+            const size_t n = std::min(piece, total - o);
+            if (used[b]) CK(cudaEventSynchronize(S.ev[b]));
+            char* out = reinterpret_cast<char*>(S.buf[b]);
+            const int nth = (int)std::max<size_t>(1, std::min<size_t>((size_t)nt, n >> 22));
+            std::vector<std::thread> pool;
+            for (int t = 0; t < nth; t++) {
+                const size_t a0 = n * t / nth, a1 = n * (t + 1) / nth;
+                try {
+                    pool.emplace_back([=]() { memcpy(out + a0, src + o + a0, a1 - a0); });
+                } catch (...) {
+                    memcpy(out + a0, src + o + a0, a1 - a0);   // no thread to be had: copy here
+                }
+            }
+            for (auto& th : pool) th.join();
+            S.sync = true;
+            CK(cudaMemcpyAsync(dst + o, out, n, cudaMemcpyHostToDevice, h->stream));
+            CK(cudaEventRecord(S.ev[b], h->stream));
+            used[b] = true;
+            b ^= 1;
+        }
+    }
     CK(cudaStreamSynchronize(h->stream));
     return C2_OK;
 }
@@ -671,16 +702,17 @@ extern "C" c2_status c2_upload_db(c2_handle* h, const c2_profiles* d, uint64_t t
     if (h->db->d_drec.ensure((size_t)N * DR_STRIDE, h->budget) || h->db->d_pbkg.ensure(bkg.size(), h->budget) || h->db->d_plen.ensure(P, h->budget) ||
         h->db->d_order.ensure(P, h->budget) || h->db->d_poff.ensure(P, h->budget) || h->d_best.ensure(P, h->budget) || h->d_coords.ensure(P, h->budget))
         return fail(h, C2_ERR_NOMEM, "device allocation for %d profiles / %lld positions failed", P, (long long)N);
-    if ((st = upload_records(h, d)) != C2_OK) return st;
+    if (h->db->d_dtrn.ensure((size_t)(N + P) * 7, h->budget))
+        return fail(h, C2_ERR_NOMEM, "device allocation of db transitions failed");
+    if ((st = upload_records(h, d)) != C2_OK) return st;   // the records and the raw transitions
     CK(cudaMemcpy(h->db->d_pbkg.p, bkg.data(), bkg.size() * 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->db->d_plen.p, d->lengths, (size_t)P * 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->db->d_order.p, order.data(), (size_t)P * 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->db->d_poff.p, poff.data(), (size_t)P * 8, cudaMemcpyHostToDevice));
     // raw transitions, residues, SS states and ENOs for the statistics and MAP stages
-    if (h->db->d_dtrn.ensure((size_t)(N + P) * 7, h->budget) || h->db->d_daa.ensure((size_t)N, h->budget) || h->db->d_dss.ensure((size_t)N, h->budget) ||
+    if (h->db->d_daa.ensure((size_t)N, h->budget) || h->db->d_dss.ensure((size_t)N, h->budget) ||
         h->db->d_peno.ensure((size_t)P, h->budget))
         return fail(h, C2_ERR_NOMEM, "device allocation of db side arrays failed");
-    CK(cudaMemcpy(h->db->d_dtrn.p, d->trn, (size_t)(N + P) * 7 * 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->db->d_daa.p, d->aa, (size_t)N, cudaMemcpyHostToDevice));
     if (d->ssstate) CK(cudaMemcpy(h->db->d_dss.p, d->ssstate, (size_t)N, cudaMemcpyHostToDevice));
     else CK(cudaMemset(h->db->d_dss.p, ' ', (size_t)N));
