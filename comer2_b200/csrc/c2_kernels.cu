@@ -774,22 +774,27 @@ p2s_kernel(P1Args a, const float* __restrict__ qbkg)
         }
         stage_chunk(rec, dr, 0, L, lane);
         stage_chunk(rec, dr, 1, L, lane);
-        for (int c = 0; c < L; c++) {
-            if ((c & (REC_CHUNK - 1)) == 0) {
-                cp_async_wait_1();
-                __syncwarp();
+        // a staged chunk of REC_CHUNK columns at a time: its cells are
+        // independent, so their chains overlap
+        for (int c0 = 0; c0 < L; c0 += REC_CHUNK) {
+            cp_async_wait_1();
+            __syncwarp();
+#pragma unroll
+            for (int u = 0; u < REC_CHUNK; u++) {
+                const int c = c0 + u;
+                if (c < L) {
+                    const float* rc = rec + (c & (REC_SLOTS - 1)) * DR_STRIDE;
+                    float mod;
+                    const float Sc =
+                        cell_score<P1TC_CVREP>(R, reinterpret_cast<const float4*>(rc), U, cvtab, sc, lane, mod);
+                    if (act) {
+                        smt[(long long)c * Lq + r] = Sc;
+                        mmt[(long long)c * Lq + r] = mod;
+                    }
+                }
             }
-            const float* rc = rec + (c & (REC_SLOTS - 1)) * DR_STRIDE;
-            float mod;
-            const float Sc = cell_score<P1TC_CVREP>(R, reinterpret_cast<const float4*>(rc), U, cvtab, sc, lane, mod);
-            if (act) {
-                smt[(long long)c * Lq + r] = Sc;
-                mmt[(long long)c * Lq + r] = mod;
-            }
-            if ((c & (REC_CHUNK - 1)) == REC_CHUNK - 1) {
-                __syncwarp();
-                stage_chunk(rec, dr, (c >> REC_CHUNK_LOG) + 2, L, lane);
-            }
+            __syncwarp();
+            stage_chunk(rec, dr, (c0 >> REC_CHUNK_LOG) + 2, L, lane);
         }
         cp_async_wait_all();
         __syncwarp();
