@@ -455,24 +455,29 @@ static inline void trn_of(const c2_profiles* d, int k, int i, float* t7)
     t7[TIM] = a[3]; t7[TII] = b[4]; t7[TDM] = a[5]; t7[TDD] = a[6];
 }
 
-// Wavefront steps by which a strip trails the one above in the sweeps' strip
-// pipeline: a strip starts a chunk once the strip above has published the
-// chunk's 32 columns, which lane 31 of that strip finishes 31 steps after
-// its lane 0.
-constexpr int STRIP_LAG = 64;
+// Dispatch lag of the sweeps' work-item order, in wavefront steps: strip s of
+// a pair is handed out about `lag` steps' worth of work after strip s - 1.
+// The physical lag is about 96 steps for the traceback sweep (the row above
+// is loaded a 32-column chunk ahead and published once per chunk) and about
+// 48 for the MAP sweeps (8 columns at a time); handing strips out later than
+// that leaves fewer warps polling for their predecessor, and the values below
+// were chosen by measurement (kernel times on configs 1 and 4 with lags of
+// 64 / 96 / 128 / 160-192 / 256-320: traceback sweep 21.4 -> 16.3 ms, MAP DP
+// 22.4 -> 17.5-18.0 ms and MAP forward-backward 74.4 -> 72.3 ms on config 4).
+constexpr int STRIP_LAG_TB = 320, STRIP_LAG_MAP = 192;
 
 // Work-item table of a strip-pipelined sweep over np pairs (in processing
 // order, lengths lens): item (p, s) at key p + K s, K = pairs started per
-// strip lag when nwarps warps are busy, so that strip s of a pair is handed
+// strip lag (lag steps) when nwarps warps are busy, so that strip s of a pair is handed
 // out about when strip s - 1 is far enough ahead.  Ties keep s order, so
 // (p, s - 1) always precedes (p, s).
 
-static void strip_items(const std::vector<int>& lens, int nstrips, int nwarps, std::vector<int>& items)
+static void strip_items(const std::vector<int>& lens, int nstrips, int nwarps, int lag, std::vector<int>& items)
 {
     const int np = (int)lens.size();
     double lm = 31.0;
     for (int L : lens) lm += (double)L / std::max(1, np);
-    const double K = (double)STRIP_LAG * nwarps / (nstrips * lm);
+    const double K = (double)lag * nwarps / (nstrips * lm);
     // key(p, s) = p + K s = b + f_s with bucket b = p + floor(K s) and
     // f_s = frac(K s): each bucket holds one item per strip, ordered by f_s
     // and, for equal f_s, larger s first (its p is smaller); the same order
@@ -1246,7 +1251,7 @@ static c2_status finalize_set(c2_handle* h, const std::vector<int>& cand, int32_
                          [&](int x, int y) { return h->h_plen[h->h_cand[x]] > h->h_plen[h->h_cand[y]]; });
         std::vector<int> lens(nc), items;
         for (int i = 0; i < nc; i++) lens[i] = h->h_plen[h->h_cand[wo[i]]];
-        strip_items(lens, (h->Lq + 31) / 32, h->nsm * P1TC_WARPS, items);
+        strip_items(lens, (h->Lq + 31) / 32, h->nsm * P1TC_WARPS, STRIP_LAG_TB, items);
         if (h->d_worder.ensure(nc, h->budget) || h->d_tbitems.ensure(items.size(), h->budget))
             return fail(h, C2_ERR_NOMEM, "candidate order allocation failed");
         CK(cudaMemcpyAsync(h->d_worder.p, wo.data(), (size_t)nc * 4, cudaMemcpyHostToDevice, h->stream));
@@ -1538,7 +1543,7 @@ extern "C" c2_status c2_run_map(c2_handle* h, int32_t* nhits)
     {
         std::vector<int> lens(nm), items;
         for (int i = 0; i < nm; i++) lens[i] = h->h_plen[h->h_cand[h->h_mapcand[i]]];
-        strip_items(lens, (h->Lq + 31) / 32, h->grid * P1_WARPS, items);
+        strip_items(lens, (h->Lq + 31) / 32, h->grid * P1_WARPS, STRIP_LAG_MAP, items);
         if (h->d_mapitems.ensure(items.size(), h->budget)) return fail(h, C2_ERR_NOMEM, "MAP work table allocation failed");
         CK(cudaMemcpyAsync(h->d_mapitems.p, items.data(), items.size() * 4, cudaMemcpyHostToDevice, h->stream));
         CK(cudaStreamSynchronize(h->stream));
