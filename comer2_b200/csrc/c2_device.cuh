@@ -101,8 +101,8 @@ constexpr int P1C_WARP_FLOATS =
     P1C_RING * 32 + P1C_RING * P1C_TRS + MAX_SSSS_CARD * 32 + REC_SLOTS * DR_STRIDE + BND_FLOATS;
 // traceback sweep over the stored score matrices: per warp the score ring, the
 // transition ring, the row above and a [32][33]-byte traceback column ring;
-// 16 warps per SM.  P1TC_CVREP: CV table replicas of the phase-2 score kernel
-constexpr int P1TC_WARPS = 16, P1TC_CVREP = 8;
+// 17 warps per SM.  P1TC_CVREP: CV table replicas of the phase-2 score kernel
+constexpr int P1TC_WARPS = 17, P1TC_CVREP = 8;
 constexpr int P1TC_WARP_FLOATS = P1C_RING * 32 + P1C_RING * P1C_TRS + BND_FLOATS;
 // phase-2 score kernel: 8 warps per CTA, per warp the SS row table and the
 // record staging ring; the CV table (P1TC_CVREP replicas) per CTA

@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(256) map_z_kernel(MapArgs a)
     // (strip t, step k) is cell (32 t + i, k - i).  (t, k) advance without a
     // division: W >= 32 > 8, so k wraps at most once per step.
     int t = 0, k = wid;
-#pragma unroll 4
+#pragma unroll 8
     for (int rw = wid; rw < nrows; rw += 8) {
         const int row = 32 * t + lane, col = k - lane;
         if (row < Lq && col >= 0 && col < L) s += fexp(fs[(long long)rw * 32 + lane] - maxF);
