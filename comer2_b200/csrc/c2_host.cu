@@ -804,6 +804,32 @@ static void colm1_exact(const c2_profiles* q, float* qx)
     }
 }
 
+// Effective search space and thresholds of a query of length Lq against the
+// database totals: AbstractScoreMatrix::ComputeLengthAdjustment
+// (libpro/srcsco/AbstractScoreMatrix.cpp:303-380) and
+// JobDispatcher::CalculateScoreThreshold (cualn/JobDispatcher.cpp:809-860)
+static void query_limits(const c2_handle* h, int Lq, unsigned long long* searchspace, unsigned long long* deltalen,
+                         float* scorethld, float* logevthld)
+{
+    length_adjustment(h->prm.gapped_lambda, h->prm.gapped_K, h->prm.gapped_alpha, h->prm.gapped_beta,
+                      (size_t)Lq, h->total_pos, (size_t)h->total_prof, searchspace, deltalen);
+    size_t sspace = (size_t)Lq * (size_t)h->total_pos;
+    float e = h->prm.eval;
+    if (e <= 0.0f) {
+        *scorethld = 999.0f;
+        *logevthld = -99.0f;
+    } else {
+        *logevthld = logf(e);
+        e = (e < 1.0f) ? e * 10.0f : e * 3.0f;
+        e /= h->prm.gapped_K * sspace;
+        if (e <= 0.0f) *scorethld = 999.0f;
+        else {
+            const float sc = -logf(e) / h->prm.gapped_lambda;
+            *scorethld = sc < 0.0f ? 0.0f : sc;
+        }
+    }
+}
+
 extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
 {
     if (!h) return C2_ERR_ARG;
@@ -948,24 +974,20 @@ extern "C" c2_status c2_set_query(c2_handle* h, const c2_profiles* q)
         else CK(cudaMemsetAsync(h->d_qss.p, ' ', (size_t)Lq, h->stream));
     }
     CK(cudaStreamSynchronize(h->stream));
-    length_adjustment(h->prm.gapped_lambda, h->prm.gapped_K, h->prm.gapped_alpha, h->prm.gapped_beta,
-                      (size_t)Lq, h->total_pos, (size_t)h->total_prof, &h->searchspace, &h->deltalen);
-    // thresholds: JobDispatcher::CalculateScoreThreshold (JobDispatcher.cpp:809-860)
-    {
-        size_t sspace = (size_t)Lq * (size_t)h->total_pos;
-        float e = h->prm.eval;
-        if (e <= 0.0f) { h->scorethld = 999.0f; h->logevthld = -99.0f; }
-        else {
-            h->logevthld = logf(e);
-            e = (e < 1.0f) ? e * 10.0f : e * 3.0f;
-            e /= h->prm.gapped_K * sspace;
-            if (e <= 0.0f) h->scorethld = 999.0f;
-            else {
-                float s = -logf(e) / h->prm.gapped_lambda;
-                h->scorethld = s < 0.0f ? 0.0f : s;
-            }
-        }
-    }
+    query_limits(h, Lq, &h->searchspace, &h->deltalen, &h->scorethld, &h->logevthld);
+    return C2_OK;
+}
+
+extern "C" c2_status c2_get_query_limits(const c2_handle* h, int32_t query_length, uint64_t* searchspace,
+                                         uint64_t* deltalen, float* score_threshold, float* logE_threshold)
+{
+    if (!h || query_length <= 0 || !searchspace || !deltalen || !score_threshold || !logE_threshold)
+        return C2_ERR_ARG;
+    if (h->nprof <= 0) return C2_ERR_STATE;
+    unsigned long long ss = 0, dl = 0;
+    query_limits(h, query_length, &ss, &dl, score_threshold, logE_threshold);
+    *searchspace = ss;
+    *deltalen = dl;
     return C2_OK;
 }
 

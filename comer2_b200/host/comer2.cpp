@@ -975,35 +975,46 @@ int run(int argc, char** argv)
         const c2_profiles dv = D.view();
         ck(hh, c2_upload_db(hh, &dv, (uint64_t)totN, (uint64_t)totP), "c2_upload_db");
     };
-    // every query against the chunk uploaded to hh; hits into acc
+    // every query against the chunk uploaded to hh, through the batch call
+    // (two workers, a query's phase 2 beside the next query's phase 1, unless
+    // --dev-mem bounds the memory: the second worker's query and phase-2
+    // buffers would come out of the chunk's budget); hits into acc with global
+    // profile indices
+    const int batch_workers = A.devmem_mb > 0 ? 1 : 2;
+    const c2_profiles qall = Q.view();
+    struct BatchCtx {
+        std::vector<QueryHits>* acc;
+        std::mutex* mu;
+        int64_t gb;
+        int failed_query = -1;
+        c2_status failed = C2_OK;
+    };
+    auto on_query = [](void* user, int32_t q, c2_status st, const c2_hit* hits, int32_t nh, const char* alns,
+                       size_t abytes) {
+        BatchCtx* ctx = static_cast<BatchCtx*>(user);
+        std::lock_guard<std::mutex> lk(*ctx->mu);
+        if (st != C2_OK) {
+            if (ctx->failed == C2_OK) { ctx->failed = st; ctx->failed_query = q; }
+            return;
+        }
+        QueryHits& a = (*ctx->acc)[q];
+        const int64_t base = (int64_t)a.alns.size();
+        for (int i = 0; i < nh; i++) {
+            c2_hit x = hits[i];
+            x.profile += (int32_t)ctx->gb;
+            x.aln_offset += base;
+            a.hits.push_back(x);
+        }
+        a.alns.insert(a.alns.end(), alns, alns + abytes);
+    };
     auto search_chunk = [&](size_t ci, c2_handle* hh) {
-        const int64_t gb = chunks[ci].gbase;
-        for (int qn = 0; qn < Q.nprof(); qn++) {
-            const c2_profiles qv = queries[qn].view();
-            int32_t nh = 0;
-            ck(hh, c2_search(hh, &qv, &nh), "c2_search");
-            size_t abytes = 0;
-            ck(hh, c2_get_hits(hh, nullptr, 0, nullptr, &abytes), "c2_get_hits");
-            std::vector<c2_hit> hits((size_t)std::max(nh, 1));
-            std::vector<char> alns(abytes + 1);
-            ck(hh, c2_get_hits(hh, hits.data(), nh, alns.data(), &abytes), "c2_get_hits");
-            uint64_t sspace = 0, dlen = 0;
-            float thld = 0.f, logevthld = 0.f;
-            ck(hh, c2_get_search_space(hh, &sspace, &dlen), "c2_get_search_space");
-            ck(hh, c2_get_thresholds(hh, &thld, &logevthld), "c2_get_thresholds");
-            std::lock_guard<std::mutex> lk(acc_mu);
-            QueryHits& a = acc[qn];
-            a.sspace = sspace;
-            a.dlen = dlen;
-            a.thld = thld;
-            a.logevthld = logevthld;
-            const int64_t base = (int64_t)a.alns.size();
-            for (int i = 0; i < nh; i++) {
-                hits[i].profile += (int32_t)gb;
-                hits[i].aln_offset += base;
-                a.hits.push_back(hits[i]);
-            }
-            a.alns.insert(a.alns.end(), alns.begin(), alns.begin() + (long)abytes);
+        BatchCtx ctx{&acc, &acc_mu, chunks[ci].gbase};
+        const c2_status st = c2_search_batch(hh, &qall, batch_workers, on_query, &ctx);
+        if (st != C2_OK || ctx.failed != C2_OK) {
+            char buf[512] = {0};
+            c2_last_error(hh, buf, sizeof buf);
+            die("c2_search_batch failed (status " + std::to_string((int)(st != C2_OK ? st : ctx.failed)) +
+                (ctx.failed_query >= 0 ? ", query " + std::to_string(ctx.failed_query) : std::string()) + "): " + buf);
         }
         note(2, "chunk " + std::to_string(ci + 1) + "/" + std::to_string(chunks.size()) + " searched");
     };
@@ -1061,6 +1072,13 @@ int run(int argc, char** argv)
         for (auto& t : th) t.join();
         for (auto& e : errs)
             if (e) std::rethrow_exception(e);
+    }
+    // search space and thresholds of every query (database totals; any
+    // handle with a chunk uploaded has them)
+    for (int qn = 0; qn < Q.nprof(); qn++) {
+        QueryHits& a = acc[qn];
+        ck(h, c2_get_query_limits(h, Q.lengths[qn], &a.sspace, &a.dlen, &a.thld, &a.logevthld),
+           "c2_get_query_limits");
     }
     std::vector<const char*> ddesc;
     for (const auto& s : desc_all) ddesc.push_back(s.c_str());

@@ -31,6 +31,7 @@ EXPORTS = [
     "c2_set_wait_limit", "c2_get_pair_scores", "c2_db2bin_descriptions", "c2_set_device_memory_limit",
     "c2_db2bin_lengths", "c2_db2bin_read_range", "c2_get_device_memory_info", "c2_db_device_bytes",
     "c2_logz_fwd_batch", "c2_set_query_batch", "c2_set_batch_sm_reserve", "c2_get_device_count",
+    "c2_get_query_limits",
     "c2_get_device_memory_use", "c2_get_search_groups",
 ]
 
@@ -209,6 +210,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.c2_set_query_batch.argtypes = [C.c_void_p, P(c2_profiles)]
     lib.c2_set_batch_sm_reserve.argtypes = [C.c_void_p, C.c_int32]
     lib.c2_get_device_count.argtypes = [_i32p]
+    lib.c2_get_query_limits.argtypes = [C.c_void_p, C.c_int32, P(C.c_uint64), P(C.c_uint64), P(C.c_float),
+                                        P(C.c_float)]
     lib.c2_logz_fwd_batch.argtypes = [C.c_void_p, _i32p, _i32p, C.c_int32, _fp, C.c_float, C.c_float, _fp]
     lib.c2_logz_cells.argtypes = [C.c_void_p, C.c_int32, _fp, _fp]
     lib.c2_db2bin_info.argtypes = [C.c_char_p, _i32p, _i64p, C.c_char_p, C.c_size_t]
@@ -479,6 +482,15 @@ class Handle:
         n = C.c_int32()
         self._ck(self.lib.c2_run_map(self._h, C.byref(n)), "c2_run_map")
         return n.value
+
+    def query_limits(self, query_length: int):
+        """(search space, length adjustment, score threshold, log E threshold) of a query
+        of this length against the uploaded database (c2_get_query_limits)."""
+        a, b = C.c_uint64(), C.c_uint64()
+        c, d = C.c_float(), C.c_float()
+        self._ck(self.lib.c2_get_query_limits(self._h, int(query_length), C.byref(a), C.byref(b), C.byref(c),
+                                              C.byref(d)), "c2_get_query_limits")
+        return a.value, b.value, c.value, d.value
 
     def search_space(self):
         a, b = C.c_uint64(), C.c_uint64()

@@ -275,6 +275,16 @@ c2_status c2_get_search_space(const c2_handle* h, uint64_t* searchspace, uint64_
 /* Thresholds computed for the current query. */
 c2_status c2_get_thresholds(const c2_handle* h, float* scorethld, float* logevthld);
 
+/* The same values -- effective search space, length adjustment, score and
+ * log E-value thresholds -- for a query of this length against the uploaded
+ * database (its totals), without setting a query: what a caller of
+ * c2_search_batch needs for the result files of each query
+ * (AbstractScoreMatrix::ComputeLengthAdjustment,
+ * src/libpro/srcsco/AbstractScoreMatrix.cpp:303-380;
+ * JobDispatcher::CalculateScoreThreshold, src/libmycu/cualn/JobDispatcher.cpp:809-860). */
+c2_status c2_get_query_limits(const c2_handle* h, int32_t query_length, uint64_t* searchspace, uint64_t* deltalen,
+                              float* score_threshold, float* logE_threshold);
+
 /* Make the handle issue its work on a caller-owned CUDA stream (a
  * cudaStream_t passed as void*; NULL restores the handle's own stream). */
 c2_status c2_set_stream(c2_handle* h, void* stream);
