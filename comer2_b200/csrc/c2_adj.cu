@@ -67,10 +67,12 @@ __device__ __forceinline__ float xlog(float x)
     return y * XLN2;
 }
 
+// the larger term's exponential is ex2(0) = 1 exactly, the smaller one's
+// difference exactly -|a - b|
 __device__ __forceinline__ float xlse2(float a, float b)
 {
     const float m = fmaxf(a, b);
-    return xlog(xexp(a - m) + xexp(b - m)) + m;
+    return xlog(1.f + xexp(-fabsf(a - b))) + m;
 }
 
 // log(e^v1 + ... + e^v5 + 1): the 1 is the local start (forward) or end (backward)

@@ -54,17 +54,32 @@ __device__ __forceinline__ float hmax3(float a, float b, float c)
     return d;
 }
 
+// flog of an argument known to be above its cut-off (a sum that holds fexp(0))
+__device__ __forceinline__ float flog_big(float x)
+{
+    return (float)(__float_as_int(x) - 1064631197) * 8.2629582959339e-08f;
+}
+
+// fexp(0): 1064631197.0f is 1064631168 as a float
+constexpr int FEXP0_BITS = 1064631168;
+
+// flog(fexp(a - mx) + fexp(b - mx)) + mx with mx = max(a, b): the larger
+// term's difference is exactly 0 and the smaller one's exactly -|a - b|
+// (IEEE subtraction is symmetric under negation), so the sum below is the
+// same float sum, and it is >= fexp(0)
 __device__ __forceinline__ float lse2(float a, float b)
 {
     const float mx = hmax(a, b);
-    return flog(fexp(a - mx) + fexp(b - mx)) + mx;
+    return flog_big(__int_as_float(FEXP0_BITS) + fexp(-fabsf(a - b))) + mx;
 }
 
-// log(sum of five terms + 1): the 1 is the local start (forward) or end (backward)
+// log(sum of five terms + 1): the 1 is the local start (forward) or end
+// (backward); the maximal term contributes fexp(0), so the sum is above
+// flog's cut-off
 __device__ __forceinline__ float lse5p1(float v1, float v2, float v3, float v4, float v5)
 {
     const float mx = hmax(hmax3(0.f, v1, v2), hmax3(v3, v4, v5));
-    return flog(fexp(v1 - mx) + fexp(v2 - mx) + fexp(v3 - mx) + fexp(v4 - mx) + fexp(v5 - mx) + fexp(-mx)) + mx;
+    return flog_big(fexp(v1 - mx) + fexp(v2 - mx) + fexp(v3 - mx) + fexp(v4 - mx) + fexp(v5 - mx) + fexp(-mx)) + mx;
 }
 
 // dynamic score parameters (src/libmycu/cumapdp/CuBatchMAPDP_fwd.cuh:157-171)
